@@ -1,0 +1,211 @@
+/*
+ * galaxy_gpu.h -- C ABI of the B200 polar-grid particle-mesh step.
+ *
+ * The entry points replace the lib15 subroutines of GALAXY v15 that make up
+ * the polar-grid (p2d / p3d) particle-mesh step.  Each one names the
+ * reference routine it stands in for (paths relative to the GALAXY source
+ * tree).  The reference keeps its state in COMMON blocks; here the state is
+ * an opaque context created by gx_grdset.
+ *
+ * Conventions
+ *  - Every entry point returns GX_OK (0) or a negative GX_ERR_* code; the
+ *    message is available from gx_last_error().  Nothing aborts the process.
+ *  - Pointers passed in are host pointers, valid for the duration of the
+ *    call only.  Device memory is owned by the context.
+ *  - A context is not re-entrant: one host thread at a time; all work is
+ *    serialised on the context's own CUDA stream.
+ *  - Coordinates are in grid units: positions x, y[, z]; velocities are
+ *    displacements per step and accelerations are velocity changes per step
+ *    (reference: SRC/lib15/stpgrp.f:26-32).  Particle arrays at the boundary
+ *    are AoS float32 records of 2*ndim words, (x, y[, z], vx, vy[, vz]),
+ *    the coordinate layout of the reference's .pcs records
+ *    (SRC/lib15/loadup.f:36-140).
+ *  - Grid arrays (mass, fields) use the reference mesh layout: index
+ *    ((ir * ngz + iz) * na + it) for ring ir, plane iz, spoke it
+ *    (SRC/lib15/weight.f:236, ncl - 1).
+ */
+#ifndef GALAXY_GPU_H
+#define GALAXY_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GX_OK               0
+#define GX_ERR_ARG         -1   /* invalid argument / configuration        */
+#define GX_ERR_CUDA        -2   /* CUDA runtime error                      */
+#define GX_ERR_STATE       -3   /* call out of order (e.g. no Green table) */
+#define GX_ERR_NOMEM       -4   /* device allocation failed                */
+#define GX_ERR_TIMEOUT     -5   /* a bounded device wait gave up           */
+#define GX_ERR_RANGE       -6   /* size beyond a stated limit              */
+#define GX_ERR_DEVICE      -7   /* device-side check raised its error word */
+
+/* radial coordinate maps u(r) (SRC/lib15/uofgr.f:22-36, grofu.f:25-41) */
+#define GX_RMAP_STDPOL      0   /* u = ln(1 + r) / a,  r = e^{a u} - 1              */
+#define GX_RMAP_LOG         1   /* u = ln(r) / a + uoffs, uoffs = -ln(r0)/a; hole r<r0 */
+
+/* softening rules (SRC/lib15/setgrd.f:178-189) */
+#define GX_SOFT_PLUMMER     1
+#define GX_SOFT_SPLINE      2
+
+/* arithmetic of the step */
+#define GX_PREC_MIXED       0   /* FP32 bulk, FP64 Green table/diagnostics  */
+#define GX_PREC_FP64        1   /* plain FP64 path (the comparison baseline) */
+
+/* flags */
+#define GX_FLAG_COMPENSATED 1   /* compensated (two-float) position update  */
+
+/* grid arrays for gx_get_grid / gx_set_mass */
+#define GX_GRID_MASS        0   /* mass (after the pmass scaling)            */
+#define GX_GRID_FR          1   /* radial force (before polcat)              */
+#define GX_GRID_FT          2   /* azimuthal force (before polcat)           */
+#define GX_GRID_FZ          3   /* vertical force (3D)                       */
+#define GX_GRID_POT         4   /* potential                                 */
+#define GX_GRID_FX          5   /* Cartesian x force (after polcat)          */
+#define GX_GRID_FY          6   /* Cartesian y force (after polcat)          */
+
+/* Green-function component types, reference itype order
+ * (SRC/lib15/p3conv.f:10-12): radial, azimuthal, vertical, potential */
+#define GX_GREEN_FR         0
+#define GX_GREEN_FT         1
+#define GX_GREEN_FZ         2
+#define GX_GREEN_POT        3
+
+#define GX_MAX_SKIP        16
+
+/* Grid and run parameters: the p2d/p3d cards of the reference
+ * (SRC/lib15/p2dset.f:22-80, p3dset.f:22-101, filset.f:101-142) plus the
+ * unit scalings that setrun/loadup derive (SRC/lib15/loadup.f:97-99). */
+typedef struct GxConfig {
+    int32_t ndim;        /* 2 (p2d) or 3 (p3d)                               */
+    int32_t nr;          /* grid rings                                        */
+    int32_t na;          /* spokes (forced even)                              */
+    int32_t ngz;         /* planes (3D; must be 3^i 5^j); ignored for 2D      */
+    float   dzg;         /* plane spacing in grid units (3D)                  */
+    int32_t ng;          /* sectoral harmonics m = 0 .. ng-1 (HASH + 1)       */
+    int32_t nsect;       /* sector symmetry (1 = whole plane)                 */
+    int32_t nskip;       /* extra harmonics to skip ('skip' card)             */
+    int32_t skip[GX_MAX_SKIP];
+    int32_t rmap;        /* GX_RMAP_*                                         */
+    float   rmap_a;      /* u scale a; 0 selects the reference alpha = 2pi/na */
+    float   rmap_r0;     /* inner edge for GX_RMAP_LOG                        */
+    float   softl;       /* softening length, grid units                      */
+    int32_t tsoft;       /* GX_SOFT_*                                         */
+    float   pmass;       /* particle mass in internal units (M lscale^3 ts^2) */
+    int32_t halo;        /* 0: none; 1: rigid cored isothermal halo (ISOT)    */
+    float   halo_v2;     /* ISOT asymptotic v^2 (M_h / r_c) in internal units */
+    float   halo_rc;     /* ISOT core radius, grid units                      */
+    int32_t precision;   /* GX_PREC_*                                         */
+    int32_t flags;       /* GX_FLAG_*                                         */
+    int32_t device;      /* CUDA device ordinal                               */
+} GxConfig;
+
+/* Grid geometry derived by setgrd (SRC/lib15/setgrd.f:52-200). */
+typedef struct GxGeometry {
+    int32_t nr, na, ngz, ng, mmax, nsect, mesh;
+    float   alpha;       /* 2 pi / na                                         */
+    float   ua;          /* scale of u(r) actually used                       */
+    float   uoffs;       /* offset of GX_RMAP_LOG                             */
+    float   rinh;        /* inner edge, grofu(0)                              */
+    float   rgrid;       /* outer edge, grofu(nr - 1)                         */
+    float   zm;          /* half-height of the grid, 0.5 dzg (ngz - 1)        */
+    float   thmax;       /* na / nsect                                        */
+    int32_t nact;        /* active harmonics (lg false)                       */
+    uint8_t lg[260];     /* lg[m] != 0: harmonic m skipped (filset.f:116-141) */
+} GxGeometry;
+
+/* Global integrals of icheck (SRC/lib15/icheck.f:61-92), FP64 sums. */
+typedef struct GxDiag {
+    double ke;           /* sum m v^2 (reference keeps the 1/2 outside)      */
+    double pe;           /* 1/2 sum m phi                                     */
+    double lz;           /* sum m (x vy - y vx)                               */
+    double virial;       /* sum m x . a                                       */
+    double a2_re, a2_im; /* sum m e^{2 i phi} / sum m                         */
+    int64_t n_on_grid;
+} GxDiag;
+
+typedef struct GxCtx GxCtx;
+
+/* grdset + setgrd: validate the cards, derive the geometry, allocate the
+ * device arrays.  SRC/lib15/grdset.f:23-42, SRC/lib15/setgrd.f:52-200. */
+int gx_grdset(const GxConfig* cfg, GxCtx** out);
+
+/* Release every resource of the context. */
+void gx_destroy(GxCtx* ctx);
+
+/* Text of the last error on this context (or of the last failed
+ * gx_grdset when ctx is NULL). */
+const char* gx_last_error(const GxCtx* ctx);
+
+/* Derived geometry (setgrd results). */
+int gx_geometry(const GxCtx* ctx, GxGeometry* geo);
+
+/* greenm: build the transformed Green table on the device in FP64 and keep
+ * it resident (the reference writes it to a .grt file and re-reads it every
+ * step).  SRC/lib15/greenm.f:27-36, p2grnm.f:73-219, p3grnm.f:94-263. */
+int gx_greenm(GxCtx* ctx);
+
+/* Copy one Green component out (FP64 build rounded as stored), layout
+ * [m][kz][is][ir] for 3D and [m][is][ir] for 2D, harmonic/wavenumber ranges
+ * as documented in DESIGN.md.  type = GX_GREEN_*.  n = element count. */
+int gx_green_get(GxCtx* ctx, int type, double* out, int64_t n);
+
+/* loadup: copy n AoS particle records (2*ndim float32 words each) into the
+ * device SoA store.  SRC/lib15/loadup.f:36-140. */
+int gx_loadup(GxCtx* ctx, const float* coords, int64_t n);
+
+/* dumpp (coordinates only): copy the particle records back out, in the
+ * order they were loaded.  SRC/lib15/dumpp.f:246-387. */
+int gx_unload(GxCtx* ctx, float* coords);
+
+/* masset: clear, assign every particle's mass (massgn) and scale by pmass.
+ * SRC/lib15/masset.f, massgn.f:68-89 (p2d), 140-172 (p3d), scaled.f:89-92. */
+int gx_masset(GxCtx* ctx);
+
+/* Test-mass placement of p2ckst/p3ckst: install a mesh-sized mass array
+ * (already scaled) directly.  SRC/lib15/p3ckst.f. */
+int gx_set_mass(GxCtx* ctx, const float* mass);
+
+/* findf: solve for the fields of the current mass array (p2fndf/p3fndf)
+ * and convert to Cartesian components (polcat).  lpot != 0 also returns
+ * the potential.  SRC/lib15/findf.f:34-80, p2fndf.f:25-66, p3fndf.f:36-104,
+ * polcat.f:22-41. */
+int gx_findf(GxCtx* ctx, int lpot);
+
+/* findf without polcat (ptest stubs polcat out, SRC/progs/ptest.f:91-101). */
+int gx_findf_polar(GxCtx* ctx, int lpot);
+
+/* Copy a mesh array out.  which = GX_GRID_*.  mesh floats. */
+int gx_get_grid(GxCtx* ctx, int which, float* out);
+
+/* getacc/grdacc: accelerations (ndim per particle, AoS) and potentials of
+ * every particle at its current position from the current fields, plus the
+ * rigid halo.  pot may be NULL.  SRC/lib15/getacc.f:36-162,
+ * grdacc.f:40-84 (p2d), 189-266 (p3d). */
+int gx_getacc(GxCtx* ctx, float* acc, float* pot);
+
+/* step: nsteps x { findf; getacc; stpgrp; massgn; scaled }.  phys != 0
+ * requests potentials on the last step (analysis step).
+ * SRC/lib15/step.f:135-290, SRC/progs/galaxy.f:107-148. */
+int gx_step(GxCtx* ctx, int nsteps, int phys);
+
+/* tmcent: move velocities half a step back (start != 0) or forward using
+ * the current fields.  SRC/lib15/tmcent.f:83-90, tmcgrp.f. */
+int gx_tmcent(GxCtx* ctx, int start);
+
+/* icheck: KE, PE, Lz, virial and the m=2 amplitude, FP64 sums.
+ * SRC/lib15/icheck.f:61-92. */
+int gx_icheck(GxCtx* ctx, GxDiag* diag);
+
+/* Device time of the last gx_step (ms, CUDA events on the context stream). */
+int gx_last_step_ms(const GxCtx* ctx, float* ms);
+
+/* Number of kernels launched by the last gx_step call. */
+int gx_last_launch_count(const GxCtx* ctx, int64_t* n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GALAXY_GPU_H */

@@ -1,0 +1,71 @@
+/*
+ * gx_oracle.h -- CPU restatement of the GALAXY v15 polar-grid PM step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path:
+ * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
+ * load it.  The product path (galaxy_b200/libgalaxy_gpu.so) never links or
+ * calls it.
+ *
+ * The reference (Fortran 77, SRC/lib15) cannot be compiled in this image (no
+ * Fortran compiler), so each routine below restates the reference routine it
+ * names, in the reference's loop order, in two flavours built from one
+ * template (gx_oracle_tmpl.h):
+ *   *_f64  FP64 throughout (the accuracy oracle),
+ *   *_f32  FP32 "mirror": the reference's single-precision expressions and
+ *          operation order (keys, weights, kernels, sums).  Transforms are
+ *          direct sums with the FFTPACK conventions, not FFTPACK itself.
+ * Parity pin: tests/test_oracle_ftest.py checks the p3d point-mass field
+ * values printed in EXAMPLES/p3d/ftest/run999.lis:26-30.
+ *
+ * Layouts (shared with the CUDA library):
+ *   particle records   AoS, 2*ndim words: x, y[, z], vx, vy[, vz]
+ *   mesh arrays        [ir][iz][it]  (ncl - 1 of SRC/lib15/weight.f:236)
+ *   Green table        [type 0..3][m 0..ng-1][kz 0..nkz-1][is][ir]
+ *                      type: 0 radial, 1 azimuthal, 2 vertical, 3 potential;
+ *                      nkz = ngz + 1 (3D) or 1 (2D)
+ *   direct table       [type][is][ir][jz 0..nkz-1][k 0..na/2]
+ */
+#ifndef GX_ORACLE_H
+#define GX_ORACLE_H
+#include <stdint.h>
+#include "../include/galaxy_gpu.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+int ox_geometry(const GxConfig* cfg, GxGeometry* geo, char* err, int errlen);
+int64_t ox_green_size(const GxConfig* cfg);
+int64_t ox_direct_size(const GxConfig* cfg);
+
+#define OX_DECL(R, S)                                                          \
+int ox_green_##S(const GxConfig* cfg, R* G, R* D);                             \
+int ox_weight_##S(const GxConfig* cfg, int old, int64_t n, const R* pos,       \
+                  int32_t* key, R* wt, uint8_t* on);                           \
+int ox_massgn_##S(const GxConfig* cfg, int64_t n, const int32_t* key,          \
+                  const R* wt, const uint8_t* on, R* mass, int32_t* jrk);      \
+int ox_findf_##S(const GxConfig* cfg, const R* G, const R* mass, int lpot,     \
+                 int jrs, int krs, R* fields);                                 \
+int ox_polcat_##S(const GxConfig* cfg, R* fields);                             \
+int ox_grdacc_##S(const GxConfig* cfg, int64_t n, const R* pos,                \
+                  const R* fields, int phys, R* acc, R* pot);                  \
+int ox_masset_##S(const GxConfig* cfg, int64_t n, const R* pos, R* mass,       \
+                  int32_t* jrk);                                               \
+int ox_step_##S(const GxConfig* cfg, const R* G, int64_t n, R* pos, R* mass,   \
+                int32_t* jrk, int nsteps, int phys, R* fields);                \
+int ox_direct_field_##S(const GxConfig* cfg, const R* D, int nmass,            \
+                        const int32_t* mr, const int32_t* mt,                  \
+                        const int32_t* mz, const R* mm, int lpot, R* fields);
+
+OX_DECL(double, f64)
+OX_DECL(float, f32)
+
+/* icheck-style integrals in FP64 from FP64 particle records and potentials */
+int ox_icheck(const GxConfig* cfg, int64_t n, const double* pos,
+              const double* acc, const double* pot, double pmass_phys,
+              GxDiag* d);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

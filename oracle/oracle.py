@@ -1,0 +1,193 @@
+"""ctypes driver of the CPU oracle (oracle/liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, as the checker.  The product path
+(galaxy_b200) never imports this module.
+
+Every function wraps one restated reference routine; see gx_oracle.h for
+the layouts and gx_oracle_tmpl.h for the file:line of each restatement.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from galaxy_b200._abi import GxConfig, GxGeometry, GxDiag
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = os.path.join(_HERE, "liboracle.so")
+_lib = None
+
+
+def build():
+    """Compile liboracle.so with the committed Makefile."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB):
+            build()
+        _lib = C.CDLL(_LIB)
+        _setup(_lib)
+    return _lib
+
+
+def _setup(L):
+    P = C.c_void_p
+    i64 = C.c_int64
+    L.ox_geometry.argtypes = [C.POINTER(GxConfig), C.POINTER(GxGeometry), C.c_char_p, C.c_int]
+    L.ox_green_size.argtypes = [C.POINTER(GxConfig)]
+    L.ox_green_size.restype = i64
+    L.ox_direct_size.argtypes = [C.POINTER(GxConfig)]
+    L.ox_direct_size.restype = i64
+    for s in ("f64", "f32"):
+        getattr(L, "ox_green_" + s).argtypes = [C.POINTER(GxConfig), P, P]
+        getattr(L, "ox_weight_" + s).argtypes = [C.POINTER(GxConfig), C.c_int, i64, P, P, P, P]
+        getattr(L, "ox_massgn_" + s).argtypes = [C.POINTER(GxConfig), i64, P, P, P, P, P]
+        getattr(L, "ox_findf_" + s).argtypes = [C.POINTER(GxConfig), P, P, C.c_int, C.c_int,
+                                                C.c_int, P]
+        getattr(L, "ox_polcat_" + s).argtypes = [C.POINTER(GxConfig), P]
+        getattr(L, "ox_grdacc_" + s).argtypes = [C.POINTER(GxConfig), i64, P, P, C.c_int, P, P]
+        getattr(L, "ox_masset_" + s).argtypes = [C.POINTER(GxConfig), i64, P, P, P]
+        getattr(L, "ox_step_" + s).argtypes = [C.POINTER(GxConfig), P, i64, P, P, P, C.c_int,
+                                               C.c_int, P]
+        getattr(L, "ox_direct_field_" + s).argtypes = [C.POINTER(GxConfig), P, C.c_int, P, P,
+                                                       P, P, C.c_int, P]
+    L.ox_icheck.argtypes = [C.POINTER(GxConfig), i64, P, P, P, C.c_double, C.POINTER(GxDiag)]
+
+
+def _p(a):
+    return a.ctypes.data_as(C.c_void_p) if a is not None else None
+
+
+def _dt(prec):
+    return (np.float64, "f64") if prec == 64 else (np.float32, "f32")
+
+
+def _chk(rc, what):
+    if rc != 0:
+        raise RuntimeError(f"oracle {what} failed with {rc}")
+
+
+def geometry(cfg):
+    g = GxGeometry()
+    err = C.create_string_buffer(256)
+    rc = lib().ox_geometry(C.byref(cfg), C.byref(g), err, 256)
+    if rc != 0:
+        raise ValueError(err.value.decode())
+    return g
+
+
+def nkz(cfg):
+    return cfg.ngz + 1 if cfg.ndim == 3 else 1
+
+
+def green(cfg, prec=64, direct=False):
+    """Transformed Green table [4][ng][nkz][is][ir] (and the direct one)."""
+    dt, s = _dt(prec)
+    g = geometry(cfg)
+    G = np.zeros(lib().ox_green_size(C.byref(cfg)), dtype=dt)
+    D = np.zeros(lib().ox_direct_size(C.byref(cfg)), dtype=dt) if direct else None
+    _chk(getattr(lib(), "ox_green_" + s)(C.byref(cfg), _p(G), _p(D)), "green")
+    G = G.reshape(4, g.ng, nkz(cfg), g.nr, g.nr)
+    if direct:
+        D = D.reshape(4, g.nr, g.nr, nkz(cfg), g.na // 2 + 1)
+        return G, D
+    return G
+
+
+def weight(cfg, pos, old=False, prec=64):
+    dt, s = _dt(prec)
+    pos = np.ascontiguousarray(pos, dtype=dt)
+    n = pos.shape[0]
+    key = np.zeros(n, np.int32)
+    wt = np.zeros((n, 8), dt)
+    on = np.zeros(n, np.uint8)
+    _chk(getattr(lib(), "ox_weight_" + s)(C.byref(cfg), int(old), n, _p(pos), _p(key), _p(wt),
+                                           _p(on)), "weight")
+    return key, wt, on
+
+
+def masset(cfg, pos, prec=64):
+    """Scaled mass array and 1-based active ring range (jrad, krad)."""
+    dt, s = _dt(prec)
+    pos = np.ascontiguousarray(pos, dtype=dt)
+    g = geometry(cfg)
+    mass = np.zeros(g.mesh, dt)
+    jrk = np.zeros(2, np.int32)
+    _chk(getattr(lib(), "ox_masset_" + s)(C.byref(cfg), pos.shape[0], _p(pos), _p(mass),
+                                           _p(jrk)), "masset")
+    return mass, (int(jrk[0]), int(jrk[1]))
+
+
+def findf(cfg, G, mass, lpot=True, jrk=None, prec=64, polar=True):
+    """Fields [4][mesh] (radial, azimuthal, vertical, potential) or, with
+    polar=False, Cartesian (fx, fy, fz, potential) after polcat."""
+    dt, s = _dt(prec)
+    g = geometry(cfg)
+    G = np.ascontiguousarray(G, dtype=dt)
+    mass = np.ascontiguousarray(mass, dtype=dt)
+    if jrk is None:
+        jrk = (1, g.nr)
+    f = np.zeros((4, g.mesh), dt)
+    _chk(getattr(lib(), "ox_findf_" + s)(C.byref(cfg), _p(G), _p(mass), int(lpot), jrk[0],
+                                          jrk[1], _p(f)), "findf")
+    if not polar:
+        _chk(getattr(lib(), "ox_polcat_" + s)(C.byref(cfg), _p(f)), "polcat")
+    return f
+
+
+def grdacc(cfg, pos, fields, phys=True, prec=64):
+    dt, s = _dt(prec)
+    pos = np.ascontiguousarray(pos, dtype=dt)
+    fields = np.ascontiguousarray(fields, dtype=dt)
+    n = pos.shape[0]
+    acc = np.zeros((n, cfg.ndim), dt)
+    pot = np.zeros(n, dt)
+    _chk(getattr(lib(), "ox_grdacc_" + s)(C.byref(cfg), n, _p(pos), _p(fields), int(phys),
+                                           _p(acc), _p(pot)), "grdacc")
+    return acc, pot
+
+
+def step(cfg, G, pos, nsteps, phys=False, prec=64):
+    """Advance AoS particle records nsteps (masset first).  Returns
+    (pos, mass, fields-of-last-solve)."""
+    dt, s = _dt(prec)
+    pos = np.array(pos, dtype=dt, copy=True, order="C")
+    G = np.ascontiguousarray(G, dtype=dt)
+    g = geometry(cfg)
+    mass, jrk = masset(cfg, pos, prec)
+    jrk = np.array(jrk, np.int32)
+    f = np.zeros((4, g.mesh), dt)
+    _chk(getattr(lib(), "ox_step_" + s)(C.byref(cfg), _p(G), pos.shape[0], _p(pos), _p(mass),
+                                         _p(jrk), nsteps, int(phys), _p(f)), "step")
+    return pos, mass, f
+
+
+def direct_field(cfg, D, masses, lpot=True, prec=64):
+    """Direct convolution for point masses [(ring, spoke, plane, m)], 1-based."""
+    dt, s = _dt(prec)
+    g = geometry(cfg)
+    D = np.ascontiguousarray(D, dtype=dt)
+    mr = np.array([m[0] for m in masses], np.int32)
+    mt = np.array([m[1] for m in masses], np.int32)
+    mz = np.array([m[2] for m in masses], np.int32)
+    mm = np.array([m[3] for m in masses], dt)
+    f = np.zeros((4, g.mesh), dt)
+    _chk(getattr(lib(), "ox_direct_field_" + s)(C.byref(cfg), _p(D), len(masses), _p(mr),
+                                                 _p(mt), _p(mz), _p(mm), int(lpot), _p(f)),
+         "direct_field")
+    return f
+
+
+def icheck(cfg, pos, acc=None, pot=None, pmass=1.0):
+    pos = np.ascontiguousarray(pos, np.float64)
+    acc = None if acc is None else np.ascontiguousarray(acc, np.float64)
+    pot = None if pot is None else np.ascontiguousarray(pot, np.float64)
+    d = GxDiag()
+    _chk(lib().ox_icheck(C.byref(cfg), pos.shape[0], _p(pos), _p(acc), _p(pot), pmass,
+                         C.byref(d)), "icheck")
+    return d
