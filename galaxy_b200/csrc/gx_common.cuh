@@ -1,0 +1,298 @@
+// gx_common.cuh -- shared device/host definitions of the B200 polar-grid
+// particle-mesh library (context, geometry constants, cell-key arithmetic).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/galaxy_gpu.h"
+
+#define GX_PI 3.141592653589793238462643
+
+// ---------------------------------------------------------------------------
+// Phases of a step timed in profile mode
+#define GX_NPHASE 8
+enum { PH_FWD = 0, PH_CONV, PH_SYN, PH_PUSH, PH_SORT, PH_DEPOSIT, PH_COMBINE, PH_OTHER };
+
+// Geometry constants passed by value to kernels.
+struct DevGeo {
+    int ndim, nr, na, ngz, nkz, ng, mmax, nsect, mesh, nrow;  // nrow = nr*ngz
+    int rmap, tsoft, halo;
+    float alpha, ua, inv_ua, uoffs, rinh, rgrid, zm, thmax, dzg, inv_dzg;
+    float t_scale;  // na / (2 pi) in FP32
+    float halo_v2, halo_rc2;
+    float pmass;
+    // FP64 copies for the plain FP64 path
+    double ua_d, uoffs_d, rinh_d, rgrid_d, zm_d, thmax_d, dzg_d, halo_v2_d, halo_rc2_d;
+};
+
+// Spectral bookkeeping: active harmonics (lg false, m < ng).
+struct Spec {
+    int nact;        // number of active harmonics
+    int m[260];      // their m values, ascending
+};
+
+// Deposit scratch sizes
+struct SortBufs {
+    uint32_t* keys[2];
+    int32_t* vals[2];
+    uint32_t* hist;     // [nbucket][ntile]
+    uint32_t* dtotal;   // [nbucket]
+    int tile;           // items per tile
+    int ntile;
+    int bits;           // bits sorted (row digits)
+    int npass;
+    int pass_bits[4];
+    int pass_shift[4];
+};
+
+struct GxCtx {
+    GxConfig cfg;
+    GxGeometry geo;
+    DevGeo g;
+    Spec spec;
+    std::string err;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+    int64_t launches = 0;
+    bool fp64 = false;
+
+    // Green table (device): [4][ng][nkz][is][ir]
+    float* green32 = nullptr;
+    double* green64 = nullptr;
+    bool have_green = false;
+
+    // particles
+    int64_t n = 0;
+    int64_t cap = 0;
+    float* pbuf[2] = {nullptr, nullptr};   // SoA [2*ndim][cap] (mixed path)
+    int cur = 0;
+    int32_t* perm = nullptr;               // processing order of pbuf[cur]
+    int32_t* origin = nullptr;             // original load index of pbuf[cur][i]
+    int32_t* origin_tmp = nullptr;
+    uint32_t* pkey = nullptr;              // per-particle keys from the last pass
+    double* p64 = nullptr;                 // SoA [2*ndim][cap] (FP64 path)
+    int32_t* key64 = nullptr;
+    double* w64 = nullptr;                 // [8][cap]
+    double* acc64 = nullptr;               // [3][cap]
+    float* ppot = nullptr;                 // per-particle potential (analysis)
+    float* pacc = nullptr;                 // per-particle acceleration (getacc)
+
+    // grids
+    float* mass = nullptr;                 // [mesh] scaled mass (mixed)
+    double* mass64 = nullptr;              // [mesh] (FP64 path)
+    float4* field = nullptr;               // [mesh] (fx, fy, fz, pot) mixed
+    float* polar = nullptr;                // [4][mesh] polar fields (fr, ft, fz, pot)
+    double* field64 = nullptr;             // [4][mesh] (FP64 path: fx, fy, fz, pot)
+    double* polar64 = nullptr;             // [4][mesh]
+    float4* specS = nullptr;               // forward spectrum [nact][nkz][nr]
+    float4* specO = nullptr;               // convolved [4][nact][nkz][nr]
+    double* spec64 = nullptr;
+    double* out64 = nullptr;
+    bool have_mass = false;
+    bool have_field = false;
+    bool field_pot = false;
+    int jrs = 1, krs = 0;                  // active source ring range (1-based)
+
+    // deposit
+    SortBufs sb{};
+    int32_t* rowstart = nullptr;           // [nrow + 1]
+    int32_t* items = nullptr;              // work items [maxitems][3]: row, start, end
+    int32_t* nitems_d = nullptr;
+    int32_t* rowitem = nullptr;            // [nrow + 1] first work item of each row
+    float* stage = nullptr;                // [maxitems][NQ][na]
+    int maxitems = 0;
+    int32_t* jrk_d = nullptr;              // device min/max ring
+    int32_t* errword = nullptr;            // device error word
+
+    // diagnostics scratch
+    double* dsum = nullptr;
+
+    // phase timing (gx_set_profile): events around the phases of a step
+    bool prof = false;
+    cudaEvent_t pev[GX_NPHASE + 1] = {};
+    float phase_ms[GX_NPHASE] = {};
+    int64_t phase_n[GX_NPHASE] = {};
+    int open_phase = -1;
+};
+
+// record the start of phase ph (prof mode) and close the previous one
+int gx_phase_mark(GxCtx* c, int ph);
+int gx_phase_end(GxCtx* c);
+
+// ---------------------------------------------------------------------------
+// error helpers (host)
+#define GX_CUDA(ctx, call)                                                  \
+    do {                                                                    \
+        cudaError_t e_ = (call);                                            \
+        if (e_ != cudaSuccess) {                                            \
+            (ctx)->err = std::string(#call) + ": " + cudaGetErrorString(e_);\
+            return GX_ERR_CUDA;                                             \
+        }                                                                   \
+    } while (0)
+
+#define GX_LAUNCHED(ctx)                                                    \
+    do {                                                                    \
+        (ctx)->launches++;                                                  \
+        cudaError_t e_ = cudaGetLastError();                                \
+        if (e_ != cudaSuccess) {                                            \
+            (ctx)->err = std::string("launch: ") + cudaGetErrorString(e_);  \
+            return GX_ERR_CUDA;                                             \
+        }                                                                   \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// cell-key arithmetic (device).  The reference (SRC/lib15/weight.f:61-101,
+// 196-250) forms r = sqrt(x*x + y*y) in FP32, u = uofgr(r) in FP32, the
+// spoke coordinate t from an FP64 atan2 rounded to FP32, z = (z + zm)/dzg in
+// FP32, and truncates.  The fast path below evaluates u and t with FP32
+// library functions; when either lies within a guard band of an integer
+// boundary it is recomputed with the reference's exact operation sequence
+// (correctly rounded log, FP64 atan2), so the integer cell indices agree
+// with the reference's wherever its own libm calls are correctly rounded.
+
+struct CellW {
+    int key;      // ncl - 1, or -1 when off the grid / in the hole
+    float du, dt, dz;
+};
+
+__device__ __forceinline__ float gx_u_exact(const DevGeo& g, float rr) {
+    if (g.rmap == GX_RMAP_STDPOL) {
+        float v = __fadd_rn(1.0f, rr);
+        float lf = (float)log((double)v);
+        return __fdiv_rn(lf, g.ua);
+    }
+    float lf = (float)log((double)rr);
+    return __fadd_rn(__fdiv_rn(lf, g.ua), g.uoffs);
+}
+
+__device__ __forceinline__ float gx_t_exact(const DevGeo& g, float x, float y) {
+    double t = atan2((double)y, (double)x) * (double)g.na / (2.0 * GX_PI);
+    float tf = (float)t;
+    if (tf < 0.f) tf = __fadd_rn(tf, (float)g.na);
+    return tf;
+}
+
+__device__ __forceinline__ bool gx_near_int(float v, float eps) {
+    float f = v - floorf(v);
+    return (f < eps) || (f > 1.f - eps);
+}
+
+// Cell of a particle; old != 0 for interpolation (no sector folding).
+__device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, float z, bool old) {
+    CellW c;
+    c.key = -1;
+    c.du = c.dt = c.dz = 0.f;
+    float rr = __fsqrt_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)));
+    if (rr > g.rgrid) return c;
+    if (g.ndim == 3 && fabsf(z) > g.zm) return c;
+    if (rr < g.rinh) return c;
+    // u (fast path + guard)
+    float u;
+    if (g.rmap == GX_RMAP_STDPOL) u = __logf(1.0f + rr) * g.inv_ua;
+    else u = __logf(rr) * g.inv_ua + g.uoffs;
+    {
+        // __logf: 2^-21.41 absolute error on [0.5, 2], 3 ulp elsewhere
+        float eps = 5.0e-7f * g.inv_ua + 2.0e-6f * (fabsf(u) + fabsf(g.uoffs) + 1.0f);
+        if (gx_near_int(u, eps) || u < eps) u = gx_u_exact(g, rr);
+    }
+    // t
+    float t;
+    if (g.ndim == 2 || rr > 0.f) {
+        t = atan2f(y, x) * g.t_scale;
+        if (t < 0.f) t += (float)g.na;
+        float eps = 4.0e-6f * (float)(g.na + 1);
+        if (gx_near_int(t, eps) || t < eps || t > (float)g.na - eps) t = gx_t_exact(g, x, y);
+    } else {
+        t = 0.f;
+    }
+    if (!old && g.nsect > 1) t = fmodf(t, g.thmax);
+    int ju = (int)u;
+    if (ju > g.nr - 2) ju = g.nr - 2;
+    int jt = (int)t;
+    c.du = u - (float)ju;
+    c.dt = t - (float)jt;
+    if (g.ndim == 2) {
+        c.key = ju * g.na + jt;
+    } else {
+        float zz = (z + g.zm) * g.inv_dzg;
+        {
+            float eps = 4.0e-6f * ((float)g.ngz + 1.f);
+            if (gx_near_int(zz, eps)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
+        }
+        int jz = (int)zz;
+        if (jz < 0) jz = 0;
+        if (jz > g.ngz - 2) jz = g.ngz - 2;
+        c.dz = zz - (float)jz;
+        c.key = (ju * g.ngz + jz) * g.na + jt;
+    }
+    return c;
+}
+
+// 8 (3D) or 4 (2D) weights in the reference order (weight.f:92-99, 241-248)
+__device__ __forceinline__ void gx_weights(const DevGeo& g, const CellW& c, float* w) {
+    if (g.ndim == 2) {
+        float dd = c.du * c.dt;
+        w[0] = 1.f - c.du - c.dt + dd;
+        w[1] = c.dt - dd;
+        w[2] = c.du - dd;
+        w[3] = dd;
+    } else {
+        float a0 = (1.f - c.dt) * (1.f - c.dz), a1 = c.dt * (1.f - c.dz);
+        float a2 = (1.f - c.dt) * c.dz, a3 = c.dt * c.dz;
+        float bu = 1.f - c.du;
+        w[0] = a0 * bu;
+        w[1] = a1 * bu;
+        w[2] = a2 * bu;
+        w[3] = a3 * bu;
+        w[4] = a0 * c.du;
+        w[5] = a1 * c.du;
+        w[6] = a2 * c.du;
+        w[7] = a3 * c.du;
+    }
+}
+
+// corner cells of a key (grdacc.f:193-202); -1 for cells past the mesh end
+__device__ __forceinline__ int gx_corners(const DevGeo& g, int key, int* ic) {
+    const int na = g.na;
+    int end = ((key + 1) % na) == 0;
+    ic[0] = key;
+    ic[1] = key + 1 - (end ? na : 0);
+    ic[2] = key + na;
+    ic[3] = ic[1] + na;
+    if (g.ndim == 2) {
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (ic[k] >= g.mesh) ic[k] = -1;
+        return 4;
+    }
+    const int pl = g.ngz * na;
+    ic[4] = key + pl;
+    ic[5] = ic[1] + pl;
+    ic[6] = ic[4] + na;
+    ic[7] = ic[5] + na;
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+        if (ic[k] >= g.mesh) ic[k] = -1;
+    return 8;
+}
+
+// ---------------------------------------------------------------------------
+// host-side entry points implemented in the .cu files
+int gx_green_build_dev(GxCtx* c);
+int gx_mixed_masset(GxCtx* c);
+int gx_mixed_findf(GxCtx* c, int lpot, bool polcat);
+int gx_mixed_getacc(GxCtx* c, float* acc, float* pot);
+int gx_mixed_step(GxCtx* c, int nsteps, int phys);
+int gx_mixed_sort_deposit(GxCtx* c);
+int gx_mixed_keys_initial(GxCtx* c);
+int gx_fp64_masset(GxCtx* c);
+int gx_fp64_findf(GxCtx* c, int lpot, bool polcat);
+int gx_fp64_getacc(GxCtx* c, float* acc, float* pot);
+int gx_fp64_step(GxCtx* c, int nsteps, int phys);
+int gx_mass_dense_from_stage(GxCtx* c);

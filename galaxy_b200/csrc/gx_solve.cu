@@ -1,0 +1,593 @@
+// gx_solve.cu -- field solve of the mixed-precision path (findf).
+//
+//   k_fwd3 / k_fwd2   p3manl.f:62-109 / p2manl.f:32-45: per ring, the
+//                     azimuthal real DFT of every plane restricted to the
+//                     active harmonics (the m = 0 term summed in FP64), then
+//                     (3D) the zero-padded length-2 ngz vertical DFT.  Both
+//                     are small GEMMs against twiddle matrices held in
+//                     shared memory; only the active harmonics are formed.
+//   k_conv            p3conv.f:137-230 / p2conv.f:114-181: for every
+//                     (harmonic, vertical wavenumber) the dense radial
+//                     contraction with the FP32 Green table of each field
+//                     type, the Green matrix streamed from HBM once per step.
+//   k_syn3 / k_syn2   p3fsyn.f:59-129 / p2fsyn.f:34-56 fused with polcat
+//                     (polcat.f:22-41): inverse vertical DFT, inverse
+//                     azimuthal DFT with the 1/(2 ngz na) (1/na) scale, then
+//                     the rotation to Cartesian components, written as one
+//                     float4 (fx, fy, fz, phi) per mesh node.
+// FFTPACK conventions (SRC/utils/sfftpack): forward a_m = sum x cos,
+// b_m = -sum x sin; backward x_j = a_0 + (-1)^j a_N + 2 sum (a cos - b sin).
+#include <algorithm>
+
+#include "gx_common.cuh"
+
+__constant__ int c_act_m[260];
+
+__host__ __device__ static inline int ru4(int x) { return (x + 3) & ~3; }
+
+// C[M][N] = A[M][K] * B[K][N] in shared memory, 4x4 register tiles.
+// A rows are read up to ru4(M) (must be addressable), B is read as float4
+// rows (ldb % 4 == 0, columns up to ru4(N) addressable).  epi(r0, c0, acc)
+// receives each tile.
+template <class Epi>
+__device__ __forceinline__ void sgemm44(int M, int N, int K, const float* A, int lda,
+                                        const float* B, int ldb, Epi epi) {
+    const int tilesN = (N + 3) >> 2, tilesM = (M + 3) >> 2, nt = tilesM * tilesN;
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        const int tm = t / tilesN, tn = t - tm * tilesN;
+        const int r0 = tm * 4, c0 = tn * 4;
+        float acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+        const float* ap = A + (size_t)r0 * lda;
+        const float* bp = B + c0;
+#pragma unroll 4
+        for (int k = 0; k < K; k++) {
+            const float4 b = *reinterpret_cast<const float4*>(bp + (size_t)k * ldb);
+            const float a0 = ap[k], a1 = ap[lda + k], a2 = ap[2 * lda + k], a3 = ap[3 * lda + k];
+            acc[0][0] += a0 * b.x; acc[0][1] += a0 * b.y; acc[0][2] += a0 * b.z; acc[0][3] += a0 * b.w;
+            acc[1][0] += a1 * b.x; acc[1][1] += a1 * b.y; acc[1][2] += a1 * b.z; acc[1][3] += a1 * b.w;
+            acc[2][0] += a2 * b.x; acc[2][1] += a2 * b.y; acc[2][2] += a2 * b.z; acc[2][3] += a2 * b.w;
+            acc[3][0] += a3 * b.x; acc[3][1] += a3 * b.y; acc[3][2] += a3 * b.z; acc[3][3] += a3 * b.w;
+        }
+        epi(r0, c0, acc);
+    }
+}
+
+// forward azimuthal twiddles T[j][2a] = cos(2 pi m_a j / na), T[j][2a+1] = -sin(...)
+__device__ void build_taz(float* T, int na, int nact, int ncp) {
+    for (int i = threadIdx.x; i < na * ncp; i += blockDim.x) {
+        int j = i / ncp, c = i - j * ncp;
+        float v = 0.f;
+        if (c < 2 * nact) {
+            int m = c_act_m[c >> 1];
+            int idx = (int)(((int64_t)m * j) % na);
+            float s, co;
+            sincospif(2.0f * (float)idx / (float)na, &s, &co);
+            v = (c & 1) ? -s : co;
+        }
+        T[i] = v;
+    }
+}
+
+// inverse azimuthal twiddles with the synthesis scale: Ti[c][j]
+__device__ void build_tazi(float* Ti, int na, int nact, int ncp, int mmax, float scale) {
+    for (int i = threadIdx.x; i < ncp * na; i += blockDim.x) {
+        int c = i / na, j = i - c * na;
+        float v = 0.f;
+        if (c < 2 * nact) {
+            int m = c_act_m[c >> 1];
+            int idx = (int)(((int64_t)m * j) % na);
+            float s, co;
+            sincospif(2.0f * (float)idx / (float)na, &s, &co);
+            if (m == 0) v = (c & 1) ? 0.f : 1.f;
+            else if (m == mmax - 1) v = (c & 1) ? 0.f : ((j & 1) ? -1.f : 1.f);
+            else v = (c & 1) ? -2.f * s : 2.f * co;
+            v *= scale;
+        }
+        Ti[i] = v;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// 3D forward transform, one CTA per active source ring.
+__global__ void k_fwd3(DevGeo g, int nact, int ncp, const int32_t* __restrict__ jrk,
+                       const float* __restrict__ mass, float4* __restrict__ S) {
+    extern __shared__ __align__(16) float sm[];
+    const int na = g.na, ngz = g.ngz, nkz = g.nkz, nr = g.nr;
+    const int ir = blockIdx.x;
+    // only the rings that hold mass are transformed (p3fndf.f:44-57)
+    if (ir < jrk[0] - 1 || ir > min(jrk[1], nr) - 1) return;
+    const int ldx = na + 1;
+    const int r0sz = max(ru4(ngz) * ldx, ru4(2 * nkz) * ngz);
+    float* X = sm;                       // [ru4(ngz)][na + 1], later Tz [ru4(2 nkz)][ngz]
+    float* T = X + r0sz;                 // [na][ncp]
+    float* C1 = T + na * ncp;            // [ru4(ngz)][ncp]
+    const float* src = mass + (size_t)ir * ngz * na;
+    for (int i = threadIdx.x; i < ngz * na; i += blockDim.x) {
+        int z = i / na, j = i - z * na;
+        X[z * ldx + j] = src[i];
+    }
+    for (int i = ngz * ldx + threadIdx.x; i < ru4(ngz) * ldx; i += blockDim.x) X[i] = 0.f;
+    build_taz(T, na, nact, ncp);
+    __syncthreads();
+    sgemm44(ngz, ncp, na, X, ldx, T, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) C1[(r0 + i) * ncp + c0 + j] = acc[i][j];
+    });
+    __syncthreads();
+    // m = 0 (when active) in FP64
+    if (c_act_m[0] == 0) {
+        for (int z = threadIdx.x; z < ngz; z += blockDim.x) {
+            double s = 0.0;
+            for (int j = 0; j < na; j++) s += (double)X[z * ldx + j];
+            C1[z * ncp] = (float)s;
+        }
+    }
+    __syncthreads();
+    // vertical twiddles Tz[2k][z] = cos(pi k z / ngz), Tz[2k+1][z] = -sin(...)
+    float* Tz = X;
+    for (int i = threadIdx.x; i < ru4(2 * nkz) * ngz; i += blockDim.x) {
+        int r = i / ngz, z = i - r * ngz;
+        int k = r >> 1;
+        float v = 0.f;
+        if (k < nkz) {
+            int idx = (int)(((int64_t)k * z) % (2 * ngz));
+            float s, co;
+            sincospif((float)idx / (float)ngz, &s, &co);
+            v = (r & 1) ? -s : co;
+        }
+        Tz[i] = v;
+    }
+    __syncthreads();
+    sgemm44(2 * nkz, ncp, ngz, Tz, ngz, C1, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
+        // rows r0 = 2k, 2k+1, 2k+2, 2k+3; cols c0 = 2a, 2a+1, 2a+2, 2a+3
+#pragma unroll
+        for (int dk = 0; dk < 2; dk++) {
+            int k = (r0 >> 1) + dk;
+            if (k >= nkz) continue;
+#pragma unroll
+            for (int da = 0; da < 2; da++) {
+                int a = (c0 >> 1) + da;
+                if (a >= nact) continue;
+                float4 v = make_float4(acc[2 * dk][2 * da], acc[2 * dk + 1][2 * da],
+                                       acc[2 * dk][2 * da + 1], acc[2 * dk + 1][2 * da + 1]);
+                S[((size_t)a * nkz + k) * nr + ir] = v;
+            }
+        }
+    });
+}
+
+// 2D forward transform, RB rings per CTA.
+#define RB2 16
+__global__ void k_fwd2(DevGeo g, int nact, int ncp, const float* __restrict__ mass,
+                       float4* __restrict__ S) {
+    extern __shared__ __align__(16) float sm[];
+    const int na = g.na, nr = g.nr;
+    const int ldx = na + 1;
+    const int jr1 = nr - 1;
+    const int ir0 = blockIdx.x * RB2;
+    float* X = sm;                   // [RB2][na + 1]
+    float* T = X + RB2 * ldx;        // [na][ncp]
+    for (int i = threadIdx.x; i < RB2 * na; i += blockDim.x) {
+        int r = i / na, j = i - r * na;
+        int ir = ir0 + r;
+        X[r * ldx + j] = (ir <= jr1) ? mass[(size_t)ir * na + j] : 0.f;
+    }
+    build_taz(T, na, nact, ncp);
+    __syncthreads();
+    sgemm44(RB2, ncp, na, X, ldx, T, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            int ir = ir0 + r0 + i;
+            if (ir > jr1) continue;
+            double s0 = 0.0;
+            bool m0 = (c0 == 0) && (c_act_m[0] == 0);
+            if (m0)
+                for (int j = 0; j < na; j++) s0 += (double)X[(r0 + i) * ldx + j];
+#pragma unroll
+            for (int da = 0; da < 2; da++) {
+                int a = (c0 >> 1) + da;
+                if (a >= nact) continue;
+                float av = (m0 && da == 0) ? (float)s0 : acc[i][2 * da];
+                S[(size_t)a * nr + ir] = make_float4(av, 0.f, acc[i][2 * da + 1], 0.f);
+            }
+        }
+    });
+}
+
+// ---------------------------------------------------------------------------
+// radial contraction; grid (nact, nkz); 8 warps split the source rings.
+// Types: 0 radial, 1 azimuthal, 2 vertical, 3 potential (p3conv.f:173-226).
+template <bool VEC>
+__global__ void __launch_bounds__(256) k_conv(DevGeo g, int nact, int tmask,
+                                              const float* __restrict__ G,
+                                              const float4* __restrict__ S,
+                                              float4* __restrict__ O,
+                                              const int32_t* __restrict__ jrk) {
+    extern __shared__ __align__(16) float4 sh4[];
+    const int nr = g.nr, nkz = g.nkz, ng = g.ng, mmax = g.mmax, ngz = g.ngz;
+    // source rings jrs..krs (p3conv.f:149-150)
+    const int js = max(jrk[0], 1) - 1, ks = min(jrk[1], nr) - 1;
+    const int a = blockIdx.x, k = blockIdx.y, m = c_act_m[a];
+    float4* Sin = sh4;              // [nr]
+    float4* part = sh4 + nr;        // [8][nr]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int i = threadIdx.x; i < nr; i += blockDim.x)
+        Sin[i] = (i >= js && i <= ks) ? S[((size_t)a * nkz + k) * nr + i] : make_float4(0, 0, 0, 0);
+    __syncthreads();
+    for (int t = 0; t < 4; t++) {
+        if (!((tmask >> t) & 1)) continue;
+        bool valid = true;
+        if (t == 1) valid = (m >= 1) && (m <= min(ng, mmax - 1) - 1);
+        if (t == 2) valid = (g.ndim == 3) && (k >= 1) && (k <= ngz - 1);
+        float4* out = O + (((size_t)t * nact + a) * nkz + k) * nr;
+        if (!valid) {
+            for (int i = threadIdx.x; i < nr; i += blockDim.x) out[i] = make_float4(0, 0, 0, 0);
+            continue;
+        }
+        const float* Gt = G + ((((size_t)t * ng + m) * nkz + k) * nr) * (size_t)nr;
+        for (int ib = 0; ib < nr; ib += 128) {
+            const int ir0 = ib + lane * 4;
+            float4 acc[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) acc[q] = make_float4(0, 0, 0, 0);
+            if (ir0 < nr) {
+#pragma unroll 4
+                for (int is = js + warp; is <= ks; is += 8) {
+                    float gv[4];
+                    const float* gp = Gt + (size_t)is * nr + ir0;
+                    if (VEC) {
+                        float4 g4 = __ldg(reinterpret_cast<const float4*>(gp));
+                        gv[0] = g4.x; gv[1] = g4.y; gv[2] = g4.z; gv[3] = g4.w;
+                    } else {
+#pragma unroll
+                        for (int q = 0; q < 4; q++) gv[q] = (ir0 + q < nr) ? __ldg(gp + q) : 0.f;
+                    }
+                    const float4 s = Sin[is];
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float gq = gv[q];
+                        if (t == 0 || t == 3) {
+                            acc[q].x += gq * s.x; acc[q].y += gq * s.y;
+                            acc[q].z += gq * s.z; acc[q].w += gq * s.w;
+                        } else if (t == 1) {
+                            acc[q].x += gq * s.z; acc[q].z -= gq * s.x;
+                            acc[q].y += gq * s.w; acc[q].w -= gq * s.y;
+                        } else {
+                            acc[q].x += gq * s.y; acc[q].y -= gq * s.x;
+                            acc[q].z += gq * s.w; acc[q].w -= gq * s.z;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                    if (ir0 + q < nr) part[warp * nr + ir0 + q] = acc[q];
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < nr; i += blockDim.x) {
+            float4 s = part[i];
+            for (int w = 1; w < 8; w++) {
+                float4 p = part[w * nr + i];
+                s.x += p.x; s.y += p.y; s.z += p.z; s.w += p.w;
+            }
+            out[i] = s;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// synthesis epilogue shared by 2D and 3D: F_t[row][j] = sum_c R_t[row][c] Ti[c][j]
+// for the 4 types at once, then polcat, one float4 store per node.
+__device__ __forceinline__ void syn_final(const DevGeo& g, int ncp, int nrows, const float* R,
+                                          int ldr_t, const float* Ti, float4* __restrict__ dst,
+                                          size_t row_stride, float* __restrict__ polar,
+                                          size_t polar_off, size_t mesh, int tmask) {
+    const int na = g.na;
+    const int nj4 = na >> 2;
+    for (int t = threadIdx.x; t < nrows * nj4; t += blockDim.x) {
+        const int row = t / nj4, j0 = (t - row * nj4) * 4;
+        float acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
+        for (int c = 0; c < ncp; c++) {
+            const float4 w = *reinterpret_cast<const float4*>(Ti + (size_t)c * na + j0);
+#pragma unroll
+            for (int ty = 0; ty < 4; ty++) {
+                const float r = R[ty * ldr_t + row * ncp + c];
+                acc[ty][0] += r * w.x; acc[ty][1] += r * w.y;
+                acc[ty][2] += r * w.z; acc[ty][3] += r * w.w;
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int j = j0 + q;
+            float s, co;
+            // polcat angle t = 2 pi (j) / na
+            sincospif(2.0f * (float)j / (float)na, &s, &co);
+            const float fr = acc[0][q], ft = acc[1][q];
+            const float fz = (tmask & 4) ? acc[2][q] : 0.f, ph = (tmask & 8) ? acc[3][q] : 0.f;
+            dst[row * row_stride + j] = make_float4(fr * co - ft * s, fr * s + ft * co, fz, ph);
+            if (polar) {
+                size_t o = polar_off + row * row_stride + j;
+                polar[o] = fr;
+                polar[mesh + o] = ft;
+                polar[2 * mesh + o] = fz;
+                polar[3 * mesh + o] = ph;
+            }
+        }
+    }
+}
+
+#define ZCH 32
+__global__ void k_syn3(DevGeo g, int nact, int ncp, int tmask, const float4* __restrict__ O,
+                       float4* __restrict__ F, float* __restrict__ polar) {
+    extern __shared__ __align__(16) float sm[];
+    const int na = g.na, ngz = g.ngz, nkz = g.nkz, nr = g.nr;
+    const int ir = blockIdx.x, z0 = blockIdx.y * ZCH;
+    const int nz = min(ZCH, ngz - z0);
+    const int K2 = 2 * nkz, ldz = ru4(K2) + 1;
+    float* Tinv = sm;                          // [ZCH][ldz]
+    float* Zc = Tinv + ZCH * ldz;              // [ru4(K2)][ncp]
+    float* R = Zc + ru4(K2) * ncp;             // [4][ZCH][ncp]
+    float* Ti = R + 4 * ZCH * ncp;             // [ncp][na]
+    for (int i = threadIdx.x; i < ZCH * ldz; i += blockDim.x) {
+        int zr = i / ldz, r = i - zr * ldz;
+        int z = z0 + zr, k = r >> 1;
+        float v = 0.f;
+        if (zr < nz && r < K2) {
+            if ((r & 1) == 0) {
+                if (k == 0) v = 1.f;
+                else if (k == ngz) v = (z & 1) ? -1.f : 1.f;
+                else {
+                    int idx = (int)(((int64_t)k * z) % (2 * ngz));
+                    v = 2.f * cospif((float)idx / (float)ngz);
+                }
+            } else if (k > 0 && k < ngz) {
+                int idx = (int)(((int64_t)k * z) % (2 * ngz));
+                v = -2.f * sinpif((float)idx / (float)ngz);
+            }
+        }
+        Tinv[i] = v;
+    }
+    build_tazi(Ti, na, nact, ncp, g.mmax, 1.0f / (float)(2 * ngz * na));
+    for (int i = threadIdx.x; i < 4 * ZCH * ncp; i += blockDim.x) R[i] = 0.f;
+    __syncthreads();
+    for (int t = 0; t < 4; t++) {
+        if (!((tmask >> t) & 1)) continue;
+        for (int i = threadIdx.x; i < ru4(K2) * ncp; i += blockDim.x) {
+            int r = i / ncp, c = i - r * ncp;
+            int k = r >> 1, a = c >> 1;
+            float v = 0.f;
+            if (k < nkz && a < nact) {
+                float4 o = O[(((size_t)t * nact + a) * nkz + k) * nr + ir];
+                // rows: 2k -> A, 2k+1 -> B; cols: 2a -> a-row, 2a+1 -> b-row
+                v = (c & 1) ? ((r & 1) ? o.w : o.z) : ((r & 1) ? o.y : o.x);
+            }
+            Zc[i] = v;
+        }
+        __syncthreads();
+        float* Rt = R + t * ZCH * ncp;
+        sgemm44(nz, ncp, K2, Tinv, ldz, Zc, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+                if (r0 + i < ZCH)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) Rt[(r0 + i) * ncp + c0 + j] = acc[i][j];
+        });
+        __syncthreads();
+    }
+    const size_t mesh = g.mesh;
+    float4* dst = F + ((size_t)ir * ngz + z0) * na;
+    syn_final(g, ncp, nz, R, ZCH * ncp, Ti, dst, (size_t)na, polar,
+              ((size_t)ir * ngz + z0) * na, mesh, tmask);
+}
+
+__global__ void k_syn2(DevGeo g, int nact, int ncp, int tmask, const float4* __restrict__ O,
+                       float4* __restrict__ F, float* __restrict__ polar) {
+    extern __shared__ __align__(16) float sm[];
+    const int na = g.na, nr = g.nr;
+    const int ir0 = blockIdx.x * RB2;
+    const int nrows = min(RB2, nr - ir0);
+    float* R = sm;                    // [4][RB2][ncp]
+    float* Ti = R + 4 * RB2 * ncp;    // [ncp][na]
+    build_tazi(Ti, na, nact, ncp, g.mmax, 1.0f / (float)na);
+    for (int i = threadIdx.x; i < 4 * RB2 * ncp; i += blockDim.x) {
+        int t = i / (RB2 * ncp), rem = i - t * RB2 * ncp;
+        int r = rem / ncp, c = rem - r * ncp;
+        int a = c >> 1, ir = ir0 + r;
+        float v = 0.f;
+        if (((tmask >> t) & 1) && a < nact && ir < nr) {
+            float4 o = O[((size_t)t * nact + a) * nr + ir];
+            v = (c & 1) ? o.z : o.x;
+        }
+        R[i] = v;
+    }
+    __syncthreads();
+    syn_final(g, ncp, nrows, R, RB2 * ncp, Ti, F + (size_t)ir0 * na, (size_t)na, polar,
+              (size_t)ir0 * na, (size_t)g.mesh, tmask);
+}
+
+// ---------------------------------------------------------------------------
+static int set_act(GxCtx* c) {
+    GX_CUDA(c, cudaMemcpyToSymbolAsync(c_act_m, c->spec.m, sizeof(int) * 260, 0,
+                                       cudaMemcpyHostToDevice, c->stream));
+    return GX_OK;
+}
+
+static size_t fwd3_smem(const DevGeo& g, int ncp) {
+    int ldx = g.na + 1;
+    int r0sz = std::max(ru4(g.ngz) * ldx, ru4(2 * g.nkz) * g.ngz);
+    return sizeof(float) * ((size_t)r0sz + (size_t)g.na * ncp + (size_t)ru4(g.ngz) * ncp);
+}
+static size_t syn3_smem(const DevGeo& g, int ncp) {
+    int K2 = 2 * g.nkz, ldz = ru4(K2) + 1;
+    return sizeof(float) * ((size_t)ZCH * ldz + (size_t)ru4(K2) * ncp + 4 * ZCH * ncp +
+                            (size_t)ncp * g.na);
+}
+
+// findf for the mixed path: mass -> field (and optional polar copy)
+int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
+    const DevGeo& g = c->g;
+    const int nact = c->spec.nact;
+    if (nact == 0) return c->err = "no active harmonics", GX_ERR_ARG;
+    const int ncp = ru4(2 * nact);
+    int rc = set_act(c);
+    if (rc) return rc;
+    float* polar = nullptr;
+    if (!polcat_only_field) {
+        if (!c->polar) GX_CUDA(c, cudaMalloc((void**)&c->polar, sizeof(float) * 4 * g.mesh));
+        polar = c->polar;
+    }
+    int tmask = 1 | 2 | (g.ndim == 3 ? 4 : 0) | (lpot ? 8 : 0);
+    if (g.ng == 1) tmask &= ~2;
+    rc = gx_phase_mark(c, PH_FWD);
+    if (rc) return rc;
+    if (g.ndim == 3) {
+        size_t sm = fwd3_smem(g, ncp);
+        GX_CUDA(c, cudaFuncSetAttribute(k_fwd3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_fwd3<<<g.nr, 512, sm, c->stream>>>(g, nact, ncp, c->jrk_d, c->mass, c->specS);
+        GX_LAUNCHED(c);
+    } else {
+        size_t sm = sizeof(float) * ((size_t)RB2 * (g.na + 1) + (size_t)g.na * ncp);
+        GX_CUDA(c, cudaFuncSetAttribute(k_fwd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int nb = (g.nr + RB2 - 1) / RB2;
+        k_fwd2<<<nb, 256, sm, c->stream>>>(g, nact, ncp, c->mass, c->specS);
+        GX_LAUNCHED(c);
+    }
+    rc = gx_phase_mark(c, PH_CONV);
+    if (rc) return rc;
+    {
+        size_t sm = sizeof(float4) * (size_t)g.nr * 9;
+        dim3 grid(nact, g.nkz);
+        bool vec = (g.nr % 4) == 0;
+        if (vec) {
+            GX_CUDA(c, cudaFuncSetAttribute(k_conv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_conv<true><<<grid, 256, sm, c->stream>>>(g, nact, tmask, c->green32, c->specS, c->specO, c->jrk_d);
+        } else {
+            GX_CUDA(c, cudaFuncSetAttribute(k_conv<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_conv<false><<<grid, 256, sm, c->stream>>>(g, nact, tmask, c->green32, c->specS, c->specO, c->jrk_d);
+        }
+        GX_LAUNCHED(c);
+    }
+    rc = gx_phase_mark(c, PH_SYN);
+    if (rc) return rc;
+    if (g.ndim == 3) {
+        size_t sm = syn3_smem(g, ncp);
+        GX_CUDA(c, cudaFuncSetAttribute(k_syn3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        dim3 grid(g.nr, (g.ngz + ZCH - 1) / ZCH);
+        k_syn3<<<grid, 256, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, c->field, polar);
+        GX_LAUNCHED(c);
+    } else {
+        size_t sm = sizeof(float) * ((size_t)4 * RB2 * ncp + (size_t)ncp * g.na);
+        GX_CUDA(c, cudaFuncSetAttribute(k_syn2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        int nb = (g.nr + RB2 - 1) / RB2;
+        k_syn2<<<nb, 256, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, c->field, polar);
+        GX_LAUNCHED(c);
+    }
+    rc = gx_phase_end(c);
+    if (rc) return rc;
+    c->have_field = true;
+    c->field_pot = lpot != 0;
+    return GX_OK;
+}
+
+// ---------------------------------------------------------------------------
+// grid access
+__global__ void k_field_comp(const float4* __restrict__ F, float* __restrict__ out, int n, int comp) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 v = F[i];
+    out[i] = comp == 0 ? v.x : comp == 1 ? v.y : comp == 2 ? v.z : v.w;
+}
+__global__ void k_d2f(const double* __restrict__ a, float* __restrict__ b, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (float)a[i];
+}
+__global__ void k_f2d(const float* __restrict__ a, double* __restrict__ b, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) b[i] = (double)a[i];
+}
+
+extern "C" int gx_get_grid(GxCtx* c, int which, float* out) {
+    if (!c || !out || which < 0 || which > 6) return GX_ERR_ARG;
+    cudaSetDevice(c->dev);
+    const int mesh = c->g.mesh;
+    float* tmp = nullptr;
+    GX_CUDA(c, cudaMallocAsync((void**)&tmp, sizeof(float) * mesh, c->stream));
+    const int bs = 256, nb = (mesh + bs - 1) / bs;
+    int rc = GX_OK;
+    if (which == GX_GRID_MASS) {
+        if (!c->have_mass) rc = GX_ERR_STATE, c->err = "no mass array";
+        else if (c->fp64) k_d2f<<<nb, bs, 0, c->stream>>>(c->mass64, tmp, mesh);
+        else GX_CUDA(c, cudaMemcpyAsync(tmp, c->mass, sizeof(float) * mesh, cudaMemcpyDeviceToDevice, c->stream));
+    } else if (which >= GX_GRID_FR && which <= GX_GRID_POT) {
+        int comp = which - GX_GRID_FR;
+        if (c->fp64) {
+            if (!c->have_field) rc = GX_ERR_STATE, c->err = "no fields";
+            else k_d2f<<<nb, bs, 0, c->stream>>>(c->polar64 + (size_t)comp * mesh, tmp, mesh);
+        } else if (comp >= 2 && c->have_field) {
+            k_field_comp<<<nb, bs, 0, c->stream>>>(c->field, tmp, mesh, comp);
+        } else if (!c->polar || !c->have_field) {
+            rc = GX_ERR_STATE, c->err = "polar fields need gx_findf_polar";
+        } else {
+            GX_CUDA(c, cudaMemcpyAsync(tmp, c->polar + (size_t)comp * mesh, sizeof(float) * mesh,
+                                       cudaMemcpyDeviceToDevice, c->stream));
+        }
+    } else {
+        int comp = which - GX_GRID_FX;
+        if (!c->have_field) rc = GX_ERR_STATE, c->err = "no fields";
+        else if (c->fp64) k_d2f<<<nb, bs, 0, c->stream>>>(c->field64 + (size_t)comp * mesh, tmp, mesh);
+        else k_field_comp<<<nb, bs, 0, c->stream>>>(c->field, tmp, mesh, comp);
+    }
+    if (rc == GX_OK) {
+        GX_CUDA(c, cudaGetLastError());
+        GX_CUDA(c, cudaMemcpyAsync(out, tmp, sizeof(float) * mesh, cudaMemcpyDeviceToHost, c->stream));
+    }
+    GX_CUDA(c, cudaFreeAsync(tmp, c->stream));
+    GX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return rc;
+}
+
+extern "C" int gx_set_mass(GxCtx* c, const float* mass) {
+    if (!c || !mass) return GX_ERR_ARG;
+    cudaSetDevice(c->dev);
+    const DevGeo& g = c->g;
+    const int mesh = g.mesh;
+    // active ring range of the installed masses (p3ckst.f sets jrad/krad)
+    int jr = g.nr, kr = 0;
+    const int per = g.ngz * g.na;
+    for (int ir = 0; ir < g.nr; ir++)
+        for (int i = 0; i < per; i++)
+            if (mass[(size_t)ir * per + i] != 0.f) {
+                jr = std::min(jr, ir + 1);
+                kr = std::max(kr, ir + 1);
+                break;
+            }
+    c->jrs = jr;
+    c->krs = kr;
+    int32_t jrk[2] = {jr, kr};
+    GX_CUDA(c, cudaMemcpyAsync(c->jrk_d, jrk, sizeof jrk, cudaMemcpyHostToDevice, c->stream));
+    if (c->fp64) {
+        float* tmp = nullptr;
+        GX_CUDA(c, cudaMallocAsync((void**)&tmp, sizeof(float) * mesh, c->stream));
+        GX_CUDA(c, cudaMemcpyAsync(tmp, mass, sizeof(float) * mesh, cudaMemcpyHostToDevice, c->stream));
+        k_f2d<<<(mesh + 255) / 256, 256, 0, c->stream>>>(tmp, c->mass64, mesh);
+        GX_LAUNCHED(c);
+        GX_CUDA(c, cudaFreeAsync(tmp, c->stream));
+    } else {
+        GX_CUDA(c, cudaMemcpyAsync(c->mass, mass, sizeof(float) * mesh, cudaMemcpyHostToDevice, c->stream));
+    }
+    GX_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->have_mass = true;
+    c->have_field = false;
+    return GX_OK;
+}

@@ -156,6 +156,12 @@ int gx_green_get(GxCtx* ctx, int type, double* out, int64_t n);
  * device SoA store.  SRC/lib15/loadup.f:36-140. */
 int gx_loadup(GxCtx* ctx, const float* coords, int64_t n);
 
+/* weight: cell numbers (ncl - 1, or -1 off the grid / in the hole) and the
+ * 4 (2D) or 8 (3D) interpolation weights, 8 floats per particle, of n AoS
+ * particle records.  old != 0 selects the interpolation form (no sector
+ * folding).  SRC/lib15/weight.f:61-101 (p2d), 196-250 (p3d). */
+int gx_weight(GxCtx* ctx, const float* coords, int64_t n, int old, int32_t* ncl, float* wt);
+
 /* dumpp (coordinates only): copy the particle records back out, in the
  * order they were loaded.  SRC/lib15/dumpp.f:246-387. */
 int gx_unload(GxCtx* ctx, float* coords);
@@ -204,6 +210,16 @@ int gx_last_step_ms(const GxCtx* ctx, float* ms);
 
 /* Number of kernels launched by the last gx_step call. */
 int gx_last_launch_count(const GxCtx* ctx, int64_t* n);
+
+/* Phase timing of gx_step: on != 0 records CUDA events between the phases
+ * of every step (forward transform, radial contraction, synthesis,
+ * particle pass, sort, deposit, mass combine, other) on the context
+ * stream.  No reference counterpart (instrumentation). */
+int gx_set_profile(GxCtx* ctx, int on);
+
+/* Accumulated device ms and step counts per phase since the last
+ * gx_set_profile(ctx, 1); arrays of 8. */
+int gx_phase_ms(const GxCtx* ctx, float* ms, int64_t* count);
 
 #ifdef __cplusplus
 }
