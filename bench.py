@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""bench.py -- particle-steps/s of the polar-grid particle-mesh step on B200.
+
+Default workload (N=1): the 3D cylindrical polar grid of 128 rings x 256
+spokes x 125 planes (dz = 0.04, harmonics m = 0..16, Plummer softening 0.1,
+log-spaced rings r = 0.05 .. 5) with 10M particles of a seeded
+Kuzmin-Toomre disc (sech^2 layer z0 = 0.1), dt = 0.02.  One step = findf
+(azimuthal + doubled-grid vertical transforms, radial contraction with the
+resident Green table, synthesis, polcat) + the fused particle pass (grdacc,
+stpgrp, new cell keys) + the row radix sort + the deterministic deposit
+(massgn, scaled).  Inputs are larger than L2 (particle store 240 MB, Green
+table 411 MB per step), so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+--impl reference times the CPU restatement of the same step (the oracle
+port; the Fortran reference cannot be built in this image) on the host
+cores, on a bounded sample of the same workload.
+Under torchrun (N > 1) each rank owns its own particles (weak scaling) and
+the ranks sum their mass grids every step (the reference's MPI design).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s on 1 B200 vs plain FP64 GPU path at force rel-err <=1e-5"
+UNIT = "particle-steps/s"
+
+WORKLOADS = {
+    # 3D polar grid, the configuration the metric is quoted on
+    "polar3d-128x256x125-10M": dict(ndim=3, nr=128, na=256, ngz=125, dzg=0.04, ng=17,
+                                    softl=0.1, n=10_000_000, dt=0.02, z0=0.1, disk_rmax=4.8,
+                                    r0=0.05, r1=5.0),
+    # 2D polar grid, the CPU-runnable case
+    "polar2d-64x128-100k": dict(ndim=2, nr=64, na=128, ngz=1, dzg=0.0, ng=9, softl=0.1,
+                                n=100_000, dt=0.025, z0=0.0, disk_rmax=4.8, r0=0.05, r1=5.0),
+}
+DEFAULT = "polar3d-128x256x125-10M"
+
+
+def make_cfg(w, precision):
+    from galaxy_b200 import make_config, GX_RMAP_LOG
+    a = float(np.log(w["r1"] / w["r0"]) / (w["nr"] - 1))
+    return make_config(w["ndim"], w["nr"], w["na"], ngz=w["ngz"], dzg=w["dzg"], ng=w["ng"],
+                       rmap=GX_RMAP_LOG, rmap_a=a, rmap_r0=w["r0"], softl=w["softl"], tsoft=1,
+                       precision=precision)
+
+
+def make_ic(w, n, seed):
+    from galaxy_b200.disk import kt_disk
+    return kt_disk(n, seed=seed, rmax=w["disk_rmax"], ndim=w["ndim"], z0=w["z0"] or 0.1,
+                   dt=w["dt"])
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 8:
+                self.rows.append(f)
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic bytes per launch of each phase (the figures roofline.achieved
+# is built from; the per-step formula of the measurement plan is
+# N * 2 * 2d * 4 + Green bytes + mesh * 4 * (2 + 2F))
+def green_counts(cfg, geo, lpot=False):
+    """(m, kz) pairs the radial contraction reads for each field type."""
+    act = [m for m in range(geo.ng) if not geo.lg[m]]
+    nkz = geo.ngz + 1 if cfg.ndim == 3 else 1
+    n_fr = len(act) * nkz
+    n_ft = len([m for m in act if 1 <= m <= min(geo.ng, geo.mmax - 1) - 1]) * nkz
+    n_fz = len(act) * (geo.ngz - 1) if cfg.ndim == 3 else 0
+    return n_fr + n_ft + n_fz + (n_fr if lpot else 0), len(act), nkz
+
+
+def phase_bytes(cfg, geo, n):
+    d = cfg.ndim
+    mesh = geo.mesh
+    npairs, nact, nkz = green_counts(cfg, geo)
+    spec = nact * nkz * geo.nr * 16
+    ntypes = 3 if d == 3 else 2
+    return {
+        "push": n * 2 * 2 * d * 4,                        # phase space read + write
+        "conv": npairs * geo.nr * geo.nr * 4 + spec * (1 + ntypes),
+        "syn": spec * ntypes + mesh * 16,                 # spectra in, float4 field out
+        "fwd": mesh * 4 + spec,
+        "deposit": n * (d * 4 + 4) + mesh * 4,            # positions + order in, mass out
+        "sort": n * 8 * 2,                                # (row key, index) in and out
+        "combine": mesh * 4,
+    }
+
+
+def step_bytes(cfg, geo, n):
+    npairs, _, _ = green_counts(cfg, geo)
+    nf = cfg.ndim  # Cartesian field components
+    return n * 2 * 2 * cfg.ndim * 4 + npairs * geo.nr * geo.nr * 4 + geo.mesh * 4 * (2 + 2 * nf)
+
+
+KERNEL_OF = {"push": "k_push", "conv": "k_conv", "syn": "k_syn3", "fwd": "k_fwd3",
+             "deposit": "k_deposit", "sort": "k_sort_scatter", "combine": "k_mass_combine"}
+
+
+def ncu_traffic(workload):
+    """dram bytes per launch per kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    if not os.path.exists(p):
+        return {}
+    d = json.load(open(p))
+    return d.get(workload, {})
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args, w, rank, world, comm):
+    import galaxy_b200 as gb
+    from galaxy_b200 import Galaxy, GX_PREC_MIXED, GX_PREC_FP64
+    n = args.n or w["n"]
+    rec, pm = make_ic(w, n, seed=12345 + rank)
+    out = {}
+    cfg = make_cfg(w, GX_PREC_MIXED)
+    cfg.pmass = pm / world          # the ranks' discs together carry the disc mass
+    cfg.device = int(os.environ.get("LOCAL_RANK", 0))
+    gal = Galaxy(cfg)
+    geo = gal.geo
+    if comm is not None:
+        comm.attach(gal)
+    gal.greenm()
+    gal.loadup(rec)
+    gal.masset()
+    gal.findf(True)
+    a32 = gal.getacc(want_pot=False) if rank == 0 and not args.no_fp64 else None
+    gal.tmcent(True)
+    gal.step(args.warmup)
+    with ClockSampler(cfg.device) as clk:
+        if comm is not None:
+            comm.barrier()
+        gal.step(args.steps)
+    ms = gal.last_step_ms()
+    launches = gal.last_launch_count()
+    ms_max = comm.max(ms) if comm is not None else ms
+    out["ms_total"] = ms_max
+    out["ms_per_step"] = ms_max / args.steps
+    out["value"] = n * world * args.steps / (ms_max * 1e-3)
+    out["gpu_launches"] = launches
+    out["clocks"] = clk.summary()
+    # phase timing pass (separate from the timed region)
+    gal.set_profile(True)
+    kp = 3
+    gal.step(kp)
+    ph = gal.phase_ms()
+    gal.set_profile(False)
+    pb = phase_bytes(cfg, geo, n)
+    peak, src = peaks()
+    traffic = ncu_traffic(args.workload)
+    phases = {}
+    for k, (t, c) in ph.items():
+        per = t / max(c, 1)
+        gbs = pb.get(k, 0) / (per * 1e-3) / 1e9 if per > 0 else 0.0
+        phases[k] = {"ms": round(per, 4), "GB_s": round(gbs, 1)}
+    top = max(ph, key=lambda k: ph[k][0])
+    per = ph[top][0] / max(ph[top][1], 1)
+    ach = pb[top] / (per * 1e-3) / 1e9
+    tr = traffic.get(KERNEL_OF.get(top, top))
+    out["roofline"] = {"kernel": KERNEL_OF.get(top, top), "bound": "hbm",
+                       "achieved": round(ach, 1), "peak": peak, "unit": "GB/s",
+                       "frac": round(ach / peak, 4), "traffic": tr,
+                       "algorithmic_bytes": pb[top], "peak_source": src}
+    sb = step_bytes(cfg, geo, n)
+    out["step_roofline"] = {"bytes": sb, "achieved": round(sb / (out["ms_per_step"] * 1e-3) / 1e9, 1),
+                            "frac": round(sb / (out["ms_per_step"] * 1e-3) / 1e9 / peak, 4)}
+    out["phases"] = phases
+    gal.close()
+    # plain FP64 path on the same particles: rate and force error
+    if rank == 0 and not args.no_fp64:
+        cfg64 = make_cfg(w, GX_PREC_FP64)
+        cfg64.pmass = pm
+        cfg64.device = cfg.device
+        g64 = Galaxy(cfg64)
+        g64.greenm()
+        g64.loadup(rec)
+        g64.masset()
+        g64.findf(True)
+        a64 = g64.getacc(want_pot=False)
+        err = float(np.linalg.norm(a32.astype(np.float64) - a64) / np.linalg.norm(a64))
+        g64.step(1)
+        k64 = 3
+        g64.step(k64)
+        ms64 = g64.last_step_ms() / k64
+        g64.close()
+        out["fp64_path"] = {"value": n * 1e3 / ms64, "ms_per_step": round(ms64, 3),
+                            "steps": k64}
+        out["speedup_vs_fp64_path"] = round(out["value"] / world / (n * 1e3 / ms64), 2)
+        out["force_rel_err"] = err
+    return out, rec, pm, cfg
+
+
+def run_e2e(args, w, rec, pm, cfg_dev):
+    """The same run through the public C ABI with host buffers: loadup (H2D
+    from pinned host memory), masset, K steps, unload (D2H), wall clock."""
+    from galaxy_b200 import Galaxy, GX_PREC_MIXED, PinnedArray
+    pin_in = PinnedArray(rec.shape)
+    pin_in.array[...] = rec
+    pin_out = PinnedArray(rec.shape)
+    src, dst, pinned = pin_in.ptr, pin_out.ptr, True
+    cfg = make_cfg(w, GX_PREC_MIXED)
+    cfg.pmass = pm
+    cfg.device = cfg_dev
+    gal = Galaxy(cfg)
+    gal.greenm()
+    gal.loadup_ptr(src, rec.shape[0])      # warm the allocation
+    gal.masset()
+    gal.step(1)
+    n = rec.shape[0]
+    t0 = time.perf_counter()
+    gal.loadup_ptr(src, n)
+    gal.masset()
+    gal.step(args.steps)
+    gal.unload_ptr(dst)
+    t1 = time.perf_counter()
+    ok = bool(np.isfinite(pin_out.array).all())
+    gal.close()
+    pin_in.free()
+    pin_out.free()
+    nbytes = n * rec.shape[1] * 4
+    return {"value": n * args.steps / (t1 - t0), "unit": UNIT,
+            "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
+            "pinned": pinned, "finite": ok, "what": "gx_loadup + gx_masset + gx_step(K) + gx_unload, wall clock"}
+
+
+def cpu_rate(w, rec, pm, steps, budget_s, threads):
+    """CPU restatement of one step (oracle, FP32 mirror) on the host cores:
+    the field solve on the full grid, the particle loop on a sample, the
+    step time extrapolated linearly in particles.  Returns a dict."""
+    from oracle import oracle as ox
+    from galaxy_b200 import GX_PREC_MIXED
+    ox.set_threads(threads)
+    cfg = make_cfg(w, GX_PREC_MIXED)
+    cfg.pmass = pm
+    n = rec.shape[0]
+    t0 = time.perf_counter()
+    G = ox.green(cfg, 32)
+    t_green = time.perf_counter() - t0
+    ns = min(n, 200_000)
+    samp = np.ascontiguousarray(rec[:ns])
+    mass, jrk = ox.masset(cfg, samp, prec=32)
+    mass *= np.float32(n / ns)
+    times = []
+    t_start = time.perf_counter()
+    for s in range(steps):
+        t0 = time.perf_counter()
+        f = ox.findf(cfg, G, mass, lpot=False, jrk=jrk, prec=32, polar=False)
+        t1 = time.perf_counter()
+        mass2, jrk2 = ox.particle_pass(cfg, samp, f, prec=32)
+        t2 = time.perf_counter()
+        times.append((t1 - t0) + (t2 - t1) * n / ns)
+        if time.perf_counter() - t_start > budget_s and s >= 1:
+            break
+    ox.set_threads(1)
+    t_step = float(np.median(times))
+    return {"value": n / t_step, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": (f"field solve on the full {w['nr']}x{w['na']}x{w['ngz']} grid + particle "
+                       f"loop (grdacc, stpgrp, massgn) on {ns} of the {n} particles, "
+                       f"extrapolated linearly to {n}; median of {len(times)} steps; "
+                       f"Green table built separately in {t_green:.1f} s"),
+            "t_step_s": t_step, "steps_timed": len(times)}
+
+
+class Comm:
+    """Per-step mass-grid sum across ranks over NCCL (torch.distributed)."""
+
+    def __init__(self):
+        import torch
+        import torch.distributed as dist
+        self.torch, self.dist = torch, dist
+        self.rank, self.world = dist.get_rank(), dist.get_world_size()
+
+    def attach(self, gal):
+        gal.set_comm(self)
+
+    def barrier(self):
+        self.dist.barrier()
+
+    def max(self, v):
+        t = self.torch.tensor([float(v)], device="cuda")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
+    ap.add_argument("--n", type=int, default=0, help="particles per GPU (default: workload)")
+    ap.add_argument("--no-fp64", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=30.0)
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    w = WORKLOADS[args.workload]
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    n = args.n or w["n"]
+    wcfg = {"workload": args.workload, "grid": [w["nr"], w["na"], w["ngz"]],
+            "harmonics": f"0..{w['ng'] - 1}", "particles_per_gpu": n, "dt": w["dt"],
+            "softening": w["softl"], "rings": f"log-spaced {w['r0']}..{w['r1']}",
+            "l2": "inputs larger than L2 (no flush)"}
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        rec, pm = make_ic(w, n, seed=12345)
+        threads = os.cpu_count() or 1
+        r = cpu_rate(w, rec, pm, args.steps + args.warmup, 150.0, threads)
+        line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": r["t_step_s"] * 1e3,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "config": wcfg, "impl": "reference",
+                "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": r["value"], "unit": UNIT, "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0},
+                "note": "CPU restatement of the reference step (Fortran reference not buildable "
+                        "here: no Fortran compiler)"}
+        print(json.dumps(line))
+        return
+    comm = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        import datetime
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        comm = Comm()
+    out, rec, pm, cfg = run_ours(args, w, rank, world, comm)
+    if comm is not None:
+        comm.barrier()
+    if rank == 0:
+        e2e = run_e2e(args, w, rec, pm, cfg.device) if world == 1 else None
+        cpu = None
+        if world == 1 and not args.no_cpu:
+            cpu = cpu_rate(w, rec, pm, 3, args.cpu_budget, os.cpu_count() or 1)
+            cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+        line = {"metric": METRIC, "value": out["value"], "unit": UNIT, "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": out["ms_per_step"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "config": wcfg,
+                "roofline": out["roofline"], "cpu_baseline": cpu, "e2e": e2e,
+                "gpu_launches": out["gpu_launches"], "clocks": out["clocks"],
+                "fp64_path": out.get("fp64_path"),
+                "speedup_vs_fp64_path": out.get("speedup_vs_fp64_path"),
+                "force_rel_err": out.get("force_rel_err"),
+                "step_roofline": out["step_roofline"], "phases": out["phases"]}
+        print(json.dumps(line))
+    if comm is not None:
+        comm.dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -64,10 +64,43 @@ def lib():
         L.gx_icheck.argtypes = [P, C.POINTER(GxDiag)]
         L.gx_last_step_ms.argtypes = [P, C.POINTER(C.c_float)]
         L.gx_last_launch_count.argtypes = [P, C.POINTER(C.c_int64)]
+        L.gx_comm_unique_id.argtypes = [C.c_char_p]
+        L.gx_comm_init.argtypes = [P, C.c_char_p, C.c_int, C.c_int]
+        L.gx_host_alloc.argtypes = [i64, C.POINTER(P)]
+        L.gx_host_free.argtypes = [P]
         L.gx_set_profile.argtypes = [P, C.c_int]
         L.gx_phase_ms.argtypes = [P, P, P]
         _lib = L
     return _lib
+
+
+class PinnedArray:
+    """numpy view of page-locked host memory allocated by the library."""
+
+    def __init__(self, shape, dtype=np.float32):
+        nbytes = int(np.prod(shape)) * np.dtype(dtype).itemsize
+        self._p = C.c_void_p()
+        rc = lib().gx_host_alloc(nbytes, C.byref(self._p))
+        if rc != GX_OK:
+            raise GxError(rc, "gx_host_alloc failed")
+        buf = (C.c_char * nbytes).from_address(self._p.value)
+        self.array = np.frombuffer(buf, dtype=dtype).reshape(shape)
+
+    @property
+    def ptr(self):
+        return self._p.value
+
+    def free(self):
+        if self._p:
+            self.array = None
+            lib().gx_host_free(self._p)
+            self._p = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def _ptr(a):
@@ -131,6 +164,25 @@ class Galaxy:
         assert coords.ndim == 2 and coords.shape[1] == 2 * self.ndim
         self.n = coords.shape[0]
         self._chk(self._L.gx_loadup(self._h, _ptr(coords), self.n))
+
+    def loadup_ptr(self, ptr, n):
+        """loadup from a host pointer (e.g. pinned memory) of n records."""
+        self.n = int(n)
+        self._chk(self._L.gx_loadup(self._h, C.c_void_p(ptr), self.n))
+
+    def unload_ptr(self, ptr):
+        self._chk(self._L.gx_unload(self._h, C.c_void_p(ptr)))
+
+    def set_comm(self, comm):
+        """Bind to the ranks of a torch.distributed job (one rank per GPU)."""
+        import torch.distributed as dist
+        rank, world = dist.get_rank(), dist.get_world_size()
+        buf = C.create_string_buffer(128)
+        if rank == 0:
+            self._chk(self._L.gx_comm_unique_id(buf))
+        obj = [bytes(buf.raw)]
+        dist.broadcast_object_list(obj, src=0)
+        self._chk(self._L.gx_comm_init(self._h, obj[0], world, rank))
 
     def unload(self):
         out = np.zeros((self.n, 2 * self.ndim), np.float32)

@@ -22,6 +22,7 @@ FLAGS = [
     "-Xcompiler", "-fPIC", "-shared",
     "--expt-relaxed-constexpr", "--extended-lambda",
     "-cudart", "static",
+    "-ldl",
 ]
 
 

@@ -217,6 +217,7 @@ void gx_destroy(GxCtx* c) {
     if (!c) return;
     cudaSetDevice(c->dev);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    gx_comm_destroy(c);
     void* ptrs[] = {c->green32, c->green64, c->pbuf[0], c->pbuf[1], c->perm, c->origin,
                     c->origin_tmp, c->pkey, c->p64, c->key64, c->w64, c->acc64, c->ppot,
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
@@ -520,6 +521,21 @@ int gx_step(GxCtx* c, int nsteps, int phys) {
         c->err = b;
         return GX_ERR_DEVICE;
     }
+    return GX_OK;
+}
+
+int gx_host_alloc(int64_t bytes, void** ptr) {
+    if (!ptr || bytes < 0) return GX_ERR_ARG;
+    *ptr = nullptr;
+    if (cudaMallocHost(ptr, (size_t)std::max<int64_t>(bytes, 1)) != cudaSuccess) {
+        *ptr = nullptr;
+        return GX_ERR_NOMEM;
+    }
+    return GX_OK;
+}
+
+int gx_host_free(void* ptr) {
+    if (ptr && cudaFreeHost(ptr) != cudaSuccess) return GX_ERR_CUDA;
     return GX_OK;
 }
 

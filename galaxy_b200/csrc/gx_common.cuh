@@ -119,6 +119,10 @@ struct GxCtx {
     float phase_ms[GX_NPHASE] = {};
     int64_t phase_n[GX_NPHASE] = {};
     int open_phase = -1;
+
+    // multi-GPU (gx_comm.cu): NCCL communicator of the particle decomposition
+    void* comm = nullptr;
+    int nranks = 1, rank = 0;
 };
 
 // record the start of phase ph (prof mode) and close the previous one
@@ -296,3 +300,6 @@ int gx_fp64_findf(GxCtx* c, int lpot, bool polcat);
 int gx_fp64_getacc(GxCtx* c, float* acc, float* pot);
 int gx_fp64_step(GxCtx* c, int nsteps, int phys);
 int gx_mass_dense_from_stage(GxCtx* c);
+int gx_comm_reduce_range(GxCtx* c);
+int gx_comm_reduce_spectrum(GxCtx* c);
+void gx_comm_destroy(GxCtx* c);

@@ -98,8 +98,13 @@ __global__ void k_fwd3(DevGeo g, int nact, int ncp, const int32_t* __restrict__ 
     extern __shared__ __align__(16) float sm[];
     const int na = g.na, ngz = g.ngz, nkz = g.nkz, nr = g.nr;
     const int ir = blockIdx.x;
-    // only the rings that hold mass are transformed (p3fndf.f:44-57)
-    if (ir < jrk[0] - 1 || ir > min(jrk[1], nr) - 1) return;
+    // only the rings that hold mass are transformed (p3fndf.f:44-57); the
+    // others get a zero spectrum so that the sum over ranks stays exact
+    if (ir < jrk[0] - 1 || ir > min(jrk[1], nr) - 1) {
+        for (int i = threadIdx.x; i < nact * nkz; i += blockDim.x)
+            S[(size_t)i * nr + ir] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
     const int ldx = na + 1;
     const int r0sz = max(ru4(ngz) * ldx, ru4(2 * nkz) * ngz);
     float* X = sm;                       // [ru4(ngz)][na + 1], later Tz [ru4(2 nkz)][ngz]
@@ -451,6 +456,8 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
     if (g.ng == 1) tmask &= ~2;
     rc = gx_phase_mark(c, PH_FWD);
     if (rc) return rc;
+    rc = gx_comm_reduce_range(c);
+    if (rc) return rc;
     if (g.ndim == 3) {
         size_t sm = fwd3_smem(g, ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_fwd3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -463,6 +470,8 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
         k_fwd2<<<nb, 256, sm, c->stream>>>(g, nact, ncp, c->mass, c->specS);
         GX_LAUNCHED(c);
     }
+    rc = gx_comm_reduce_spectrum(c);
+    if (rc) return rc;
     rc = gx_phase_mark(c, PH_CONV);
     if (rc) return rc;
     {

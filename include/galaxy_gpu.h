@@ -211,6 +211,22 @@ int gx_last_step_ms(const GxCtx* ctx, float* ms);
 /* Number of kernels launched by the last gx_step call. */
 int gx_last_launch_count(const GxCtx* ctx, int64_t* n);
 
+/* Multi-GPU particle decomposition (the reference's MPI overlay,
+ * SRC/lib15_mpi/massum.f:54-65, p2manlp.f:164-233, p3manlp.f:102): every
+ * rank holds its own particles and a full grid; once bound to a
+ * communicator, every findf reduces the active ring range (min/max) and
+ * sums the forward spectrum of the active harmonics over the ranks, so all
+ * ranks solve for the fields of all particles.  gx_comm_unique_id fills
+ * 128 bytes on one rank, the caller broadcasts them, and every rank calls
+ * gx_comm_init with them.  Mixed path only. */
+int gx_comm_unique_id(char* id128);
+int gx_comm_init(GxCtx* ctx, const char* id128, int nranks, int rank);
+
+/* Page-locked host buffers for gx_loadup/gx_unload (cudaMallocHost in the
+ * library's own runtime).  No reference counterpart. */
+int gx_host_alloc(int64_t bytes, void** ptr);
+int gx_host_free(void* ptr);
+
 /* Phase timing of gx_step: on != 0 records CUDA events between the phases
  * of every step (forward transform, radial contraction, synthesis,
  * particle pass, sort, deposit, mass combine, other) on the context

@@ -12,6 +12,25 @@
 
 #define OX_PI 3.141592653589793238462643
 
+#ifdef _OPENMP
+#include <omp.h>
+#define OX_TID (ox_threads > 1 ? omp_get_thread_num() : 0)
+#else
+#define OX_TID 0
+#endif
+
+/* host threads used by the restated loops (1: sequential, deterministic) */
+static int ox_threads = 1;
+int ox_set_threads(int n) {
+#ifdef _OPENMP
+    ox_threads = n < 1 ? 1 : (n > 256 ? 256 : n);
+#else
+    (void)n;
+    ox_threads = 1;
+#endif
+    return ox_threads;
+}
+
 /* setgrd (SRC/lib15/setgrd.f:52-200) for p2d/p3d, the harmonic filter of
  * filset (SRC/lib15/filset.f:116-141), and the grid-size checks of p3dset
  * (SRC/lib15/p3dset.f:99-100).  Reals are formed in FP32 as the reference

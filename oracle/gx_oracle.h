@@ -35,6 +35,9 @@ extern "C" {
 #endif
 
 int ox_geometry(const GxConfig* cfg, GxGeometry* geo, char* err, int errlen);
+/* host threads of the restated loops; 1 (the default) runs them in the
+ * reference's sequential order */
+int ox_set_threads(int n);
 int64_t ox_green_size(const GxConfig* cfg);
 int64_t ox_direct_size(const GxConfig* cfg);
 
@@ -51,6 +54,8 @@ int ox_grdacc_##S(const GxConfig* cfg, int64_t n, const R* pos,                \
                   const R* fields, int phys, R* acc, R* pot);                  \
 int ox_masset_##S(const GxConfig* cfg, int64_t n, const R* pos, R* mass,       \
                   int32_t* jrk);                                               \
+int ox_particle_pass_##S(const GxConfig* cfg, int64_t n, R* pos, const R* fields,   \
+                         R* mass, int32_t* jrk);                               \
 int ox_step_##S(const GxConfig* cfg, const R* G, int64_t n, R* pos, R* mass,   \
                 int32_t* jrk, int nsteps, int phys, R* fields);                \
 int ox_direct_field_##S(const GxConfig* cfg, const R* D, int nmass,            \

@@ -188,15 +188,16 @@ int F(ox_green)(const GxConfig* c, R* G, R* D) {
     const int64_t gsz = (int64_t)4 * ng * nkz * nr * nr;
     memset(G, 0, sizeof(R) * gsz);
     if (D) memset(D, 0, sizeof(R) * (int64_t)4 * nr * nr * nkz * nth);
-    R* f = (R*)malloc(sizeof(R) * nth * (nkz + 1));
-    R* tr = (R*)malloc(sizeof(R) * nth * (nkz + 1));
-    R* zb = (R*)malloc(sizeof(R) * (nkz + 1));
-    R* zt = (R*)malloc(sizeof(R) * (nkz + 1));
+    const int T = ox_threads;
+    R* f_all = (R*)malloc(sizeof(R) * nth * (nkz + 1) * T);
+    R* tr_all = (R*)malloc(sizeof(R) * nth * (nkz + 1) * T);
+    R* zb_all = (R*)malloc(sizeof(R) * (nkz + 1) * T);
+    R* zt_all = (R*)malloc(sizeof(R) * (nkz + 1) * T);
+    R* back_all = (R*)malloc(sizeof(R) * nth * T);
     R* ctab = F(cos_tab)(na / 2 + 1);
     R* stab = F(sin_tab)(na / 2 - 1);
     R* zctab = (g.ndim == 3) ? F(cos_tab)(ngz + 1) : NULL;
     R* zstab = (g.ndim == 3) ? F(sin_tab)(ngz - 1) : NULL;
-    R* back = (R*)malloc(sizeof(R) * nth);
     for (int type = 0; type < 4; type++) {
         if (g.ndim == 2 && type == 2) continue;
         if (type == 1 && ng == 1) continue;
@@ -205,7 +206,14 @@ int F(ox_green)(const GxConfig* c, R* G, R* D) {
         const int nt = it2 - it1 + 1;
         const int iz1 = vert ? 2 : 1, iz2 = (g.ndim == 3) ? (vert ? ngz : ngz + 1) : 1;
         const int nz = iz2 - iz1 + 1;
+#pragma omp parallel for schedule(dynamic) num_threads(T) if (T > 1)
         for (int is = 0; is < nr; is++) {
+            const int tid = OX_TID;
+            R* f = f_all + (size_t)tid * nth * (nkz + 1);
+            R* tr = tr_all + (size_t)tid * nth * (nkz + 1);
+            R* zb = zb_all + (size_t)tid * (nkz + 1);
+            R* zt = zt_all + (size_t)tid * (nkz + 1);
+            R* back = back_all + (size_t)tid * nth;
             R rs = F(grofu)(&g, (R)is);
             for (int ir = 0; ir < nr; ir++) {
                 R rf = F(grofu)(&g, (R)ir);
@@ -266,80 +274,82 @@ int F(ox_green)(const GxConfig* c, R* G, R* D) {
             }
         }
     }
-    free(f);
-    free(tr);
-    free(zb);
-    free(zt);
+    free(f_all);
+    free(tr_all);
+    free(zb_all);
+    free(zt_all);
+    free(back_all);
     free(ctab);
     free(stab);
     free(zctab);
     free(zstab);
-    free(back);
     return 0;
 }
 
 /* ------------------------------------------------------------------ */
 /* weight (SRC/lib15/weight.f:61-101 p2d, 196-250 p3d linear) together
  * with the off-grid test of offgrd.f:51-77.  key = ncl - 1 or -1.      */
+static int F(weight1)(const F(og) * gp, int old, const R* q, int32_t* keyp, R* w) {
+    const int nd = gp->ndim;
+    R x = q[0], y = q[1], z = (nd == 3) ? q[2] : (R)0;
+    for (int k = 0; k < 8; k++) w[k] = 0;
+    *keyp = -1;
+    R rr = SQRT(x * x + y * y);
+    if (rr > gp->rgrid) return 0;
+    if (nd == 3 && FABS(z) > gp->zm) return 0;
+    R u = F(uofgr)(gp, rr);
+    R t;
+    if (nd == 2 || rr > (R)0) {
+#if MIRROR
+        t = (R)(atan2((double)y, (double)x) * (double)gp->na / (2.0 * OX_PI));
+#else
+        t = atan2(y, x) * (double)gp->na / (2.0 * OX_PI);
+#endif
+        if (t < (R)0) t = t + (R)gp->na;
+    } else {
+        t = 0;
+    }
+    if (!old && gp->nsect > 1) t = FMOD(t, gp->thmax);
+    if (rr < gp->rinh) return 0;
+    int ju = (int)u;
+    if (ju > gp->nr - 2) ju = gp->nr - 2;
+    int jt = (int)t;
+    R du = u - (R)ju, dt = t - (R)jt;
+    if (nd == 2) {
+        *keyp = ju * gp->na + jt;
+        R dd = du * dt;
+        w[0] = (R)1 - du - dt + dd;
+        w[1] = dt - dd;
+        w[2] = du - dd;
+        w[3] = dd;
+    } else {
+        R zz = z + gp->zm;
+        zz = zz / gp->dzg;
+        int jz = (int)zz;
+        if (jz < 0) jz = 0;
+        if (jz > gp->ngz - 2) jz = gp->ngz - 2;
+        *keyp = (ju * gp->ngz + jz) * gp->na + jt;
+        R dz = zz - (R)jz;
+        w[0] = ((R)1 - dt) * ((R)1 - dz) * ((R)1 - du);
+        w[1] = dt * ((R)1 - dz) * ((R)1 - du);
+        w[2] = ((R)1 - dt) * dz * ((R)1 - du);
+        w[3] = dt * dz * ((R)1 - du);
+        w[4] = ((R)1 - dt) * ((R)1 - dz) * du;
+        w[5] = dt * ((R)1 - dz) * du;
+        w[6] = ((R)1 - dt) * dz * du;
+        w[7] = dt * dz * du;
+    }
+    return 1;
+}
+
 int F(ox_weight)(const GxConfig* c, int old, int64_t n, const R* pos, int32_t* key,
                  R* wt, uint8_t* on) {
     F(og) g;
     if (F(og_init)(c, &g)) return GX_ERR_ARG;
-    const int nd = g.ndim, stride = 2 * nd;
-    for (int64_t p = 0; p < n; p++) {
-        const R* q = pos + p * stride;
-        R x = q[0], y = q[1], z = (nd == 3) ? q[2] : (R)0;
-        R* w = wt + p * 8;
-        for (int k = 0; k < 8; k++) w[k] = 0;
-        key[p] = -1;
-        on[p] = 0;
-        R rr = SQRT(x * x + y * y);
-        if (rr > g.rgrid) continue;
-        if (nd == 3 && FABS(z) > g.zm) continue;
-        R u = F(uofgr)(&g, rr);
-        R t;
-        if (nd == 2 || rr > (R)0) {
-#if MIRROR
-            t = (R)(atan2((double)y, (double)x) * (double)g.na / (2.0 * OX_PI));
-#else
-            t = atan2(y, x) * (double)g.na / (2.0 * OX_PI);
-#endif
-            if (t < (R)0) t = t + (R)g.na;
-        } else {
-            t = 0;
-        }
-        if (!old && g.nsect > 1) t = FMOD(t, g.thmax);
-        if (rr < g.rinh) continue;
-        int ju = (int)u;
-        if (ju > g.nr - 2) ju = g.nr - 2;
-        int jt = (int)t;
-        R du = u - (R)ju, dt = t - (R)jt;
-        if (nd == 2) {
-            key[p] = ju * g.na + jt;
-            R dd = du * dt;
-            w[0] = (R)1 - du - dt + dd;
-            w[1] = dt - dd;
-            w[2] = du - dd;
-            w[3] = dd;
-        } else {
-            R zz = z + g.zm;
-            zz = zz / g.dzg;
-            int jz = (int)zz;
-            if (jz < 0) jz = 0;
-            if (jz > g.ngz - 2) jz = g.ngz - 2;
-            key[p] = (ju * g.ngz + jz) * g.na + jt;
-            R dz = zz - (R)jz;
-            w[0] = ((R)1 - dt) * ((R)1 - dz) * ((R)1 - du);
-            w[1] = dt * ((R)1 - dz) * ((R)1 - du);
-            w[2] = ((R)1 - dt) * dz * ((R)1 - du);
-            w[3] = dt * dz * ((R)1 - du);
-            w[4] = ((R)1 - dt) * ((R)1 - dz) * du;
-            w[5] = dt * ((R)1 - dz) * du;
-            w[6] = ((R)1 - dt) * dz * du;
-            w[7] = dt * dz * du;
-        }
-        on[p] = 1;
-    }
+    const int stride = 2 * g.ndim;
+#pragma omp parallel for schedule(static) num_threads(ox_threads) if (ox_threads > 1)
+    for (int64_t p = 0; p < n; p++)
+        on[p] = (uint8_t)F(weight1)(&g, old, pos + p * stride, key + p, wt + p * 8);
     return 0;
 }
 
@@ -374,23 +384,51 @@ int F(ox_massgn)(const GxConfig* c, int64_t n, const int32_t* key, const R* wt,
                  const uint8_t* on, R* mass, int32_t* jrk) {
     F(og) g;
     if (F(og_init)(c, &g)) return GX_ERR_ARG;
-    int32_t ic[8];
     const int div = (g.ndim == 2) ? g.na : g.na * g.ngz;
-    for (int64_t p = 0; p < n; p++) {
-        if (!on[p]) continue;
-        int j = key[p] / div;
-        if (j + 1 < jrk[0]) jrk[0] = j + 1;
-        if (j + 2 > jrk[1]) jrk[1] = j + 2;
-        int nc = F(corners)(&g, key[p], ic);
-        const R* w = wt + p * 8;
-        /* reference update order: w1, w3, w2, w4 (, w5, w7, w6, w8) */
-        static const int ord4[4] = {0, 2, 1, 3};
-        static const int ord8[8] = {0, 2, 1, 3, 4, 6, 5, 7};
-        const int* ord = (nc == 4) ? ord4 : ord8;
-        for (int k = 0; k < nc; k++) {
-            int cidx = ic[ord[k]];
-            if (cidx >= 0) mass[cidx] += w[ord[k]];
+    /* reference update order: w1, w3, w2, w4 (, w5, w7, w6, w8) */
+    static const int ord4[4] = {0, 2, 1, 3};
+    static const int ord8[8] = {0, 2, 1, 3, 4, 6, 5, 7};
+    const int nt = ox_threads;
+    /* threaded: each thread deposits a contiguous block of particles into
+     * its own array; the arrays are summed in thread order */
+    R* priv = (nt > 1) ? (R*)calloc((size_t)nt * g.mesh, sizeof(R)) : NULL;
+    int32_t jlo[256], khi[256];
+    for (int t = 0; t < nt && t < 256; t++) {
+        jlo[t] = jrk[0];
+        khi[t] = jrk[1];
+    }
+#pragma omp parallel num_threads(nt) if (nt > 1)
+    {
+        const int tid = OX_TID;
+        R* dst = priv ? priv + (size_t)tid * g.mesh : mass;
+        int64_t p0 = n * tid / nt, p1 = n * (tid + 1) / nt;
+        int32_t ic[8];
+        for (int64_t p = p0; p < p1; p++) {
+            if (!on[p]) continue;
+            int j = key[p] / div;
+            if (j + 1 < jlo[tid]) jlo[tid] = j + 1;
+            if (j + 2 > khi[tid]) khi[tid] = j + 2;
+            int nc = F(corners)(&g, key[p], ic);
+            const R* w = wt + p * 8;
+            const int* ord = (nc == 4) ? ord4 : ord8;
+            for (int k = 0; k < nc; k++) {
+                int cidx = ic[ord[k]];
+                if (cidx >= 0) dst[cidx] += w[ord[k]];
+            }
         }
+    }
+    for (int t = 0; t < nt; t++) {
+        if (jlo[t] < jrk[0]) jrk[0] = jlo[t];
+        if (khi[t] > jrk[1]) jrk[1] = khi[t];
+    }
+    if (priv) {
+#pragma omp parallel for schedule(static) num_threads(nt)
+        for (int64_t i = 0; i < g.mesh; i++) {
+            R v = mass[i];
+            for (int t = 0; t < nt; t++) v += priv[(size_t)t * g.mesh + i];
+            mass[i] = v;
+        }
+        free(priv);
     }
     return 0;
 }
@@ -438,8 +476,9 @@ int F(ox_findf)(const GxConfig* c, const R* G, const R* mass, int lpot, int jrs,
     R* spec = (R*)calloc((size_t)nr * nspec, sizeof(R));
     R* outs = (R*)calloc((size_t)nr * nspec, sizeof(R));
     R* row = (R*)malloc(sizeof(R) * (na > 2 * ngz ? na : 2 * ngz) * 2);
-    R* ca = (R*)malloc(sizeof(R) * ngz * ng); /* a_m(z) */
-    R* cb = (R*)malloc(sizeof(R) * ngz * ng); /* b_m(z) */
+    /* per-thread a_m(z), b_m(z) scratch */
+    R* ca_all = (R*)malloc(sizeof(R) * ngz * ng * ox_threads);
+    R* cb_all = (R*)malloc(sizeof(R) * ngz * ng * ox_threads);
     /* twiddles formed in FP64, rounded to R: azimuth [m][j], vertical [k][z] */
     R* acos_ = (R*)malloc(sizeof(R) * ng * na);
     R* asin_ = (R*)malloc(sizeof(R) * ng * na);
@@ -459,7 +498,10 @@ int F(ox_findf)(const GxConfig* c, const R* G, const R* mass, int lpot, int jrs,
         }
 #define SP(buf, ir, m, part, kz) buf[(((int64_t)(ir) * ng + (m)) * 4 + (part)) * nkz + (kz)]
     /* forward transforms of the active source rings */
+#pragma omp parallel for schedule(dynamic) num_threads(ox_threads) if (ox_threads > 1)
     for (int ir = jrs - 1; ir < krs; ir++) {
+        R* ca = ca_all + (size_t)OX_TID * ngz * ng;
+        R* cb = cb_all + (size_t)OX_TID * ngz * ng;
         for (int iz = 0; iz < ngz; iz++) {
             const R* x = mass + ((int64_t)ir * ngz + iz) * na;
             for (int m = 0; m < ng; m++) {
@@ -519,6 +561,7 @@ int F(ox_findf)(const GxConfig* c, const R* G, const R* mass, int lpot, int jrs,
             for (int kz = klo; kz <= khi; kz++) {
                 const int nvskip = (nd == 3) && (kz > 0 && kz < ngz);
                 const R* Gm = G + ((((int64_t)type * ng + m) * nkz + kz) * nr) * nr;
+#pragma omp parallel for schedule(static) num_threads(ox_threads) if (ox_threads > 1)
                 for (int ir = 0; ir < nr; ir++) {
                     R oAa = 0, oBa = 0, oAb = 0, oBb = 0;
                     for (int is = jrs - 1; is < krs; is++) {
@@ -557,7 +600,10 @@ int F(ox_findf)(const GxConfig* c, const R* G, const R* mass, int lpot, int jrs,
         }
         /* synthesis (p2fsyn.f:42-53 / p3fsyn.f:59-129) */
         const R scale = (nd == 3) ? (R)1 / (R)(2 * ngz * na) : (R)1 / (R)na;
+#pragma omp parallel for schedule(dynamic) num_threads(ox_threads) if (ox_threads > 1)
         for (int ir = 0; ir < nr; ir++) {
+            R* ca = ca_all + (size_t)OX_TID * ngz * ng;
+            R* cb = cb_all + (size_t)OX_TID * ngz * ng;
             /* vertical synthesis of each active row */
             for (int m = 0; m < ng; m++) {
                 if (g.lg[m]) continue;
@@ -598,8 +644,8 @@ int F(ox_findf)(const GxConfig* c, const R* G, const R* mass, int lpot, int jrs,
     free(spec);
     free(outs);
     free(row);
-    free(ca);
-    free(cb);
+    free(ca_all);
+    free(cb_all);
     free(acos_);
     free(asin_);
     free(zcos_);
@@ -639,14 +685,14 @@ int F(ox_grdacc)(const GxConfig* c, int64_t n, const R* pos, const R* fields, in
     if (F(og_init)(c, &g)) return GX_ERR_ARG;
     const int nd = g.ndim, stride = 2 * nd;
     const int64_t mesh = g.mesh;
-    int32_t ic[8];
+#pragma omp parallel for schedule(static) num_threads(ox_threads) if (ox_threads > 1)
     for (int64_t p = 0; p < n; p++) {
         const R* q = pos + p * stride;
         R a[3] = {0, 0, 0}, ph = 0;
         int32_t key;
         R w[8];
-        uint8_t on;
-        F(ox_weight)(c, 1, 1, q, &key, w, &on);
+        int32_t ic[8];
+        int on = F(weight1)(&g, 1, q, &key, w);
         if (on) {
             int nc = F(corners)(&g, key, ic);
             for (int i = 0; i < nd; i++) {
@@ -698,6 +744,7 @@ int F(ox_step)(const GxConfig* c, const R* G, int64_t n, R* pos, R* mass, int32_
         F(ox_findf)(c, G, mass, lpot, jrk[0], jrk[1], fl);
         F(ox_polcat)(c, fl);
         F(ox_grdacc)(c, n, pos, fl, 0, acc, NULL);
+#pragma omp parallel for schedule(static) num_threads(ox_threads) if (ox_threads > 1)
         for (int64_t p = 0; p < n; p++) {
             R* q = pos + p * stride;
             for (int i = 0; i < nd; i++) {
@@ -710,6 +757,28 @@ int F(ox_step)(const GxConfig* c, const R* G, int64_t n, R* pos, R* mass, int32_
     free(acc);
     if (!fields) free(fl);
     return 0;
+}
+
+/* the particle loop of step (SRC/lib15/step.f:186-242) for one step over
+ * pos with given Cartesian fields: getacc, stpgrp, then massgn + scaled of
+ * the new positions into mass (zeroed here) */
+int F(ox_particle_pass)(const GxConfig* c, int64_t n, R* pos, const R* fields, R* mass,
+                        int32_t* jrk) {
+    F(og) g;
+    if (F(og_init)(c, &g)) return GX_ERR_ARG;
+    const int nd = g.ndim, stride = 2 * nd;
+    R* acc = (R*)malloc(sizeof(R) * nd * (n ? n : 1));
+    F(ox_grdacc)(c, n, pos, fields, 0, acc, NULL);
+#pragma omp parallel for schedule(static) num_threads(ox_threads) if (ox_threads > 1)
+    for (int64_t p = 0; p < n; p++) {
+        R* q = pos + p * stride;
+        for (int i = 0; i < nd; i++) {
+            q[nd + i] = q[nd + i] + acc[p * nd + i];
+            q[i] = q[i] + q[nd + i];
+        }
+    }
+    free(acc);
+    return F(ox_masset)(c, n, pos, mass, jrk);
 }
 
 /* ------------------------------------------------------------------ */

@@ -54,8 +54,10 @@ def _setup(L):
         getattr(L, "ox_masset_" + s).argtypes = [C.POINTER(GxConfig), i64, P, P, P]
         getattr(L, "ox_step_" + s).argtypes = [C.POINTER(GxConfig), P, i64, P, P, P, C.c_int,
                                                C.c_int, P]
+        getattr(L, "ox_particle_pass_" + s).argtypes = [C.POINTER(GxConfig), i64, P, P, P, P]
         getattr(L, "ox_direct_field_" + s).argtypes = [C.POINTER(GxConfig), P, C.c_int, P, P,
                                                        P, P, C.c_int, P]
+    L.ox_set_threads.argtypes = [C.c_int]
     L.ox_icheck.argtypes = [C.POINTER(GxConfig), i64, P, P, P, C.c_double, C.POINTER(GxDiag)]
 
 
@@ -70,6 +72,11 @@ def _dt(prec):
 def _chk(rc, what):
     if rc != 0:
         raise RuntimeError(f"oracle {what} failed with {rc}")
+
+
+def set_threads(n):
+    """Host threads of the restated loops (1 = sequential reference order)."""
+    return lib().ox_set_threads(int(n))
 
 
 def geometry(cfg):
@@ -165,6 +172,20 @@ def step(cfg, G, pos, nsteps, phys=False, prec=64):
     _chk(getattr(lib(), "ox_step_" + s)(C.byref(cfg), _p(G), pos.shape[0], _p(pos), _p(mass),
                                          _p(jrk), nsteps, int(phys), _p(f)), "step")
     return pos, mass, f
+
+
+def particle_pass(cfg, pos, fields, prec=32):
+    """One step's particle loop in place on pos (grdacc, stpgrp, massgn,
+    scaled); returns the new mass array and ring range."""
+    dt, s = _dt(prec)
+    assert pos.dtype == dt and pos.flags.c_contiguous
+    g = geometry(cfg)
+    mass = np.zeros(g.mesh, dt)
+    jrk = np.zeros(2, np.int32)
+    fields = np.ascontiguousarray(fields, dtype=dt)
+    _chk(getattr(lib(), "ox_particle_pass_" + s)(C.byref(cfg), pos.shape[0], _p(pos), _p(fields),
+                                                  _p(mass), _p(jrk)), "particle_pass")
+    return mass, (int(jrk[0]), int(jrk[1]))
 
 
 def direct_field(cfg, D, masses, lpot=True, prec=64):

