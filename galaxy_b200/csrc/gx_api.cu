@@ -164,7 +164,12 @@ static int alloc_grids(GxCtx* c) {
         DALLOC(c, c->specO, 4 * nspec);
         DALLOC(c, c->rowstart, (size_t)g.nrow + 2);
         DALLOC(c, c->rowitem, (size_t)g.nrow + 2);
+        DALLOC(c, c->rowcnt, (size_t)NCOPY * (g.nrow + 1));
+        DALLOC(c, c->rowfill, (size_t)NCOPY * (g.nrow + 1));
+        DALLOC(c, c->rowbase, (size_t)NCOPY * (g.nrow + 1));
+        DALLOC(c, c->rowtot, (size_t)g.nrow + 1);
         DALLOC(c, c->nitems_d, 4);
+        GX_CUDA(c, cudaMemsetAsync(c->rowcnt, 0, sizeof(uint32_t) * NCOPY * (g.nrow + 1), c->stream));
     }
     DALLOC(c, c->jrk_d, 4);
     DALLOC(c, c->errword, 4);
@@ -221,9 +226,9 @@ void gx_destroy(GxCtx* c) {
     void* ptrs[] = {c->green32, c->green64, c->pbuf[0], c->pbuf[1], c->perm, c->origin,
                     c->origin_tmp, c->pkey, c->p64, c->key64, c->w64, c->acc64, c->ppot,
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
-                    c->specS, c->specO, c->spec64, c->out64, c->sb.keys[0], c->sb.keys[1],
-                    c->sb.vals[0], c->sb.vals[1], c->sb.hist, c->sb.dtotal, c->rowstart,
-                    c->items, c->nitems_d, c->rowitem, c->stage, c->jrk_d, c->errword, c->dsum};
+                    c->specS, c->specO, c->syntab, c->synR, c->spec64, c->out64, c->perm_next, c->rowstart,
+                    c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->stage, c->jrk_d,
+                    c->errword, c->dsum};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i <= GX_NPHASE; i++)
@@ -340,8 +345,7 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     if (n <= c->cap && c->cap > 0) return GX_OK;
     // grow: free old
     void* old[] = {c->pbuf[0], c->pbuf[1], c->perm, c->origin, c->origin_tmp, c->pkey, c->p64,
-                   c->key64, c->w64, c->acc64, c->ppot, c->pacc, c->sb.keys[0], c->sb.keys[1],
-                   c->sb.vals[0], c->sb.vals[1], c->sb.hist, c->sb.dtotal, c->items, c->stage};
+                   c->key64, c->w64, c->acc64, c->ppot, c->pacc, c->perm_next, c->items, c->stage};
     for (void* p : old)
         if (p) cudaFree(p);
     c->pbuf[0] = c->pbuf[1] = nullptr;
@@ -351,9 +355,7 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     c->key64 = nullptr;
     c->w64 = c->acc64 = nullptr;
     c->ppot = c->pacc = nullptr;
-    c->sb.keys[0] = c->sb.keys[1] = nullptr;
-    c->sb.vals[0] = c->sb.vals[1] = nullptr;
-    c->sb.hist = c->sb.dtotal = nullptr;
+    c->perm_next = nullptr;
     c->items = nullptr;
     c->stage = nullptr;
     int64_t cap = std::max<int64_t>(n, 1);
@@ -373,30 +375,9 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     DALLOC(c, c->origin, cap);
     DALLOC(c, c->origin_tmp, cap);
     DALLOC(c, c->pkey, cap);
-    // sort scratch: keys are ring-plane rows (plus one off-grid row)
-    SortBufs& sb = c->sb;
-    int nrow = c->g.nrow;
-    int bits = 1;
-    while ((1 << bits) < nrow + 1) bits++;
-    sb.bits = bits;
-    sb.npass = (bits + 7) / 8;
-    int base = bits / sb.npass, extra = bits % sb.npass, sh = 0;
-    for (int p = 0; p < sb.npass; p++) {
-        sb.pass_bits[p] = base + (p < extra ? 1 : 0);
-        sb.pass_shift[p] = sh;
-        sh += sb.pass_bits[p];
-    }
-    sb.tile = 4096;
-    sb.ntile = (int)((cap + sb.tile - 1) / sb.tile);
-    DALLOC(c, sb.keys[0], cap);
-    DALLOC(c, sb.keys[1], cap);
-    DALLOC(c, sb.vals[0], cap);
-    DALLOC(c, sb.vals[1], cap);
-    DALLOC(c, sb.hist, (size_t)256 * sb.ntile);
-    DALLOC(c, sb.dtotal, 256);
-    // deposit work items: every row once plus one per CH particles
-    const int CH = 2048;
-    c->maxitems = nrow + 1 + (int)((cap + CH - 1) / CH);
+    DALLOC(c, c->perm_next, cap);
+    // deposit work items: every row once plus one per DEP_CH particles
+    c->maxitems = c->g.nrow + 1 + (int)((cap + DEP_CH - 1) / DEP_CH);
     DALLOC(c, c->items, (size_t)3 * c->maxitems);
     int nq = (c->g.ndim == 3) ? 4 : 2;
     DALLOC(c, c->stage, (size_t)c->maxitems * nq * c->g.na);

@@ -13,6 +13,12 @@
 #define GX_PI 3.141592653589793238462643
 
 // ---------------------------------------------------------------------------
+// particles per deposit work item (bounds the fixed-point bin sums)
+#define DEP_CH 1024
+// striped copies of the row counters (copy = block index mod NCOPY); spreads
+// the integer atomics of row-sorted particles over NCOPY addresses per row
+#define NCOPY 32
+
 // Phases of a step timed in profile mode
 #define GX_NPHASE 8
 enum { PH_FWD = 0, PH_CONV, PH_SYN, PH_PUSH, PH_SORT, PH_DEPOSIT, PH_COMBINE, PH_OTHER };
@@ -33,20 +39,6 @@ struct DevGeo {
 struct Spec {
     int nact;        // number of active harmonics
     int m[260];      // their m values, ascending
-};
-
-// Deposit scratch sizes
-struct SortBufs {
-    uint32_t* keys[2];
-    int32_t* vals[2];
-    uint32_t* hist;     // [nbucket][ntile]
-    uint32_t* dtotal;   // [nbucket]
-    int tile;           // items per tile
-    int ntile;
-    int bits;           // bits sorted (row digits)
-    int npass;
-    int pass_bits[4];
-    int pass_shift[4];
 };
 
 struct GxCtx {
@@ -73,9 +65,10 @@ struct GxCtx {
     float* pbuf[2] = {nullptr, nullptr};   // SoA [2*ndim][cap] (mixed path)
     int cur = 0;
     int32_t* perm = nullptr;               // processing order of pbuf[cur]
+    int32_t* perm_next = nullptr;          // permutation being built by the deposit
     int32_t* origin = nullptr;             // original load index of pbuf[cur][i]
     int32_t* origin_tmp = nullptr;
-    uint32_t* pkey = nullptr;              // per-particle keys from the last pass
+    uint32_t* pkey = nullptr;              // per-particle rows from the last pass
     double* p64 = nullptr;                 // SoA [2*ndim][cap] (FP64 path)
     int32_t* key64 = nullptr;
     double* w64 = nullptr;                 // [8][cap]
@@ -92,6 +85,8 @@ struct GxCtx {
     double* polar64 = nullptr;             // [4][mesh]
     float4* specS = nullptr;               // forward spectrum [nact][nkz][nr]
     float4* specO = nullptr;               // convolved [4][nact][nkz][nr]
+    float* syntab = nullptr;               // synthesis twiddle tables (gx_synth.cu)
+    float* synR = nullptr;                 // vertically synthesised rows [4][nr][ngz][ncp]
     double* spec64 = nullptr;
     double* out64 = nullptr;
     bool have_mass = false;
@@ -100,12 +95,15 @@ struct GxCtx {
     int jrs = 1, krs = 0;                  // active source ring range (1-based)
 
     // deposit
-    SortBufs sb{};
     int32_t* rowstart = nullptr;           // [nrow + 1]
     int32_t* items = nullptr;              // work items [maxitems][3]: row, start, end
     int32_t* nitems_d = nullptr;
     int32_t* rowitem = nullptr;            // [nrow + 1] first work item of each row
-    float* stage = nullptr;                // [maxitems][NQ][na]
+    int32_t* stage = nullptr;              // [maxitems][NQ][na] fixed-point rows
+    uint32_t* rowcnt = nullptr;            // [NCOPY][nrow + 1] particles per row (zeroed after use)
+    uint32_t* rowfill = nullptr;           // [NCOPY][nrow + 1] slots handed out per row
+    uint32_t* rowbase = nullptr;           // [NCOPY][nrow + 1] offset of each copy in its row
+    uint32_t* rowtot = nullptr;            // [nrow + 1] particles per row
     int maxitems = 0;
     int32_t* jrk_d = nullptr;              // device min/max ring
     int32_t* errword = nullptr;            // device error word
@@ -286,6 +284,19 @@ __device__ __forceinline__ int gx_corners(const DevGeo& g, int key, int* ic) {
     return 8;
 }
 
+__device__ __forceinline__ uint32_t lanemask_lt() {
+    uint32_t m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// warp-aggregated count of row (all 32 lanes must call)
+__device__ __forceinline__ void gx_row_count(uint32_t row, bool act, uint32_t* __restrict__ cnt) {
+    const uint32_t am = __ballot_sync(0xffffffffu, act);
+    const uint32_t peers = __match_any_sync(0xffffffffu, act ? row : 0xffffffffu) & am;
+    if (act && (peers & lanemask_lt()) == 0) atomicAdd(&cnt[row], (uint32_t)__popc(peers));
+}
+
 // ---------------------------------------------------------------------------
 // host-side entry points implemented in the .cu files
 int gx_green_build_dev(GxCtx* c);
@@ -299,7 +310,8 @@ int gx_fp64_masset(GxCtx* c);
 int gx_fp64_findf(GxCtx* c, int lpot, bool polcat);
 int gx_fp64_getacc(GxCtx* c, float* acc, float* pot);
 int gx_fp64_step(GxCtx* c, int nsteps, int phys);
-int gx_mass_dense_from_stage(GxCtx* c);
+int gx_deposit_rows(GxCtx* c, const float* P, const uint32_t* rowkey, int32_t* perm_out);
 int gx_comm_reduce_range(GxCtx* c);
+int gx_synthesis(GxCtx* c, int tmask, float* polar);
 int gx_comm_reduce_spectrum(GxCtx* c);
 void gx_comm_destroy(GxCtx* c);

@@ -1,0 +1,283 @@
+// gx_deposit.cu -- deterministic mass assignment of the mixed path.
+//
+// massgn (SRC/lib15/massgn.f:68-89 p2d, 140-172 p3d) scatter-adds the 4 / 8
+// weights of every particle into the mesh.  Here:
+//
+//   1. counting sort of the cell keys by their ring-plane row (one radix
+//      digit of the key, ncl = (ju*ngz + jz)*na + jt + 1): the particle pass
+//      counts its new rows with warp-aggregated integer atomics (k_push),
+//      k_row_scan turns the counts into row starts, k_place gives every
+//      particle its slot in the row-ordered permutation;
+//   2. owner-computes deposit: a work item is up to DEP_CH particles of one
+//      base row; the CTA recomputes each particle's cell and weights and adds
+//      them, as 2^-20 fixed-point integers, into shared-memory bins of the 4
+//      (2D: 2) output rows the base row feeds (same row, plane above, ring
+//      above, both); bins are staged per item as int32 rows;
+//   3. k_mass_combine sums, per mesh row, the staged rows of the base rows
+//      that feed it in int64 and converts once (x pmass, scaled.f:89-92).
+//
+// Every sum is an integer sum, so the mass array is bitwise reproducible
+// whatever order the atomics resolve in; no floating-point atomics are used.
+// The fixed-point quantum is 2^-20 of one particle's mass (9.5e-7); a bin
+// holds at most DEP_CH (1 + 1e-6) 2^20 < 2^31 (each particle feeds one bin
+// per (output row, weight)), so int32 never overflows.
+#include <algorithm>
+
+#include "gx_common.cuh"
+
+#define FIXQ 1048576.0f  // 2^20
+
+// per row: total over the counter copies, each copy's offset in the row;
+// clears the counters for the next pass
+__global__ void k_row_reduce(int nrow, uint32_t* __restrict__ rowcnt, uint32_t* __restrict__ rowfill,
+                             uint32_t* __restrict__ rowbase, uint32_t* __restrict__ rowtot) {
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r > nrow) return;
+    const size_t st = (size_t)nrow + 1;
+    uint32_t run = 0;
+#pragma unroll 8
+    for (int c = 0; c < NCOPY; c++) {
+        const uint32_t v = rowcnt[c * st + r];
+        rowbase[c * st + r] = run;
+        run += v;
+        rowcnt[c * st + r] = 0;
+        rowfill[c * st + r] = 0;
+    }
+    rowtot[r] = run;
+}
+
+// row totals -> row starts, deposit work items, active ring range.  One CTA.
+__global__ void k_row_scan(int nrow, int ngz, int nr, const uint32_t* __restrict__ rowcnt,
+                           int32_t* __restrict__ rowstart,
+                           int32_t* __restrict__ rowitem, int32_t* __restrict__ items,
+                           int32_t* __restrict__ nitems, int32_t* __restrict__ jrk) {
+    __shared__ int32_t ws_a[32], ws_b[32];
+    __shared__ int32_t carry_a, carry_b, rmin, rmax;
+    if (threadIdx.x == 0) {
+        carry_a = carry_b = 0;
+        rmin = 0x7fffffff;
+        rmax = -1;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    // rows 0 .. nrow (row nrow collects particles off the grid)
+    for (int base = 0; base <= nrow; base += blockDim.x) {
+        const int r = base + threadIdx.x;
+        const int cnt = (r <= nrow) ? (int)rowcnt[r] : 0;
+        const int nit = (r < nrow) ? (cnt + DEP_CH - 1) / DEP_CH : 0;
+        if (r < nrow && cnt > 0) {
+            atomicMin(&rmin, r);
+            atomicMax(&rmax, r);
+        }
+        int xa = cnt, xb = nit;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int ya = __shfl_up_sync(0xffffffffu, xa, o);
+            int yb = __shfl_up_sync(0xffffffffu, xb, o);
+            if (lane >= o) {
+                xa += ya;
+                xb += yb;
+            }
+        }
+        if (lane == 31) {
+            ws_a[warp] = xa;
+            ws_b[warp] = xb;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            int sa = (lane < nw) ? ws_a[lane] : 0, sb = (lane < nw) ? ws_b[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int ya = __shfl_up_sync(0xffffffffu, sa, o);
+                int yb = __shfl_up_sync(0xffffffffu, sb, o);
+                if (lane >= o) {
+                    sa += ya;
+                    sb += yb;
+                }
+            }
+            if (lane < nw) {
+                ws_a[lane] = sa;
+                ws_b[lane] = sb;
+            }
+        }
+        __syncthreads();
+        const int ea = carry_a + ((warp > 0) ? ws_a[warp - 1] : 0) + xa - cnt;
+        const int eb = carry_b + ((warp > 0) ? ws_b[warp - 1] : 0) + xb - nit;
+        if (r <= nrow) rowstart[r] = ea;
+        if (r < nrow) {
+            rowitem[r] = eb;
+            for (int q = 0; q < nit; q++) {
+                int it = eb + q;
+                items[3 * it + 0] = r;
+                items[3 * it + 1] = ea + q * DEP_CH;
+                items[3 * it + 2] = min(ea + (q + 1) * DEP_CH, ea + cnt);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            carry_a += ws_a[nw - 1];
+            carry_b += ws_b[nw - 1];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        rowstart[nrow + 1] = carry_a;
+        rowitem[nrow] = carry_b;
+        *nitems = carry_b;
+        // 1-based ring range as massgn tracks it (jrad = j + 1, krad = j + 2)
+        if (rmax >= 0) {
+            jrk[0] = rmin / ngz + 1;
+            jrk[1] = min(rmax / ngz + 2, nr);
+        } else {
+            jrk[0] = nr;
+            jrk[1] = 0;
+        }
+    }
+}
+
+// slot of every particle in the row-ordered permutation: perm[slot] = t
+__global__ void k_place(const uint32_t* __restrict__ rowkey, int64_t n, int nrow,
+                        const int32_t* __restrict__ rowstart, const uint32_t* __restrict__ rowbase,
+                        uint32_t* __restrict__ rowfill, int32_t* __restrict__ perm) {
+    // same block -> counter-copy map as the pass that counted the rows
+    const size_t co = (size_t)(blockIdx.x & (NCOPY - 1)) * (nrow + 1);
+    rowfill += co;
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool act = t < n;
+    const uint32_t row = act ? rowkey[t] : 0xffffffffu;
+    const uint32_t am = __ballot_sync(0xffffffffu, act);
+    const uint32_t peers = __match_any_sync(0xffffffffu, row) & am;
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0;
+    if (act && (int)(threadIdx.x & 31) == leader) base = atomicAdd(&rowfill[row], (uint32_t)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader < 0 ? 0 : leader);
+    if (act) perm[rowstart[row] + rowbase[co + row] + base + __popc(peers & lanemask_lt())] = (int32_t)t;
+}
+
+// owner-computes deposit of one work item per CTA iteration
+template <int NW>
+__global__ void __launch_bounds__(256) k_deposit(DevGeo g, const int32_t* __restrict__ items,
+                                                 const int32_t* __restrict__ nitems,
+                                                 const float* __restrict__ P, int64_t cap,
+                                                 const int32_t* __restrict__ perm,
+                                                 int32_t* __restrict__ stage,
+                                                 int32_t* __restrict__ errword) {
+    extern __shared__ __align__(16) int32_t bins[];  // [NW][na]
+    const int na = g.na;
+    constexpr int NQ = NW / 2;
+    const int nit = *nitems;
+    const float* X = P;
+    const float* Y = P + cap;
+    const float* Z = (g.ndim == 3) ? P + 2 * cap : nullptr;
+    for (int item = blockIdx.x; item < nit; item += gridDim.x) {
+        const int row = items[3 * item], s0 = items[3 * item + 1], s1 = items[3 * item + 2];
+        for (int i = threadIdx.x; i < NW * na; i += blockDim.x) bins[i] = 0;
+        __syncthreads();
+        for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
+            const int p = perm[s];
+            const float z = Z ? Z[p] : 0.f;
+            const CellW cw = gx_cell(g, X[p], Y[p], z, false);
+            if (cw.key < 0 || cw.key / na != row) {
+                atomicExch(errword, 1);
+                continue;
+            }
+            const int jt = cw.key - row * na;
+            float w[8];
+            gx_weights(g, cw, w);
+#pragma unroll
+            for (int k = 0; k < NW; k++) atomicAdd(&bins[k * na + jt], __float2int_rn(w[k] * FIXQ));
+        }
+        __syncthreads();
+        // output row q gets the lo weight at j and the hi weight from j - 1
+        int32_t* dst = stage + (size_t)item * NQ * na;
+        for (int i = threadIdx.x; i < NQ * na; i += blockDim.x) {
+            const int q = i / na, j = i - q * na;
+            const int jm = (j == 0) ? na - 1 : j - 1;
+            dst[i] = bins[(2 * q) * na + j] + bins[(2 * q + 1) * na + jm];
+        }
+        __syncthreads();
+    }
+}
+
+// mass[R][j] = pmass 2^-20 (sum over the base rows R, R-1, R-ngz, R-ngz-1)
+__global__ void k_mass_combine(DevGeo g, const int32_t* __restrict__ stage,
+                               const int32_t* __restrict__ rowitem, float* __restrict__ mass) {
+    const int na = g.na, nrow = g.nrow;
+    const int NQ = (g.ndim == 3) ? 4 : 2;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= (int64_t)nrow * na) return;
+    const int R = (int)(i / na), j = (int)(i - (int64_t)R * na);
+    const int off[4] = {0, 1, g.ngz, g.ngz + 1};
+    long long v = 0;
+    for (int q = 0; q < NQ; q++) {
+        const int B = R - off[q];
+        if (B < 0) continue;
+        for (int it = rowitem[B]; it < rowitem[B + 1]; it++) v += stage[((size_t)it * NQ + q) * na + j];
+    }
+    mass[i] = (float)((double)v * (1.0 / (double)FIXQ)) * g.pmass;
+}
+
+__global__ void k_row_keys(DevGeo g, const float* __restrict__ P, int64_t cap, int64_t n,
+                           uint32_t* __restrict__ rowkey, uint32_t* __restrict__ rowcnt) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const bool act = i < n;
+    uint32_t row = 0;
+    if (act) {
+        const float z = (g.ndim == 3) ? P[2 * cap + i] : 0.f;
+        const CellW c = gx_cell(g, P[i], P[cap + i], z, false);
+        row = (c.key >= 0) ? (uint32_t)(c.key / g.na) : (uint32_t)g.nrow;
+        rowkey[i] = row;
+    }
+    gx_row_count(row, act, rowcnt + (size_t)(blockIdx.x & (NCOPY - 1)) * (g.nrow + 1));
+}
+
+// rows counted by the caller's pass -> permutation, deposit, mass
+int gx_deposit_rows(GxCtx* c, const float* P, const uint32_t* rowkey, int32_t* perm_out) {
+    const DevGeo& g = c->g;
+    const int64_t n = c->n;
+    int rc = gx_phase_mark(c, PH_SORT);
+    if (rc) return rc;
+    k_row_reduce<<<(g.nrow + 1 + 255) / 256, 256, 0, c->stream>>>(g.nrow, c->rowcnt, c->rowfill,
+                                                                  c->rowbase, c->rowtot);
+    GX_LAUNCHED(c);
+    k_row_scan<<<1, 1024, 0, c->stream>>>(g.nrow, g.ngz, g.nr, c->rowtot, c->rowstart, c->rowitem,
+                                          c->items, c->nitems_d, c->jrk_d);
+    GX_LAUNCHED(c);
+    if (n > 0) {
+        k_place<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(rowkey, n, g.nrow, c->rowstart,
+                                                                  c->rowbase, c->rowfill, perm_out);
+        GX_LAUNCHED(c);
+    }
+    rc = gx_phase_mark(c, PH_DEPOSIT);
+    if (rc) return rc;
+    const int nw = (g.ndim == 3) ? 8 : 4;
+    const size_t sm = sizeof(int32_t) * (size_t)nw * g.na;
+    const int grid = std::min(c->maxitems, 148 * 16);
+    if (nw == 8)
+        k_deposit<8><<<grid, 256, sm, c->stream>>>(g, c->items, c->nitems_d, P, c->cap, perm_out,
+                                                   c->stage, c->errword);
+    else
+        k_deposit<4><<<grid, 256, sm, c->stream>>>(g, c->items, c->nitems_d, P, c->cap, perm_out,
+                                                   c->stage, c->errword);
+    GX_LAUNCHED(c);
+    rc = gx_phase_mark(c, PH_COMBINE);
+    if (rc) return rc;
+    const int64_t tot = (int64_t)g.nrow * g.na;
+    k_mass_combine<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(g, c->stage, c->rowitem,
+                                                                       c->mass);
+    GX_LAUNCHED(c);
+    return GX_OK;
+}
+
+int gx_mixed_masset(GxCtx* c) {
+    const DevGeo& g = c->g;
+    const int64_t n = c->n;
+    if (n > 0) {
+        k_row_keys<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(g, c->pbuf[c->cur], c->cap, n,
+                                                                      c->pkey, c->rowcnt);
+        GX_LAUNCHED(c);
+    }
+    int rc = gx_deposit_rows(c, c->pbuf[c->cur], c->pkey, c->perm);
+    if (rc) return rc;
+    return gx_phase_end(c);
+}

@@ -10,11 +10,7 @@
 //                     (harmonic, vertical wavenumber) the dense radial
 //                     contraction with the FP32 Green table of each field
 //                     type, the Green matrix streamed from HBM once per step.
-//   k_syn3 / k_syn2   p3fsyn.f:59-129 / p2fsyn.f:34-56 fused with polcat
-//                     (polcat.f:22-41): inverse vertical DFT, inverse
-//                     azimuthal DFT with the 1/(2 ngz na) (1/na) scale, then
-//                     the rotation to Cartesian components, written as one
-//                     float4 (fx, fy, fz, phi) per mesh node.
+//   synthesis         p3fsyn.f / p2fsyn.f fused with polcat: gx_synth.cu.
 // FFTPACK conventions (SRC/utils/sfftpack): forward a_m = sum x cos,
 // b_m = -sum x sin; backward x_j = a_0 + (-1)^j a_N + 2 sum (a cos - b sin).
 #include <algorithm>
@@ -69,25 +65,6 @@ __device__ void build_taz(float* T, int na, int nact, int ncp) {
             v = (c & 1) ? -s : co;
         }
         T[i] = v;
-    }
-}
-
-// inverse azimuthal twiddles with the synthesis scale: Ti[c][j]
-__device__ void build_tazi(float* Ti, int na, int nact, int ncp, int mmax, float scale) {
-    for (int i = threadIdx.x; i < ncp * na; i += blockDim.x) {
-        int c = i / na, j = i - c * na;
-        float v = 0.f;
-        if (c < 2 * nact) {
-            int m = c_act_m[c >> 1];
-            int idx = (int)(((int64_t)m * j) % na);
-            float s, co;
-            sincospif(2.0f * (float)idx / (float)na, &s, &co);
-            if (m == 0) v = (c & 1) ? 0.f : 1.f;
-            else if (m == mmax - 1) v = (c & 1) ? 0.f : ((j & 1) ? -1.f : 1.f);
-            else v = (c & 1) ? -2.f * s : 2.f * co;
-            v *= scale;
-        }
-        Ti[i] = v;
     }
 }
 
@@ -288,140 +265,6 @@ __global__ void __launch_bounds__(256) k_conv(DevGeo g, int nact, int tmask,
 }
 
 // ---------------------------------------------------------------------------
-// synthesis epilogue shared by 2D and 3D: F_t[row][j] = sum_c R_t[row][c] Ti[c][j]
-// for the 4 types at once, then polcat, one float4 store per node.
-__device__ __forceinline__ void syn_final(const DevGeo& g, int ncp, int nrows, const float* R,
-                                          int ldr_t, const float* Ti, float4* __restrict__ dst,
-                                          size_t row_stride, float* __restrict__ polar,
-                                          size_t polar_off, size_t mesh, int tmask) {
-    const int na = g.na;
-    const int nj4 = na >> 2;
-    for (int t = threadIdx.x; t < nrows * nj4; t += blockDim.x) {
-        const int row = t / nj4, j0 = (t - row * nj4) * 4;
-        float acc[4][4];
-#pragma unroll
-        for (int a = 0; a < 4; a++)
-#pragma unroll
-            for (int b = 0; b < 4; b++) acc[a][b] = 0.f;
-        for (int c = 0; c < ncp; c++) {
-            const float4 w = *reinterpret_cast<const float4*>(Ti + (size_t)c * na + j0);
-#pragma unroll
-            for (int ty = 0; ty < 4; ty++) {
-                const float r = R[ty * ldr_t + row * ncp + c];
-                acc[ty][0] += r * w.x; acc[ty][1] += r * w.y;
-                acc[ty][2] += r * w.z; acc[ty][3] += r * w.w;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int j = j0 + q;
-            float s, co;
-            // polcat angle t = 2 pi (j) / na
-            sincospif(2.0f * (float)j / (float)na, &s, &co);
-            const float fr = acc[0][q], ft = acc[1][q];
-            const float fz = (tmask & 4) ? acc[2][q] : 0.f, ph = (tmask & 8) ? acc[3][q] : 0.f;
-            dst[row * row_stride + j] = make_float4(fr * co - ft * s, fr * s + ft * co, fz, ph);
-            if (polar) {
-                size_t o = polar_off + row * row_stride + j;
-                polar[o] = fr;
-                polar[mesh + o] = ft;
-                polar[2 * mesh + o] = fz;
-                polar[3 * mesh + o] = ph;
-            }
-        }
-    }
-}
-
-#define ZCH 32
-__global__ void k_syn3(DevGeo g, int nact, int ncp, int tmask, const float4* __restrict__ O,
-                       float4* __restrict__ F, float* __restrict__ polar) {
-    extern __shared__ __align__(16) float sm[];
-    const int na = g.na, ngz = g.ngz, nkz = g.nkz, nr = g.nr;
-    const int ir = blockIdx.x, z0 = blockIdx.y * ZCH;
-    const int nz = min(ZCH, ngz - z0);
-    const int K2 = 2 * nkz, ldz = ru4(K2) + 1;
-    float* Tinv = sm;                          // [ZCH][ldz]
-    float* Zc = Tinv + ZCH * ldz;              // [ru4(K2)][ncp]
-    float* R = Zc + ru4(K2) * ncp;             // [4][ZCH][ncp]
-    float* Ti = R + 4 * ZCH * ncp;             // [ncp][na]
-    for (int i = threadIdx.x; i < ZCH * ldz; i += blockDim.x) {
-        int zr = i / ldz, r = i - zr * ldz;
-        int z = z0 + zr, k = r >> 1;
-        float v = 0.f;
-        if (zr < nz && r < K2) {
-            if ((r & 1) == 0) {
-                if (k == 0) v = 1.f;
-                else if (k == ngz) v = (z & 1) ? -1.f : 1.f;
-                else {
-                    int idx = (int)(((int64_t)k * z) % (2 * ngz));
-                    v = 2.f * cospif((float)idx / (float)ngz);
-                }
-            } else if (k > 0 && k < ngz) {
-                int idx = (int)(((int64_t)k * z) % (2 * ngz));
-                v = -2.f * sinpif((float)idx / (float)ngz);
-            }
-        }
-        Tinv[i] = v;
-    }
-    build_tazi(Ti, na, nact, ncp, g.mmax, 1.0f / (float)(2 * ngz * na));
-    for (int i = threadIdx.x; i < 4 * ZCH * ncp; i += blockDim.x) R[i] = 0.f;
-    __syncthreads();
-    for (int t = 0; t < 4; t++) {
-        if (!((tmask >> t) & 1)) continue;
-        for (int i = threadIdx.x; i < ru4(K2) * ncp; i += blockDim.x) {
-            int r = i / ncp, c = i - r * ncp;
-            int k = r >> 1, a = c >> 1;
-            float v = 0.f;
-            if (k < nkz && a < nact) {
-                float4 o = O[(((size_t)t * nact + a) * nkz + k) * nr + ir];
-                // rows: 2k -> A, 2k+1 -> B; cols: 2a -> a-row, 2a+1 -> b-row
-                v = (c & 1) ? ((r & 1) ? o.w : o.z) : ((r & 1) ? o.y : o.x);
-            }
-            Zc[i] = v;
-        }
-        __syncthreads();
-        float* Rt = R + t * ZCH * ncp;
-        sgemm44(nz, ncp, K2, Tinv, ldz, Zc, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
-#pragma unroll
-            for (int i = 0; i < 4; i++)
-                if (r0 + i < ZCH)
-#pragma unroll
-                    for (int j = 0; j < 4; j++) Rt[(r0 + i) * ncp + c0 + j] = acc[i][j];
-        });
-        __syncthreads();
-    }
-    const size_t mesh = g.mesh;
-    float4* dst = F + ((size_t)ir * ngz + z0) * na;
-    syn_final(g, ncp, nz, R, ZCH * ncp, Ti, dst, (size_t)na, polar,
-              ((size_t)ir * ngz + z0) * na, mesh, tmask);
-}
-
-__global__ void k_syn2(DevGeo g, int nact, int ncp, int tmask, const float4* __restrict__ O,
-                       float4* __restrict__ F, float* __restrict__ polar) {
-    extern __shared__ __align__(16) float sm[];
-    const int na = g.na, nr = g.nr;
-    const int ir0 = blockIdx.x * RB2;
-    const int nrows = min(RB2, nr - ir0);
-    float* R = sm;                    // [4][RB2][ncp]
-    float* Ti = R + 4 * RB2 * ncp;    // [ncp][na]
-    build_tazi(Ti, na, nact, ncp, g.mmax, 1.0f / (float)na);
-    for (int i = threadIdx.x; i < 4 * RB2 * ncp; i += blockDim.x) {
-        int t = i / (RB2 * ncp), rem = i - t * RB2 * ncp;
-        int r = rem / ncp, c = rem - r * ncp;
-        int a = c >> 1, ir = ir0 + r;
-        float v = 0.f;
-        if (((tmask >> t) & 1) && a < nact && ir < nr) {
-            float4 o = O[((size_t)t * nact + a) * nr + ir];
-            v = (c & 1) ? o.z : o.x;
-        }
-        R[i] = v;
-    }
-    __syncthreads();
-    syn_final(g, ncp, nrows, R, RB2 * ncp, Ti, F + (size_t)ir0 * na, (size_t)na, polar,
-              (size_t)ir0 * na, (size_t)g.mesh, tmask);
-}
-
-// ---------------------------------------------------------------------------
 static int set_act(GxCtx* c) {
     GX_CUDA(c, cudaMemcpyToSymbolAsync(c_act_m, c->spec.m, sizeof(int) * 260, 0,
                                        cudaMemcpyHostToDevice, c->stream));
@@ -433,12 +276,6 @@ static size_t fwd3_smem(const DevGeo& g, int ncp) {
     int r0sz = std::max(ru4(g.ngz) * ldx, ru4(2 * g.nkz) * g.ngz);
     return sizeof(float) * ((size_t)r0sz + (size_t)g.na * ncp + (size_t)ru4(g.ngz) * ncp);
 }
-static size_t syn3_smem(const DevGeo& g, int ncp) {
-    int K2 = 2 * g.nkz, ldz = ru4(K2) + 1;
-    return sizeof(float) * ((size_t)ZCH * ldz + (size_t)ru4(K2) * ncp + 4 * ZCH * ncp +
-                            (size_t)ncp * g.na);
-}
-
 // findf for the mixed path: mass -> field (and optional polar copy)
 int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
     const DevGeo& g = c->g;
@@ -489,19 +326,8 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
     }
     rc = gx_phase_mark(c, PH_SYN);
     if (rc) return rc;
-    if (g.ndim == 3) {
-        size_t sm = syn3_smem(g, ncp);
-        GX_CUDA(c, cudaFuncSetAttribute(k_syn3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        dim3 grid(g.nr, (g.ngz + ZCH - 1) / ZCH);
-        k_syn3<<<grid, 256, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, c->field, polar);
-        GX_LAUNCHED(c);
-    } else {
-        size_t sm = sizeof(float) * ((size_t)4 * RB2 * ncp + (size_t)ncp * g.na);
-        GX_CUDA(c, cudaFuncSetAttribute(k_syn2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        int nb = (g.nr + RB2 - 1) / RB2;
-        k_syn2<<<nb, 256, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, c->field, polar);
-        GX_LAUNCHED(c);
-    }
+    rc = gx_synthesis(c, tmask, polar);
+    if (rc) return rc;
     rc = gx_phase_end(c);
     if (rc) return rc;
     c->have_field = true;

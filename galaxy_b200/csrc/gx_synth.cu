@@ -1,0 +1,325 @@
+// gx_synth.cu -- field synthesis of the mixed path (p3fsyn.f:59-129,
+// p2fsyn.f:34-56) fused with polcat (polcat.f:22-41).
+//
+// The inverse transforms are small GEMMs against twiddle tables built once
+// per context; both exploit the symmetry of a real inverse DFT:
+//   k_synz   vertical synthesis r(z) = sum_k A_k wA(k,z) + B_k wB(k,z) over
+//            the ngz + 1 wavenumbers of the doubled grid, only for the
+//            physical planes.  With E/O the sums over even/odd k,
+//            r(z) = EA + OA + EB + OB and r(ngz - z) = EA - OA - EB + OB, so
+//            each pass of the k loop yields two planes.
+//   k_synaz  azimuthal synthesis with the 1/(2 ngz na) (2D: 1/na) scale:
+//            C = sum_a (a_m 2cos m th), S = sum_a (b_m (-2 sin m th)),
+//            f(j) = C + S and f(na - j) = C - S; then the rotation to
+//            (fx, fy) and one float4 (fx, fy, fz, phi) store per node.
+#include <algorithm>
+
+#include "gx_common.cuh"
+
+struct ActList {
+    int m[64];
+};
+
+struct SynTab {
+    const float* WAe;  // [ru4(Z0)][KE]  wA(2i, z)
+    const float* WBe;  // [ru4(Z0)][KE]  wB(2i, z)
+    const float* WAo;  // [ru4(Z0)][KO]  wA(2i+1, z)
+    const float* WBo;  // [ru4(Z0)][KO]  wB(2i+1, z)
+    const float* TC;   // [nact][njp]    cosine row weights (scaled)
+    const float* TS;   // [nact][njp]    sine row weights (scaled)
+    int Z0, KE, KO, njp;
+};
+
+__host__ __device__ static inline int ru4s(int x) { return (x + 3) & ~3; }
+
+static void syn_dims(const DevGeo& g, int& Z0, int& KE, int& KO, int& njp) {
+    Z0 = g.ngz / 2 + 1;
+    KE = g.ngz / 2 + 1;          // k = 0, 2, ..., <= ngz
+    KO = (g.ngz + 1) / 2;        // k = 1, 3, ..., <= ngz
+    njp = ru4s(g.na / 2 + 1);
+}
+
+__device__ __forceinline__ float wA(int k, int z, int ngz) {
+    if (k == 0) return 1.f;
+    if (k == ngz) return (z & 1) ? -1.f : 1.f;
+    int idx = (int)(((int64_t)k * z) % (2 * ngz));
+    return 2.f * cospif((float)idx / (float)ngz);
+}
+__device__ __forceinline__ float wB(int k, int z, int ngz) {
+    if (k <= 0 || k >= ngz) return 0.f;
+    int idx = (int)(((int64_t)k * z) % (2 * ngz));
+    return -2.f * sinpif((float)idx / (float)ngz);
+}
+
+__global__ void k_syntab(DevGeo g, ActList act, int nact, float scale, float* WAe, float* WBe,
+                         float* WAo, float* WBo, float* TC, float* TS, int Z0, int KE, int KO,
+                         int njp) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nz = ru4s(Z0);
+    if (tid < nz * KE) {
+        int z = tid / KE, i = tid - z * KE;
+        WAe[tid] = (z < Z0) ? wA(2 * i, z, g.ngz) : 0.f;
+        WBe[tid] = (z < Z0) ? wB(2 * i, z, g.ngz) : 0.f;
+    }
+    if (tid < nz * KO) {
+        int z = tid / KO, i = tid - z * KO;
+        WAo[tid] = (z < Z0) ? wA(2 * i + 1, z, g.ngz) : 0.f;
+        WBo[tid] = (z < Z0) ? wB(2 * i + 1, z, g.ngz) : 0.f;
+    }
+    if (tid < nact * njp) {
+        int a = tid / njp, j = tid - a * njp;
+        int m = act.m[a];
+        float c = 0.f, s = 0.f;
+        if (j <= g.na / 2) {
+            int idx = (int)(((int64_t)m * j) % g.na);
+            float sn, cs;
+            sincospif(2.0f * (float)idx / (float)g.na, &sn, &cs);
+            if (m == 0) c = 1.f;
+            else if (m == g.mmax - 1) c = (j & 1) ? -1.f : 1.f;
+            else {
+                c = 2.f * cs;
+                s = -2.f * sn;
+            }
+        }
+        TC[tid] = c * scale;
+        TS[tid] = s * scale;
+    }
+}
+
+// vertical synthesis, one CTA per (ring, field type); R[t][ir][z][ncp]
+__global__ void __launch_bounds__(128) k_synz(DevGeo g, int nact, int ncp, int tmask,
+                                             const float4* __restrict__ O, SynTab tb,
+                                             float* __restrict__ R) {
+    extern __shared__ __align__(16) float sm[];
+    const int ir = blockIdx.x, t = blockIdx.y;
+    if (!((tmask >> t) & 1)) return;
+    const int nr = g.nr, nkz = g.nkz, ngz = g.ngz;
+    float* Rt = R + (((size_t)t * nr + ir) * ngz) * ncp;
+    const float4* Ot = O + (size_t)t * nact * nkz * nr;
+    if (g.ndim == 2) {
+        for (int c = threadIdx.x; c < ncp; c += blockDim.x) {
+            const int a = c >> 1;
+            float v = 0.f;
+            if (a < nact) {
+                float4 o = Ot[(size_t)a * nr + ir];
+                v = (c & 1) ? o.z : o.x;
+            }
+            Rt[c] = v;
+        }
+        return;
+    }
+    const int Z0 = tb.Z0, KE = tb.KE, KO = tb.KO, nz4 = ru4s(Z0);
+    float* sWAe = sm;
+    float* sWBe = sWAe + nz4 * KE;
+    float* sWAo = sWBe + nz4 * KE;
+    float* sWBo = sWAo + nz4 * KO;
+    float* Ae = sWBo + nz4 * KO;        // [KE][ncp]
+    float* Be = Ae + KE * ncp;
+    float* Ao = Be + KE * ncp;          // [KO][ncp]
+    float* Bo = Ao + KO * ncp;
+    for (int i = threadIdx.x; i < nz4 * KE; i += blockDim.x) {
+        sWAe[i] = tb.WAe[i];
+        sWBe[i] = tb.WBe[i];
+    }
+    for (int i = threadIdx.x; i < nz4 * KO; i += blockDim.x) {
+        sWAo[i] = tb.WAo[i];
+        sWBo[i] = tb.WBo[i];
+    }
+    // spectrum of this ring: rows k, columns (a-row, b-row) of each harmonic
+    for (int i = threadIdx.x; i < nkz * nact; i += blockDim.x) {
+        const int k = i / nact, a = i - k * nact;
+        const float4 o = Ot[((size_t)a * nkz + k) * nr + ir];
+        const int h = k >> 1;
+        float* A = (k & 1) ? Ao : Ae;
+        float* B = (k & 1) ? Bo : Be;
+        A[h * ncp + 2 * a] = o.x;
+        B[h * ncp + 2 * a] = o.y;
+        A[h * ncp + 2 * a + 1] = o.z;
+        B[h * ncp + 2 * a + 1] = o.w;
+    }
+    for (int i = threadIdx.x; i < (KE + KO) * (ncp - 2 * nact); i += blockDim.x) {
+        const int w = ncp - 2 * nact;
+        const int h = i / w, c = 2 * nact + (i - h * w);
+        if (h < KE) {
+            Ae[h * ncp + c] = 0.f;
+            Be[h * ncp + c] = 0.f;
+        } else {
+            Ao[(h - KE) * ncp + c] = 0.f;
+            Bo[(h - KE) * ncp + c] = 0.f;
+        }
+    }
+    __syncthreads();
+    const int tilesN = ncp >> 2, tilesM = nz4 >> 2;
+    for (int tile = threadIdx.x; tile < tilesM * tilesN; tile += blockDim.x) {
+        const int tm = tile / tilesN, tn = tile - tm * tilesN;
+        const int z0 = tm * 4, c0 = tn * 4;
+        float EA[4][4], EB[4][4], OA[4][4], OB[4][4];
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) EA[r][q] = EB[r][q] = OA[r][q] = OB[r][q] = 0.f;
+#pragma unroll 2
+        for (int i = 0; i < KE; i++) {
+            const float4 a4 = *reinterpret_cast<const float4*>(Ae + i * ncp + c0);
+            const float4 b4 = *reinterpret_cast<const float4*>(Be + i * ncp + c0);
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const float wa = sWAe[(z0 + r) * KE + i], wb = sWBe[(z0 + r) * KE + i];
+                EA[r][0] += wa * a4.x; EA[r][1] += wa * a4.y; EA[r][2] += wa * a4.z; EA[r][3] += wa * a4.w;
+                EB[r][0] += wb * b4.x; EB[r][1] += wb * b4.y; EB[r][2] += wb * b4.z; EB[r][3] += wb * b4.w;
+            }
+        }
+#pragma unroll 2
+        for (int i = 0; i < KO; i++) {
+            const float4 a4 = *reinterpret_cast<const float4*>(Ao + i * ncp + c0);
+            const float4 b4 = *reinterpret_cast<const float4*>(Bo + i * ncp + c0);
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const float wa = sWAo[(z0 + r) * KO + i], wb = sWBo[(z0 + r) * KO + i];
+                OA[r][0] += wa * a4.x; OA[r][1] += wa * a4.y; OA[r][2] += wa * a4.z; OA[r][3] += wa * a4.w;
+                OB[r][0] += wb * b4.x; OB[r][1] += wb * b4.y; OB[r][2] += wb * b4.z; OB[r][3] += wb * b4.w;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 4; r++) {
+            const int z = z0 + r;
+            if (z >= Z0) continue;
+            float4 lo, hi;
+            lo.x = EA[r][0] + OA[r][0] + EB[r][0] + OB[r][0];
+            lo.y = EA[r][1] + OA[r][1] + EB[r][1] + OB[r][1];
+            lo.z = EA[r][2] + OA[r][2] + EB[r][2] + OB[r][2];
+            lo.w = EA[r][3] + OA[r][3] + EB[r][3] + OB[r][3];
+            *reinterpret_cast<float4*>(Rt + (size_t)z * ncp + c0) = lo;
+            const int zm = ngz - z;
+            if (z >= 1 && zm != z && zm < ngz) {
+                hi.x = EA[r][0] - OA[r][0] - EB[r][0] + OB[r][0];
+                hi.y = EA[r][1] - OA[r][1] - EB[r][1] + OB[r][1];
+                hi.z = EA[r][2] - OA[r][2] - EB[r][2] + OB[r][2];
+                hi.w = EA[r][3] - OA[r][3] - EB[r][3] + OB[r][3];
+                *reinterpret_cast<float4*>(Rt + (size_t)zm * ncp + c0) = hi;
+            }
+        }
+    }
+}
+
+#define SYN_ZB 8
+// azimuthal synthesis + polcat, one CTA per (ring, SYN_ZB planes)
+__global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int tmask,
+                                              const float* __restrict__ R, SynTab tb,
+                                              float4* __restrict__ F, float* __restrict__ polar) {
+    extern __shared__ __align__(16) float sm[];
+    const int ir = blockIdx.x, zb = blockIdx.y * SYN_ZB;
+    const int nr = g.nr, ngz = g.ngz, na = g.na, njp = tb.njp;
+    const int nz = min(SYN_ZB, ngz - zb);
+    float* TC = sm;                      // [nact][njp]
+    float* TS = TC + nact * njp;
+    float* Rs = TS + nact * njp;         // [4][SYN_ZB][ncp]
+    for (int i = threadIdx.x; i < nact * njp; i += blockDim.x) {
+        TC[i] = tb.TC[i];
+        TS[i] = tb.TS[i];
+    }
+    for (int i = threadIdx.x; i < 4 * SYN_ZB * ncp; i += blockDim.x) {
+        const int t = i / (SYN_ZB * ncp), rem = i - t * SYN_ZB * ncp;
+        const int z = rem / ncp, c = rem - z * ncp;
+        float v = 0.f;
+        if (((tmask >> t) & 1) && z < nz) v = R[(((size_t)t * nr + ir) * ngz + zb + z) * ncp + c];
+        Rs[i] = v;
+    }
+    __syncthreads();
+    const int nq = njp >> 2, half = na / 2;
+    const size_t mesh = g.mesh;
+    for (int it = threadIdx.x; it < nz * nq; it += blockDim.x) {
+        const int z = it / nq, j0 = (it - z * nq) * 4;
+        float C[4][4], S[4][4];
+#pragma unroll
+        for (int t = 0; t < 4; t++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) C[t][q] = S[t][q] = 0.f;
+        for (int a = 0; a < nact; a++) {
+            const float4 tc = *reinterpret_cast<const float4*>(TC + a * njp + j0);
+            const float4 ts = *reinterpret_cast<const float4*>(TS + a * njp + j0);
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const float rc = Rs[(t * SYN_ZB + z) * ncp + 2 * a];
+                const float rs = Rs[(t * SYN_ZB + z) * ncp + 2 * a + 1];
+                C[t][0] += rc * tc.x; C[t][1] += rc * tc.y; C[t][2] += rc * tc.z; C[t][3] += rc * tc.w;
+                S[t][0] += rs * ts.x; S[t][1] += rs * ts.y; S[t][2] += rs * ts.z; S[t][3] += rs * ts.w;
+            }
+        }
+        const size_t rowb = ((size_t)ir * ngz + zb + z) * na;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int j = j0 + q;
+            if (j > half) continue;
+            float sn, cs;
+            sincospif(2.0f * (float)j / (float)na, &sn, &cs);
+            {
+                const float fr = C[0][q] + S[0][q], ft = C[1][q] + S[1][q];
+                const float fz = C[2][q] + S[2][q], ph = C[3][q] + S[3][q];
+                F[rowb + j] = make_float4(fr * cs - ft * sn, fr * sn + ft * cs, fz, ph);
+                if (polar) {
+                    polar[rowb + j] = fr;
+                    polar[mesh + rowb + j] = ft;
+                    polar[2 * mesh + rowb + j] = fz;
+                    polar[3 * mesh + rowb + j] = ph;
+                }
+            }
+            if (j > 0 && j < half) {
+                const int jm = na - j;  // angle -theta_j: cos same, sin negated
+                const float fr = C[0][q] - S[0][q], ft = C[1][q] - S[1][q];
+                const float fz = C[2][q] - S[2][q], ph = C[3][q] - S[3][q];
+                F[rowb + jm] = make_float4(fr * cs + ft * sn, -fr * sn + ft * cs, fz, ph);
+                if (polar) {
+                    polar[rowb + jm] = fr;
+                    polar[mesh + rowb + jm] = ft;
+                    polar[2 * mesh + rowb + jm] = fz;
+                    polar[3 * mesh + rowb + jm] = ph;
+                }
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+int gx_synthesis(GxCtx* c, int tmask, float* polar) {
+    const DevGeo& g = c->g;
+    const int nact = c->spec.nact;
+    const int ncp = ru4s(2 * nact);
+    int Z0, KE, KO, njp;
+    syn_dims(g, Z0, KE, KO, njp);
+    const int nz4 = ru4s(Z0);
+    const size_t nWe = (size_t)nz4 * KE, nWo = (size_t)nz4 * KO, nT = (size_t)nact * njp;
+    if (!c->syntab) {
+        if (nact > 64) return c->err = "more than 64 active harmonics", GX_ERR_RANGE;
+        const size_t tot = 2 * nWe + 2 * nWo + 2 * nT;
+        GX_CUDA(c, cudaMalloc((void**)&c->syntab, sizeof(float) * tot));
+        ActList act;
+        for (int a = 0; a < 64; a++) act.m[a] = a < nact ? c->spec.m[a] : 0;
+        const float scale = (g.ndim == 3) ? 1.0f / (float)(2 * g.ngz * g.na) : 1.0f / (float)g.na;
+        float* b = c->syntab;
+        const size_t mx = std::max(std::max(nWe, nWo), nT);
+        k_syntab<<<(unsigned)((mx + 255) / 256), 256, 0, c->stream>>>(
+            g, act, nact, scale, b, b + nWe, b + 2 * nWe, b + 2 * nWe + nWo, b + 2 * nWe + 2 * nWo,
+            b + 2 * nWe + 2 * nWo + nT, Z0, KE, KO, njp);
+        GX_LAUNCHED(c);
+    }
+    if (!c->synR) GX_CUDA(c, cudaMalloc((void**)&c->synR, sizeof(float) * 4 * g.nr * g.ngz * ncp));
+    const float* b = c->syntab;
+    SynTab tb{b, b + nWe, b + 2 * nWe, b + 2 * nWe + nWo, b + 2 * nWe + 2 * nWo,
+              b + 2 * nWe + 2 * nWo + nT, Z0, KE, KO, njp};
+    {
+        const size_t sm = sizeof(float) * (2 * nWe + 2 * nWo + (size_t)(KE + KO) * 2 * ncp);
+        GX_CUDA(c, cudaFuncSetAttribute(k_synz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        dim3 grid(g.nr, 4);
+        k_synz<<<grid, 128, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, tb, c->synR);
+        GX_LAUNCHED(c);
+    }
+    {
+        const size_t sm = sizeof(float) * (2 * nT + (size_t)4 * SYN_ZB * ncp);
+        GX_CUDA(c, cudaFuncSetAttribute(k_synaz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        dim3 grid(g.nr, (g.ngz + SYN_ZB - 1) / SYN_ZB);
+        k_synaz<<<grid, 256, sm, c->stream>>>(g, nact, ncp, tmask, c->synR, tb, c->field, polar);
+        GX_LAUNCHED(c);
+    }
+    return GX_OK;
+}
