@@ -94,9 +94,13 @@ extern "C" int gx_comm_init(GxCtx* c, const char* id128, int nranks, int rank) {
     return GX_OK;
 }
 
+// NCCL is loaded only when a communicator is bound: loading the system copy
+// into a process that later imports a framework bundling a newer libnccl.so.2
+// would shadow that copy
 void gx_comm_destroy(GxCtx* c) {
+    if (!c->comm) return;
     NcclApi* a = nccl();
-    if (a && c->comm) a->commDestroy((ncclComm_t)c->comm);
+    if (a) a->commDestroy((ncclComm_t)c->comm);
     c->comm = nullptr;
 }
 
