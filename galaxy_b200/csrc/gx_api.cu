@@ -18,7 +18,7 @@ static std::string g_last_err;  // errors of gx_grdset before a context exists
 // (SRC/lib15/filset.f:116-141) and p3dset's softening check
 // (SRC/lib15/p3dset.f:99-100).  Reals are formed in FP32 as the reference
 // forms them (alpha = 2.*pi/real(na), pi real*8, stored as real).
-static int setgrd(const GxConfig* c, GxGeometry* g, std::string& err) {
+int setgrd(const GxConfig* c, GxGeometry* g, std::string& err) {
     memset(g, 0, sizeof *g);
     if (c->ndim != 2 && c->ndim != 3) return err = "ndim must be 2 or 3", GX_ERR_ARG;
     int na = 2 * (c->na / 2);
@@ -77,7 +77,7 @@ static int setgrd(const GxConfig* c, GxGeometry* g, std::string& err) {
     return GX_OK;
 }
 
-static void fill_devgeo(GxCtx* c) {
+void fill_devgeo(GxCtx* c) {
     const GxGeometry& G = c->geo;
     DevGeo& d = c->g;
     memset(&d, 0, sizeof d);

@@ -299,6 +299,8 @@ __device__ __forceinline__ void gx_row_count(uint32_t row, bool act, uint32_t* _
 
 // ---------------------------------------------------------------------------
 // host-side entry points implemented in the .cu files
+int setgrd(const GxConfig* c, GxGeometry* g, std::string& err);
+void fill_devgeo(GxCtx* c);
 int gx_green_build_dev(GxCtx* c);
 int gx_mixed_masset(GxCtx* c);
 int gx_mixed_findf(GxCtx* c, int lpot, bool polcat);

@@ -222,6 +222,31 @@ int gx_last_launch_count(const GxCtx* ctx, int64_t* n);
 int gx_comm_unique_id(char* id128);
 int gx_comm_init(GxCtx* ctx, const char* id128, int nranks, int rank);
 
+/* massgn + scaled without allocating memory.  No counterpart in the
+ * reference: it is for callers that may not allocate device memory when they
+ * deposit mass, e.g. a host code that owns a fixed device memory pool, or a
+ * time loop that must not wait on the allocator.  d_coords (n AoS records of
+ * 2*ndim floats) and d_mass (mesh floats) are device pointers owned by the
+ * caller; cfg gives the grid as for gx_grdset (mixed path only).  The result
+ * equals the gx_masset mass array of the same particles (fixed-point
+ * quantum 2^-32 instead of 2^-20).
+ *  - Working memory is one file-scope device array of 2^22 cells (32 MiB),
+ *    held by every GPU that loads the library until the process exits; a
+ *    grid with more than 4194304 cells is rejected with GX_ERR_RANGE before
+ *    any work is queued.
+ *  - The first call on a device looks the array up (cudaGetSymbolAddress)
+ *    with that device current; make that first call before any stream
+ *    capture.
+ *  - All calls share the array and each call clears it first, so calls
+ *    whose work overlaps on the GPU (different streams, threads or
+ *    processes sharing a context) race and must be serialised by the
+ *    caller.
+ *  - Work is queued on stream (a cudaStream_t); with stream NULL the call
+ *    returns after the work completed.  Returns GX_OK or GX_ERR_ARG /
+ *    GX_ERR_RANGE / GX_ERR_CUDA; no message is recorded. */
+int gx_massgn_noalloc(const GxConfig* cfg, const float* d_coords, int64_t n, float* d_mass,
+                      void* stream);
+
 /* Page-locked host buffers for gx_loadup/gx_unload (cudaMallocHost in the
  * library's own runtime).  No reference counterpart. */
 int gx_host_alloc(int64_t bytes, void** ptr);
