@@ -286,6 +286,36 @@ def run_e2e(args, w, rec, pm, cfg_dev):
             "pinned": pinned, "finite": ok, "what": "gx_loadup + gx_masset + gx_step(K) + gx_unload, wall clock"}
 
 
+def run_sfp(n=20_000_000, reps=5):
+    """The SFP coefficient sum of the 2D Abel-Jacobi configuration: 20M
+    particles of an exponential disc (scale 1, truncated at r = 6), k = 7,
+    n = 0..19, m = 0..8, maxr = 6; tensor-core path against the FP64 path."""
+    from galaxy_b200.disk import exp_disk
+    from galaxy_b200.sfp import Basis, Sfp
+    basis = Basis.from_json(os.path.join(ROOT, "tests", "golden", "aj07.json"), maxm=8, maxn=19)
+    pos = exp_disk(n, seed=12345)
+    out = {"workload": "sfp2d-aj07-m0..8-n0..19-20M"}
+    with Sfp(basis, 6.0) as s:
+        s.load(pos)
+        s.sum(1.0 / n, 0)
+        t = []
+        for _ in range(reps):
+            c32 = s.sum(1.0 / n, 0)
+            t.append(s.last_ms()[0])
+        c64 = s.sum(1.0 / n, 1)
+        t64 = s.last_ms()[0]
+    ms = float(np.median(t))
+    peak, src = peaks()
+    nbytes = n * 8
+    out.update({"ms": round(ms, 4), "particles_per_s": n / (ms * 1e-3),
+                "ms_fp64_path": round(t64, 3), "speedup_vs_fp64_path": round(t64 / ms, 2),
+                "coeff_rel_err_vs_fp64": float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64)),
+                "hbm_GB_s": round(nbytes / (ms * 1e-3) / 1e9, 1),
+                "hbm_frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 4),
+                "useful_tflops": round(2 * n * 340 / (ms * 1e-3) / 1e12, 3)})
+    return out
+
+
 def cpu_rate(w, rec, pm, steps, budget_s, threads):
     """CPU restatement of one step (oracle, FP32 mirror) on the host cores:
     the field solve on the full grid, the particle loop on a sample, the
@@ -356,6 +386,7 @@ def main():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=30.0)
+    ap.add_argument("--no-sfp", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     w = WORKLOADS[args.workload]
@@ -396,6 +427,7 @@ def main():
         comm.barrier()
     if rank == 0:
         e2e = run_e2e(args, w, rec, pm, cfg.device) if world == 1 else None
+        sfp = run_sfp() if (world == 1 and not args.no_sfp) else None
         cpu = None
         if world == 1 and not args.no_cpu:
             cpu = cpu_rate(w, rec, pm, 3, args.cpu_budget, os.cpu_count() or 1)
@@ -409,7 +441,7 @@ def main():
                 "fp64_path": out.get("fp64_path"),
                 "speedup_vs_fp64_path": out.get("speedup_vs_fp64_path"),
                 "force_rel_err": out.get("force_rel_err"),
-                "step_roofline": out["step_roofline"], "phases": out["phases"]}
+                "step_roofline": out["step_roofline"], "phases": out["phases"], "sfp": sfp}
         print(json.dumps(line))
     if comm is not None:
         comm.dist.destroy_process_group()

@@ -97,6 +97,20 @@ class GxDiag(C.Structure):
     ]
 
 
+class GxSfpBasis(C.Structure):
+    _fields_ = [
+        ("k", C.c_int32),
+        ("minm", C.c_int32),
+        ("maxm", C.c_int32),
+        ("minn", C.c_int32),
+        ("maxn", C.c_int32),
+        ("nsect", C.c_int32),
+        ("nrtab", C.c_int32),
+        ("roots", C.c_void_p),
+        ("xcoeff", C.c_void_p),
+    ]
+
+
 def make_config(ndim, nr, na, ngz=1, dzg=0.0, ng=1, nsect=1, skip=(),
                 rmap=GX_RMAP_STDPOL, rmap_a=0.0, rmap_r0=0.0, softl=1.0,
                 tsoft=GX_SOFT_PLUMMER, pmass=1.0, halo=0, halo_v2=0.0,

@@ -1,0 +1,573 @@
+// gx_sfp.cu -- SFP (smooth-field-particle) Abel-Jacobi method: coefficient
+// sum (sfpadd/sfpsum, scaled) and force evaluation (sfpacc).
+//
+// The reference tabulates U_nm(r/maxr) at nrtab radii and interpolates
+// per particle (sfptab.f:43-78, sfpval.f:24-52), then accumulates
+// C[n, +m] += U cos(m phi), C[n, -m] += U sin(m phi) in FP64
+// (sfpadd.f:37-93).  Each U_nm(p) = p^m P_nm(p^2) with P_nm a polynomial of
+// degree n + k (ajfun.f:33-47); with e = m mod 2, U_nm / p^e is a polynomial
+// in p^2 of degree n + k + (m - e)/2, so with x = 2 p^2 - 1 it is exactly a
+// Chebyshev series sum_d a_nmd T_d(x).  (Keeping the even power of p inside
+// the series keeps its coefficients of the size of U itself; dividing out all
+// of p^m would blow them up near the centre.)  The sum over particles
+// factors through the moment matrix
+//     M[d][c] = sum_p T_d(x_p) g_c(p),  g = (1, p^e cos m phi, p^e sin m phi)
+// and C[n, m, .] = sum_d a_nmd M[d][c(m, .)].  M is a GEMM with K = N
+// (particles): it runs on the tensor cores with mma.sync m16n8k8 TF32,
+// each operand split hi + lo (three products, FP32 accumulate per warp over
+// a chunk of particles, chunks summed in FP64).  The fragments are formed
+// in registers from each lane's particles: no shared-memory staging of
+// per-particle features, which would otherwise bound the kernel.
+// a_nmd are formed once on the host in FP64 from the roots and
+// coefficients of the basis (Chebyshev interpolation at 64 nodes).
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "gx_common.cuh"
+
+#define SFP_CHUNK 1024  // particles per warp-chunk (FP32 accumulation span)
+
+struct GxSfp {
+    GxSfpBasis b;
+    std::vector<double> roots, xcoeff;
+    int dev = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    std::string err;
+    int nfun = 0;
+    std::vector<int> msel, nsel;
+    int D = 32;   // Chebyshev terms
+    int NC = 0;   // feature columns 2 maxm + 1
+    std::vector<double> acheb;  // [nfun][D]
+    double maxr = 1.0;
+    int64_t n = 0, cap = 0;
+    float* xy = nullptr;        // [2][cap]
+    float* part = nullptr;      // per-warp partial moments
+    double* mom = nullptr;      // [D][NCP] FP64 moments
+    double* qc = nullptr;       // device force series [2][maxm+1][D]
+    float last_ms = 0.f;
+    int64_t launches = 0;
+};
+
+static std::string g_sfp_err;
+
+// ---------------------------------------------------------------------------
+// host: ajfun in FP64 (ajfun.f:33-47) and its Chebyshev coefficients
+static double ajfun_h(const GxSfp* s, int m, int n, double r) {
+    const GxSfpBasis& b = s->b;
+    const double* xc = s->xcoeff.data() + ((size_t)m * (b.maxn + 1) + n) * (b.k + 1);
+    const double* rt = s->roots.data() + ((size_t)m * (b.maxn + 1) + n) * b.maxn;
+    const double r2 = r * r, x = 1.0 - r2;
+    double f = xc[0];
+    for (int i = 1; i <= b.k; i++) f += xc[i] * pow(x, i);
+    for (int i = 0; i < n; i++) f *= (r2 - rt[i] * rt[i]);
+    return GX_PI / (double)sqrtf(2.0f) * f;  // pi / sqrt(2.), sqrt in single precision
+}
+
+static void cheb_coeffs(GxSfp* s) {
+    const int NN = 64;
+    s->acheb.assign((size_t)s->nfun * s->D, 0.0);
+    std::vector<double> vals(NN);
+    for (int f = 0; f < s->nfun; f++) {
+        const int m = s->msel[f], n = s->nsel[f];
+        for (int j = 0; j < NN; j++) {
+            double xj = cos(GX_PI * (j + 0.5) / NN);
+            double p = sqrt(0.5 * (xj + 1.0));
+            // U_nm / p^(m mod 2): ajfun_h leaves out the r^m factor
+            vals[j] = ajfun_h(s, m, n, p) * pow(p, (double)(m - (m & 1)));
+        }
+        for (int d = 0; d < s->D; d++) {
+            double acc = 0;
+            for (int j = 0; j < NN; j++) acc += vals[j] * cos(d * GX_PI * (j + 0.5) / NN);
+            s->acheb[(size_t)f * s->D + d] = (d == 0 ? 1.0 : 2.0) * acc / NN;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// device helpers
+// round to TF32 (nearest, ties away) and clear the 13 low mantissa bits, so
+// that the returned bits are exactly the TF32 value as an FP32 number
+__device__ __forceinline__ uint32_t f2tf32(float v) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+    return r & 0xffffe000u;
+}
+
+__device__ __forceinline__ void mma_tf32(float* d, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Features of one particle for the lane's fragment slots: T_d for
+// d = q + 8 j (j < 2 MT) and g_n for n = q + 8 u (u < NT):
+// g_0 = 1, g_{2m-1} = p^e cos m phi, g_{2m} = p^e sin m phi, e = m mod 2.
+template <int MT, int NT>
+__device__ __forceinline__ void sfp_features(float x, float y, float inv_maxr, int q, int maxm,
+                                             float* T, float* G) {
+    const float px = x * inv_maxr, py = y * inv_maxr;
+    const float p2 = px * px + py * py;
+    const bool act = p2 <= 1.0f;
+    const float xc = 2.f * p2 - 1.f;
+    // T_0 .. T_8 by the three-term recurrence
+    float t[9];
+    t[0] = 1.f;
+    t[1] = xc;
+#pragma unroll
+    for (int i = 2; i <= 8; i++) t[i] = 2.f * xc * t[i - 1] - t[i - 2];
+    float tq = 0.f, tm = 0.f;  // T_q, T_{8-q}
+#pragma unroll
+    for (int i = 0; i <= 8; i++) {
+        if (i == q) tq = t[i];
+        if (i == 8 - q) tm = t[i];
+    }
+    // T_{d+8} = 2 T_8 T_d - T_{|d-8|}
+    float prev = tm, cur = tq;
+#pragma unroll
+    for (int j = 0; j < 2 * MT; j++) {
+        T[j] = act ? cur : 0.f;
+        float nx = 2.f * t[8] * cur - prev;
+        prev = cur;
+        cur = nx;
+    }
+    // e^{i m phi} by repeated multiplication
+    const float pr = sqrtf(p2);
+    const float cr = pr > 0.f ? px / pr : 1.f, ci = pr > 0.f ? py / pr : 0.f;
+    float zr = 1.f, zi = 0.f;
+#pragma unroll
+    for (int u = 0; u < NT; u++) G[u] = 0.f;
+    for (int m = 0; m <= maxm; m++) {
+        if (m > 0) {
+            float nr = zr * cr - zi * ci;
+            zi = zr * ci + zi * cr;
+            zr = nr;
+        }
+        const float f = (m & 1) ? pr : 1.f;
+#pragma unroll
+        for (int u = 0; u < NT; u++) {
+            const int n = q + 8 * u;
+            if (m == 0 && n == 0) G[u] = 1.f;
+            if (m > 0 && n == 2 * m - 1) G[u] = zr * f;
+            if (m > 0 && n == 2 * m) G[u] = zi * f;
+        }
+    }
+    if (!act)
+#pragma unroll
+        for (int u = 0; u < NT; u++) G[u] = 0.f;
+}
+
+// moments of one SFP_CHUNK of particles per warp; part[warp][d][c]
+template <int MT, int NT>
+__global__ void __launch_bounds__(256) k_sfp_moments(const float* __restrict__ X,
+                                                     const float* __restrict__ Y, int64_t n,
+                                                     float inv_maxr, int maxm,
+                                                     float* __restrict__ part) {
+    const int lane = threadIdx.x & 31;
+    const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t base = wid * SFP_CHUNK;
+    if (base >= n) return;
+    const int q = lane >> 2, c4 = lane & 3;
+    float acc[MT][NT][4];
+#pragma unroll
+    for (int a = 0; a < MT; a++)
+#pragma unroll
+        for (int u = 0; u < NT; u++)
+#pragma unroll
+            for (int i = 0; i < 4; i++) acc[a][u][i] = 0.f;
+    const int64_t end = min(base + (int64_t)SFP_CHUNK, n);
+    for (int64_t k0 = base; k0 < end; k0 += 8) {
+        float T[2][2 * MT], G[2][NT];
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            const int64_t i = k0 + c4 + 4 * e;
+            float x = 2.f / inv_maxr, y = 0.f;  // outside the basis edge: no contribution
+            if (i < end) {
+                x = __ldg(X + i);
+                y = __ldg(Y + i);
+            }
+            sfp_features<MT, NT>(x, y, inv_maxr, q, maxm, T[e], G[e]);
+        }
+        // split operands: hi = tf32(v), lo = tf32(v - hi)
+        uint32_t bh[NT][2], bl[NT][2];
+#pragma unroll
+        for (int u = 0; u < NT; u++)
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const float v = G[e][u];
+                bh[u][e] = f2tf32(v);
+                bl[u][e] = f2tf32(v - __uint_as_float(bh[u][e]));
+            }
+#pragma unroll
+        for (int a = 0; a < MT; a++) {
+            // a0 = A[q][c4], a1 = A[q+8][c4], a2 = A[q][c4+4], a3 = A[q+8][c4+4]
+            const float v[4] = {T[0][2 * a], T[0][2 * a + 1], T[1][2 * a], T[1][2 * a + 1]};
+            uint32_t ah[4], al[4];
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                ah[i] = f2tf32(v[i]);
+                al[i] = f2tf32(v[i] - __uint_as_float(ah[i]));
+            }
+#pragma unroll
+            for (int u = 0; u < NT; u++) {
+                mma_tf32(acc[a][u], al, bh[u]);
+                mma_tf32(acc[a][u], ah, bl[u]);
+                mma_tf32(acc[a][u], ah, bh[u]);
+            }
+        }
+    }
+    // c0 = D[q][2c4], c1 = D[q][2c4+1], c2 = D[q+8][2c4], c3 = D[q+8][2c4+1]
+    const int NCP = NT * 8;
+    float* dst = part + wid * (size_t)(MT * 16) * NCP;
+#pragma unroll
+    for (int a = 0; a < MT; a++)
+#pragma unroll
+        for (int u = 0; u < NT; u++) {
+            const int r0 = a * 16 + q, c0 = u * 8 + 2 * c4;
+            dst[r0 * NCP + c0] = acc[a][u][0];
+            dst[r0 * NCP + c0 + 1] = acc[a][u][1];
+            dst[(r0 + 8) * NCP + c0] = acc[a][u][2];
+            dst[(r0 + 8) * NCP + c0 + 1] = acc[a][u][3];
+        }
+}
+
+// FP64 sum of the per-warp partials: one block per moment, each thread a
+// strided subset of the warps, then a fixed-shape tree (deterministic)
+template <typename T>
+__global__ void k_sfp_reduce(const T* __restrict__ part, int64_t nwarp, int nmom,
+                             double* __restrict__ mom) {
+    __shared__ double sh[256];
+    const int i = blockIdx.x;
+    double s = 0.0;
+    for (int64_t w = threadIdx.x; w < nwarp; w += blockDim.x) s += (double)part[w * nmom + i];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) mom[i] = sh[0];
+}
+
+// plain FP64 moments on CUDA cores: features staged per block, one thread
+// per (d, c) moment summing over the block's particles, FP64 partial per block
+__global__ void k_sfp_moments64(const float* __restrict__ X, const float* __restrict__ Y, int64_t n,
+                                double inv_maxr, int maxm, int D, int NCP,
+                                double* __restrict__ part) {
+    extern __shared__ double fs[];  // [256][D + NCP]
+    const int w = D + NCP;
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    double* f = fs + threadIdx.x * w;
+    for (int k = 0; k < w; k++) f[k] = 0.0;
+    if (i < n) {
+        const double px = X[i] * inv_maxr, py = Y[i] * inv_maxr, p2 = px * px + py * py;
+        if (p2 <= 1.0) {
+            const double xc = 2.0 * p2 - 1.0;
+            f[0] = 1.0;
+            if (D > 1) f[1] = xc;
+            for (int d = 2; d < D; d++) f[d] = 2.0 * xc * f[d - 1] - f[d - 2];
+            const double pr = sqrt(p2);
+            const double cr = pr > 0.0 ? px / pr : 1.0, ci = pr > 0.0 ? py / pr : 0.0;
+            double zr = 1.0, zi = 0.0;
+            f[D] = 1.0;
+            for (int m = 1; m <= maxm; m++) {
+                double nr = zr * cr - zi * ci;
+                zi = zr * ci + zi * cr;
+                zr = nr;
+                const double e = (m & 1) ? pr : 1.0;
+                f[D + 2 * m - 1] = zr * e;
+                f[D + 2 * m] = zi * e;
+            }
+        }
+    }
+    __syncthreads();
+    const int nb = min((int64_t)blockDim.x, n - blockIdx.x * (int64_t)blockDim.x);
+    for (int mo = threadIdx.x; mo < D * NCP; mo += blockDim.x) {
+        const int d = mo / NCP, c = mo - d * NCP;
+        double s = 0.0;
+        for (int p = 0; p < nb; p++) s += fs[p * w + d] * fs[p * w + D + c];
+        part[blockIdx.x * (size_t)D * NCP + mo] = s;
+    }
+}
+
+// sfpacc (sfpacc.f:41-112, 249-259) from the per-m Chebyshev series of the
+// scaled coefficients: qc[(0/1)][m][d] (cosine / sine), FP64
+__global__ void k_sfp_acc(const float* __restrict__ X, const float* __restrict__ Y, int64_t n,
+                          double maxr, int maxm, int D, const double* __restrict__ qs,
+                          float* __restrict__ acc, float* __restrict__ pot) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double x = X[i], y = Y[i];
+    double rr = sqrt(x * x + y * y);
+    double ar = 0, at = 0, ph = 0;
+    if (rr <= maxr) {
+        const double r = rr > 1e-5 ? rr : 1e-5;
+        const double c1 = x / r, s1 = y / r;
+        const double p = rr / maxr, xc = 2.0 * p * p - 1.0;
+        double cm = 1.0, sm = 0.0;  // cos m phi, sin m phi
+        for (int m = 0; m <= maxm; m++) {
+            if (m > 0) {
+                double nc = cm * c1 - sm * s1;
+                sm = sm * c1 + cm * s1;
+                cm = nc;
+            }
+            // Clenshaw for Q(x) and Q'(x) of both series
+            double val[2], der[2];
+            for (int h = 0; h < 2; h++) {
+                const double* a = qs + ((size_t)h * (maxm + 1) + m) * D;
+                double b1 = 0, b2 = 0, d1 = 0, d2 = 0;
+                for (int d = D - 1; d >= 1; d--) {
+                    double bn = 2.0 * xc * b1 - b2 + a[d];
+                    double dn = 2.0 * xc * d1 - d2 + 2.0 * b1;
+                    b2 = b1;
+                    b1 = bn;
+                    d2 = d1;
+                    d1 = dn;
+                }
+                val[h] = xc * b1 - b2 + a[0];
+                der[h] = xc * d1 - d2 + b1;
+            }
+            // f = p^e Q(x) (e = m mod 2), df/dp = e Q + p^e Q'(x) dx/dp, dx/dp = 4 p
+            const double pe = (m & 1) ? p : 1.0, e = (double)(m & 1);
+            const double fc = pe * val[0], fs = pe * val[1];
+            const double dc = e * val[0] + pe * der[0] * 4.0 * p;
+            const double ds = e * val[1] + pe * der[1] * 4.0 * p;
+            if (m == 0) {
+                ar += dc;
+                ph -= fc;
+            } else {
+                ar += dc * cm + ds * sm;
+                at += (double)m * (fs * cm - fc * sm);
+                ph -= fc * cm + fs * sm;
+            }
+        }
+        at = at * maxr / r;
+        acc[2 * i] = (float)(ar * c1 - at * s1);
+        acc[2 * i + 1] = (float)(ar * s1 + at * c1);
+    } else {
+        acc[2 * i] = acc[2 * i + 1] = 0.f;
+    }
+    if (pot) pot[i] = (float)ph;
+}
+
+// ---------------------------------------------------------------------------
+#define SFP_CUDA(s, call)                                                        \
+    do {                                                                         \
+        cudaError_t e_ = (call);                                                 \
+        if (e_ != cudaSuccess) {                                                 \
+            (s)->err = std::string(#call) + ": " + cudaGetErrorString(e_);       \
+            return GX_ERR_CUDA;                                                  \
+        }                                                                        \
+    } while (0)
+
+extern "C" int gx_sfp_init(const GxSfpBasis* b, double maxr, int device, GxSfp** out) {
+    if (!b || !out || !(maxr > 0.0)) return g_sfp_err = "null argument or maxr <= 0", GX_ERR_ARG;
+    *out = nullptr;
+    if (b->minm < 0 || b->maxm < b->minm || b->minn < 0 || b->maxn < b->minn || b->nsect < 1 ||
+        b->k < 0 || !b->xcoeff || (b->maxn > 0 && !b->roots))
+        return g_sfp_err = "invalid basis selection", GX_ERR_ARG;
+    if (b->maxm > 11) return g_sfp_err = "maxm > 11 not supported", GX_ERR_RANGE;
+    if (b->maxn + b->k + 1 > 64) return g_sfp_err = "maxn + k + 1 > 64 not supported", GX_ERR_RANGE;
+    GxSfp* s = new GxSfp();
+    s->b = *b;
+    s->roots.assign(b->roots ? b->roots : b->xcoeff,
+                    (b->roots ? b->roots : b->xcoeff) +
+                        (b->roots ? (size_t)(b->maxm + 1) * (b->maxn + 1) * b->maxn : 0));
+    s->xcoeff.assign(b->xcoeff, b->xcoeff + (size_t)(b->maxm + 1) * (b->maxn + 1) * (b->k + 1));
+    s->b.roots = s->roots.data();
+    s->b.xcoeff = s->xcoeff.data();
+    s->maxr = maxr;
+    for (int m = b->minm; m <= b->maxm; m += b->nsect)
+        for (int n = b->minn; n <= b->maxn; n++) {
+            s->msel.push_back(m);
+            s->nsel.push_back(n);
+        }
+    s->nfun = (int)s->msel.size();
+    s->D = (b->maxn + b->k + 1 <= 32) ? 32 : 64;
+    s->NC = 2 * b->maxm + 1;
+    cheb_coeffs(s);
+    s->dev = device;
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->e1);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s->mom, sizeof(double) * 64 * 32);
+    if (e != cudaSuccess) {
+        g_sfp_err = std::string("CUDA: ") + cudaGetErrorString(e);
+        delete s;
+        return GX_ERR_CUDA;
+    }
+    *out = s;
+    return GX_OK;
+}
+
+extern "C" void gx_sfp_destroy(GxSfp* s) {
+    if (!s) return;
+    cudaSetDevice(s->dev);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    void* p[] = {s->xy, s->part, s->mom, s->qc};
+    for (void* q : p)
+        if (q) cudaFree(q);
+    if (s->e0) cudaEventDestroy(s->e0);
+    if (s->e1) cudaEventDestroy(s->e1);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+extern "C" const char* gx_sfp_last_error(const GxSfp* s) { return s ? s->err.c_str() : g_sfp_err.c_str(); }
+
+__global__ void k_sfp_xy(const float* __restrict__ aos, int stride, int64_t n, int64_t cap,
+                         float* __restrict__ xy) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    xy[i] = aos[i * stride];
+    xy[cap + i] = aos[i * stride + 1];
+}
+
+extern "C" int gx_sfp_load(GxSfp* s, const float* coords, int64_t n, int stride) {
+    if (!s || n < 0 || stride < 2 || (n > 0 && !coords)) return GX_ERR_ARG;
+    cudaSetDevice(s->dev);
+    if (n > s->cap) {
+        if (s->xy) cudaFree(s->xy);
+        if (s->part) cudaFree(s->part);
+        s->xy = nullptr;
+        s->part = nullptr;
+        s->cap = std::max<int64_t>(n, 1);
+        SFP_CUDA(s, cudaMalloc((void**)&s->xy, sizeof(float) * 2 * s->cap));
+        const int64_t nw = (s->cap + SFP_CHUNK - 1) / SFP_CHUNK;
+        const int64_t nb = (s->cap + 255) / 256;
+        const size_t bytes = std::max(sizeof(float) * nw * 64 * 32, sizeof(double) * nb * 64 * 32);
+        SFP_CUDA(s, cudaMalloc((void**)&s->part, bytes));
+    }
+    s->n = n;
+    if (n == 0) return GX_OK;
+    float* tmp = nullptr;
+    SFP_CUDA(s, cudaMallocAsync((void**)&tmp, sizeof(float) * stride * n, s->stream));
+    SFP_CUDA(s, cudaMemcpyAsync(tmp, coords, sizeof(float) * stride * n, cudaMemcpyHostToDevice, s->stream));
+    k_sfp_xy<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(tmp, stride, n, s->cap, s->xy);
+    SFP_CUDA(s, cudaGetLastError());
+    SFP_CUDA(s, cudaFreeAsync(tmp, s->stream));
+    SFP_CUDA(s, cudaStreamSynchronize(s->stream));
+    return GX_OK;
+}
+
+// moments on the device (precision GX_PREC_MIXED: tensor cores; GX_PREC_FP64: CUDA cores)
+static int sfp_moments(GxSfp* s, int precision) {
+    const int D = s->D, NCP = (s->NC + 7) / 8 * 8, nmom = D * NCP;
+    const int64_t n = s->n;
+    if (precision == GX_PREC_FP64) {
+        const int64_t nb = (n + 255) / 256;
+        const size_t sm = sizeof(double) * 256 * (D + NCP);
+        SFP_CUDA(s, cudaFuncSetAttribute(k_sfp_moments64, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_sfp_moments64<<<(unsigned)nb, 256, sm, s->stream>>>(s->xy, s->xy + s->cap, n, 1.0 / s->maxr,
+                                                              s->b.maxm, D, NCP, (double*)s->part);
+        SFP_CUDA(s, cudaGetLastError());
+        k_sfp_reduce<double><<<nmom, 256, 0, s->stream>>>((double*)s->part, nb, nmom, s->mom);
+        SFP_CUDA(s, cudaGetLastError());
+        s->launches += 2;
+        return GX_OK;
+    }
+    const int64_t nw = (n + SFP_CHUNK - 1) / SFP_CHUNK;
+    const unsigned grid = (unsigned)((nw * 32 + 255) / 256);
+    const float inv = (float)(1.0 / s->maxr);
+    const int NT = NCP / 8;
+    if (D == 32) {
+        if (NT == 1) k_sfp_moments<2, 1><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
+        else if (NT == 2) k_sfp_moments<2, 2><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
+        else k_sfp_moments<2, 3><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
+    } else {
+        if (NT == 1) k_sfp_moments<4, 1><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
+        else if (NT == 2) k_sfp_moments<4, 2><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
+        else k_sfp_moments<4, 3><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
+    }
+    SFP_CUDA(s, cudaGetLastError());
+    k_sfp_reduce<float><<<nmom, 256, 0, s->stream>>>(s->part, nw, nmom, s->mom);
+    SFP_CUDA(s, cudaGetLastError());
+    s->launches += 2;
+    return GX_OK;
+}
+
+// sfpsum + scaled: coeff[n * (2 maxm + 1) + m + maxm] (cosine +m, sine -m)
+extern "C" int gx_sfp_sum(GxSfp* s, int precision, double pmass, double* coeff) {
+    if (!s || !coeff) return GX_ERR_ARG;
+    if (precision != GX_PREC_MIXED && precision != GX_PREC_FP64) return GX_ERR_ARG;
+    cudaSetDevice(s->dev);
+    const int D = s->D, NCP = (s->NC + 7) / 8 * 8;
+    const int ngx = 2 * s->b.maxm + 1, maxm = s->b.maxm;
+    std::vector<double> mom((size_t)D * NCP, 0.0);
+    s->launches = 0;
+    SFP_CUDA(s, cudaEventRecord(s->e0, s->stream));
+    if (s->n > 0) {
+        int rc = sfp_moments(s, precision);
+        if (rc) return rc;
+    }
+    SFP_CUDA(s, cudaEventRecord(s->e1, s->stream));
+    if (s->n > 0)
+        SFP_CUDA(s, cudaMemcpyAsync(mom.data(), s->mom, sizeof(double) * D * NCP, cudaMemcpyDeviceToHost, s->stream));
+    SFP_CUDA(s, cudaStreamSynchronize(s->stream));
+    SFP_CUDA(s, cudaEventElapsedTime(&s->last_ms, s->e0, s->e1));
+    memset(coeff, 0, sizeof(double) * (size_t)(s->b.maxn + 1) * ngx);
+    const double fac = pmass / (s->maxr * s->maxr);
+    for (int f = 0; f < s->nfun; f++) {
+        const int m = s->msel[f], n = s->nsel[f];
+        const double* a = s->acheb.data() + (size_t)f * D;
+        const int cc = (m == 0) ? 0 : 2 * m - 1, cs = 2 * m;
+        double vc = 0, vs = 0;
+        for (int d = 0; d < D; d++) {
+            vc += a[d] * mom[(size_t)d * NCP + cc];
+            if (m > 0) vs += a[d] * mom[(size_t)d * NCP + cs];
+        }
+        const int k = n * ngx + maxm;
+        coeff[k + m] = vc * fac;
+        if (m > 0) coeff[k - m] = vs * fac;
+    }
+    return GX_OK;
+}
+
+// sfpacc for the loaded particles from scaled coefficients; acc [n][2], pot [n]
+extern "C" int gx_sfp_acc(GxSfp* s, const double* coeff, float* acc, float* pot) {
+    if (!s || !coeff || (!acc && s->n > 0)) return GX_ERR_ARG;
+    cudaSetDevice(s->dev);
+    const int D = s->D, maxm = s->b.maxm, ngx = 2 * maxm + 1;
+    std::vector<double> qs((size_t)2 * (maxm + 1) * D, 0.0);
+    for (int f = 0; f < s->nfun; f++) {
+        const int m = s->msel[f], n = s->nsel[f];
+        const double* a = s->acheb.data() + (size_t)f * D;
+        const int l = n * ngx + maxm;
+        const double cr = coeff[l + m], ci = (m > 0) ? coeff[l - m] : 0.0;
+        for (int d = 0; d < D; d++) {
+            qs[((size_t)0 * (maxm + 1) + m) * D + d] += cr * a[d];
+            qs[((size_t)1 * (maxm + 1) + m) * D + d] += ci * a[d];
+        }
+    }
+    if (!s->qc) SFP_CUDA(s, cudaMalloc((void**)&s->qc, sizeof(double) * 2 * 12 * 64));
+    SFP_CUDA(s, cudaMemcpyAsync(s->qc, qs.data(), sizeof(double) * qs.size(), cudaMemcpyHostToDevice, s->stream));
+    const int64_t n = s->n;
+    if (n > 0) {
+        float *dacc = nullptr, *dpot = nullptr;
+        SFP_CUDA(s, cudaMallocAsync((void**)&dacc, sizeof(float) * 2 * n, s->stream));
+        SFP_CUDA(s, cudaMallocAsync((void**)&dpot, sizeof(float) * n, s->stream));
+        k_sfp_acc<<<(unsigned)((n + 127) / 128), 128, 0, s->stream>>>(s->xy, s->xy + s->cap, n, s->maxr,
+                                                                    maxm, D, s->qc, dacc, dpot);
+        SFP_CUDA(s, cudaGetLastError());
+        SFP_CUDA(s, cudaMemcpyAsync(acc, dacc, sizeof(float) * 2 * n, cudaMemcpyDeviceToHost, s->stream));
+        if (pot) SFP_CUDA(s, cudaMemcpyAsync(pot, dpot, sizeof(float) * n, cudaMemcpyDeviceToHost, s->stream));
+        SFP_CUDA(s, cudaFreeAsync(dacc, s->stream));
+        SFP_CUDA(s, cudaFreeAsync(dpot, s->stream));
+    }
+    SFP_CUDA(s, cudaStreamSynchronize(s->stream));
+    return GX_OK;
+}
+
+extern "C" int gx_sfp_last_ms(const GxSfp* s, float* ms, int64_t* launches) {
+    if (!s || !ms) return GX_ERR_ARG;
+    *ms = s->last_ms;
+    if (launches) *launches = s->launches;
+    return GX_OK;
+}

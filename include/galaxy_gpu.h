@@ -126,6 +126,20 @@ typedef struct GxDiag {
     int64_t n_on_grid;
 } GxDiag;
 
+/* Abel-Jacobi basis of the SFP method (sf2d): set k, the selected
+ * functions m = minm..maxm (step nsect) x n = minn..maxn (filset.f:101-114),
+ * and the roots and coefficients the reference reads from Basis/ajKK.dat
+ * (SRC/lib15/ajsetup.f:23-58).  roots[(m*(maxn+1) + n)*maxn + i] is the
+ * (i+1)-th root of U_nm, i < n; xcoeff[(m*(maxn+1) + n)*(k+1) + i] is the
+ * coefficient of (1 - r^2)^i (ajfun.f:33-47). */
+typedef struct GxSfpBasis {
+    int32_t k;
+    int32_t minm, maxm, minn, maxn, nsect;
+    int32_t nrtab;          /* radii of the reference's look-up table (sfptab)   */
+    const double* roots;
+    const double* xcoeff;
+} GxSfpBasis;
+
 typedef struct GxCtx GxCtx;
 
 /* grdset + setgrd: validate the cards, derive the geometry, allocate the
@@ -246,6 +260,34 @@ int gx_comm_init(GxCtx* ctx, const char* id128, int nranks, int rank);
  *    GX_ERR_RANGE / GX_ERR_CUDA; no message is recorded. */
 int gx_massgn_noalloc(const GxConfig* cfg, const float* d_coords, int64_t n, float* d_mass,
                       void* stream);
+
+/* SFP method (sf2d, Abel-Jacobi basis).  A GxSfp holds the basis (as
+ * Chebyshev series, built in FP64 from roots and coefficients) and a device
+ * copy of particle positions.  SRC/lib15/sfpset.f:31-126,
+ * sfptab.f:43-78, ajfun.f:33-47, ajsetup.f:23-58. */
+typedef struct GxSfp GxSfp;
+int gx_sfp_init(const GxSfpBasis* basis, double maxr, int device, GxSfp** out);
+void gx_sfp_destroy(GxSfp* sfp);
+const char* gx_sfp_last_error(const GxSfp* sfp);
+
+/* Copy n particle records (stride floats each; x, y first) to the device. */
+int gx_sfp_load(GxSfp* sfp, const float* coords, int64_t n, int stride);
+
+/* sfpsum/sfpadd + scaled: coefficients of the loaded particles with
+ * r <= maxr, x pmass / maxr^2, into coeff[n * (2 maxm + 1) + m + maxm]
+ * (cosine terms at +m, sine terms at -m).  precision GX_PREC_MIXED runs the
+ * moment sum on the tensor cores (3xTF32, FP32 accumulate per chunk, FP64
+ * across chunks); GX_PREC_FP64 on the CUDA cores in FP64.
+ * SRC/lib15/sfpsum.f:26-47, sfpadd.f:37-93, scaled.f:53-72. */
+int gx_sfp_sum(GxSfp* sfp, int precision, double pmass, double* coeff);
+
+/* sfpacc: Cartesian accelerations [n][2] and potentials [n] (pot may be
+ * NULL) of the loaded particles from scaled coefficients (FP64 evaluation).
+ * SRC/lib15/sfpacc.f:41-112, 249-259. */
+int gx_sfp_acc(GxSfp* sfp, const double* coeff, float* acc, float* pot);
+
+/* Device ms and kernel launches of the last gx_sfp_sum. */
+int gx_sfp_last_ms(const GxSfp* sfp, float* ms, int64_t* launches);
 
 /* Page-locked host buffers for gx_loadup/gx_unload (cudaMallocHost in the
  * library's own runtime).  No reference counterpart. */

@@ -65,6 +65,14 @@ int ox_direct_field_##S(const GxConfig* cfg, const R* D, int nmass,            \
 OX_DECL(double, f64)
 OX_DECL(float, f32)
 
+/* SFP Abel-Jacobi method (gx_oracle_sfp.c), FP64 */
+double ox_ajfun(const GxSfpBasis* b, int m, int n, double r);
+double ox_ajder(const GxSfpBasis* b, int m, int n, double r);
+int ox_sfp_coeffs(const GxSfpBasis* b, int64_t n, const double* pos, int stride, double maxr,
+                  double pmass, double* coeff);
+int ox_sfp_acc(const GxSfpBasis* b, const double* coeff, int64_t n, const double* pos, int stride,
+               double maxr, double* acc, double* pot);
+
 /* icheck-style integrals in FP64 from FP64 particle records and potentials */
 int ox_icheck(const GxConfig* cfg, int64_t n, const double* pos,
               const double* acc, const double* pot, double pmass_phys,

@@ -13,7 +13,7 @@ import subprocess
 
 import numpy as np
 
-from galaxy_b200._abi import GxConfig, GxGeometry, GxDiag
+from galaxy_b200._abi import GxConfig, GxGeometry, GxDiag, GxSfpBasis
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = os.path.join(_HERE, "liboracle.so")
@@ -58,6 +58,12 @@ def _setup(L):
         getattr(L, "ox_direct_field_" + s).argtypes = [C.POINTER(GxConfig), P, C.c_int, P, P,
                                                        P, P, C.c_int, P]
     L.ox_set_threads.argtypes = [C.c_int]
+    L.ox_ajfun.argtypes = [C.POINTER(GxSfpBasis), C.c_int, C.c_int, C.c_double]
+    L.ox_ajfun.restype = C.c_double
+    L.ox_ajder.argtypes = [C.POINTER(GxSfpBasis), C.c_int, C.c_int, C.c_double]
+    L.ox_ajder.restype = C.c_double
+    L.ox_sfp_coeffs.argtypes = [C.POINTER(GxSfpBasis), i64, P, C.c_int, C.c_double, C.c_double, P]
+    L.ox_sfp_acc.argtypes = [C.POINTER(GxSfpBasis), P, i64, P, C.c_int, C.c_double, P, P]
     L.ox_icheck.argtypes = [C.POINTER(GxConfig), i64, P, P, P, C.c_double, C.POINTER(GxDiag)]
 
 
@@ -212,3 +218,31 @@ def icheck(cfg, pos, acc=None, pot=None, pmass=1.0):
     _chk(lib().ox_icheck(C.byref(cfg), pos.shape[0], _p(pos), _p(acc), _p(pot), pmass,
                          C.byref(d)), "icheck")
     return d
+
+
+def ajfun(basis, m, n, r):
+    return lib().ox_ajfun(C.byref(basis.c), m, n, float(r))
+
+
+def ajder(basis, m, n, r):
+    return lib().ox_ajder(C.byref(basis.c), m, n, float(r))
+
+
+def sfp_coeffs(basis, pos, maxr, pmass=1.0):
+    """sfpadd over all particles (table + Lagrange, FP64), scaled; layout
+    [maxn + 1][2 maxm + 1], cosine at +m, sine at -m."""
+    pos = np.ascontiguousarray(pos, np.float64)
+    out = np.zeros((basis.maxn + 1) * (2 * basis.maxm + 1), np.float64)
+    _chk(lib().ox_sfp_coeffs(C.byref(basis.c), pos.shape[0], _p(pos), pos.shape[1], float(maxr),
+                             float(pmass), _p(out)), "sfp_coeffs")
+    return out.reshape(basis.maxn + 1, 2 * basis.maxm + 1)
+
+
+def sfp_acc(basis, coeff, pos, maxr):
+    pos = np.ascontiguousarray(pos, np.float64)
+    coeff = np.ascontiguousarray(coeff, np.float64)
+    acc = np.zeros((pos.shape[0], 2), np.float64)
+    pot = np.zeros(pos.shape[0], np.float64)
+    _chk(lib().ox_sfp_acc(C.byref(basis.c), _p(coeff), pos.shape[0], _p(pos), pos.shape[1],
+                          float(maxr), _p(acc), _p(pot)), "sfp_acc")
+    return acc, pot

@@ -1,0 +1,81 @@
+"""SFP (Abel-Jacobi, k = 7, m = 0..8, n = 0..19) coefficient sum and forces.
+
+CPU: the oracle's restatement of ajfun/ajder/sfptab/sfpval (table of nrtab
+radii + 5-point Lagrange interpolation, the reference's algorithm) agrees
+with direct evaluation of the basis functions, and its coefficient sum
+agrees with the direct-evaluation sum.
+GPU: gx_sfp_sum (tensor-core moments, 3xTF32) and its FP64 path against the
+oracle's FP64 sum; gx_sfp_acc against the oracle's sfpacc.
+Basis data: tests/golden/aj07.json (tests/golden/make_aj_fixture.py).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from galaxy_b200.disk import exp_disk
+from galaxy_b200.sfp import Basis
+from oracle import oracle as ox
+
+
+@pytest.fixture(scope="module")
+def basis(golden_dir):
+    return Basis.from_json(os.path.join(golden_dir, "aj07.json"), maxm=8, maxn=19)
+
+
+def test_table_interpolation_matches_direct_basis(basis):
+    """sfpval's 5-point Lagrange interpolation (sfpval.f:33-52) on the
+    1001-radius table reproduces ajfun; the coefficient sum built on it
+    equals the sum of directly evaluated functions."""
+    pos = exp_disk(3000, seed=4).astype(np.float64)
+    maxr = 6.0
+    C = ox.sfp_coeffs(basis, pos, maxr)
+    r = np.hypot(pos[:, 0], pos[:, 1])
+    ph = np.arctan2(pos[:, 1], pos[:, 0])
+    D = np.zeros_like(C)
+    for m, n in basis.functions():
+        U = np.array([ox.ajfun(basis, m, n, ri / maxr) for ri in r])
+        if m == 0:
+            D[n, 8] = U.sum()
+        else:
+            D[n, 8 + m] = (U * np.cos(m * ph)).sum()
+            D[n, 8 - m] = (U * np.sin(m * ph)).sum()
+    D /= maxr ** 2
+    assert np.linalg.norm(C - D) / np.linalg.norm(D) < 1e-9
+
+
+def test_ajder_is_the_derivative_of_ajfun(basis):
+    h = 1e-6
+    for m, n in [(0, 0), (2, 5), (8, 19), (5, 11)]:
+        for p in (0.2, 0.5, 0.9):
+            fd = (ox.ajfun(basis, m, n, p + h) - ox.ajfun(basis, m, n, p - h)) / (2 * h)
+            assert abs(ox.ajder(basis, m, n, p) - fd) <= 1e-6 * max(1.0, abs(fd))
+
+
+@pytest.mark.gpu
+def test_sfp_sum_matches_fp64_oracle(basis):
+    from galaxy_b200.sfp import Sfp
+    pos = exp_disk(400000, seed=11)
+    ref = ox.sfp_coeffs(basis, pos.astype(np.float64), 6.0, pmass=2.5e-6)
+    with Sfp(basis, 6.0) as s:
+        s.load(pos)
+        c32 = s.sum(pmass=2.5e-6, precision=0)
+        c64 = s.sum(pmass=2.5e-6, precision=1)
+    e32 = np.linalg.norm(c32 - ref) / np.linalg.norm(ref)
+    e64 = np.linalg.norm(c64 - ref) / np.linalg.norm(ref)
+    # positions are float32 on the device; the oracle uses the same floats
+    assert e64 < 1e-9, e64
+    assert e32 < 1e-5, e32
+
+
+@pytest.mark.gpu
+def test_sfp_forces_match_oracle(basis):
+    from galaxy_b200.sfp import Sfp
+    pos = exp_disk(50000, seed=12)
+    coeff = ox.sfp_coeffs(basis, pos.astype(np.float64), 6.0, pmass=1e-5)
+    acc_ref, pot_ref = ox.sfp_acc(basis, coeff, pos.astype(np.float64), 6.0)
+    with Sfp(basis, 6.0) as s:
+        s.load(pos)
+        acc, pot = s.acc(coeff)
+    assert np.linalg.norm(acc - acc_ref) / np.linalg.norm(acc_ref) < 1e-5
+    assert np.linalg.norm(pot - pot_ref) / np.linalg.norm(pot_ref) < 1e-5
