@@ -224,9 +224,9 @@ void gx_destroy(GxCtx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     gx_comm_destroy(c);
     void* ptrs[] = {c->green32, c->green64, c->pbuf[0], c->pbuf[1], c->perm, c->origin,
-                    c->origin_tmp, c->pkey, c->p64, c->key64, c->w64, c->acc64, c->ppot,
+                    c->origin_tmp, c->pkey[0], c->pkey[1], c->pfr[0], c->pfr[1], c->p64, c->key64, c->w64, c->acc64, c->ppot,
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
-                    c->specS, c->specO, c->syntab, c->synR, c->spec64, c->out64, c->perm_next, c->rowstart,
+                    c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->perm_next, c->rowstart,
                     c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->stage, c->jrk_d,
                     c->errword, c->dsum};
     for (void* p : ptrs)
@@ -344,13 +344,15 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     const int nw = 2 * c->g.ndim;
     if (n <= c->cap && c->cap > 0) return GX_OK;
     // grow: free old
-    void* old[] = {c->pbuf[0], c->pbuf[1], c->perm, c->origin, c->origin_tmp, c->pkey, c->p64,
+    void* old[] = {c->pbuf[0], c->pbuf[1], c->perm, c->origin, c->origin_tmp, c->pkey[0], c->pkey[1],
+                   c->pfr[0], c->pfr[1], c->p64,
                    c->key64, c->w64, c->acc64, c->ppot, c->pacc, c->perm_next, c->items, c->stage};
     for (void* p : old)
         if (p) cudaFree(p);
     c->pbuf[0] = c->pbuf[1] = nullptr;
     c->perm = c->origin = c->origin_tmp = nullptr;
-    c->pkey = nullptr;
+    c->pkey[0] = c->pkey[1] = nullptr;
+    c->pfr[0] = c->pfr[1] = nullptr;
     c->p64 = nullptr;
     c->key64 = nullptr;
     c->w64 = c->acc64 = nullptr;
@@ -374,7 +376,10 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     DALLOC(c, c->perm, cap);
     DALLOC(c, c->origin, cap);
     DALLOC(c, c->origin_tmp, cap);
-    DALLOC(c, c->pkey, cap);
+    DALLOC(c, c->pkey[0], cap);
+    DALLOC(c, c->pkey[1], cap);
+    DALLOC(c, c->pfr[0], 3 * cap);
+    DALLOC(c, c->pfr[1], 3 * cap);
     DALLOC(c, c->perm_next, cap);
     // deposit work items: every row once plus one per DEP_CH particles
     c->maxitems = c->g.nrow + 1 + (int)((cap + DEP_CH - 1) / DEP_CH);
@@ -393,7 +398,7 @@ int gx_loadup(GxCtx* c, const float* coords, int64_t n) {
     int rc = alloc_particles(c, n);
     if (rc) return rc;
     c->n = n;
-    c->have_mass = c->have_field = false;
+    c->have_mass = c->have_field = c->have_keys = false;
     const int nw = 2 * c->g.ndim;
     if (n == 0) return GX_OK;
     float* staging = nullptr;

@@ -68,7 +68,9 @@ struct GxCtx {
     int32_t* perm_next = nullptr;          // permutation being built by the deposit
     int32_t* origin = nullptr;             // original load index of pbuf[cur][i]
     int32_t* origin_tmp = nullptr;
-    uint32_t* pkey = nullptr;              // per-particle rows from the last pass
+    int32_t* pkey[2] = {nullptr, nullptr}; // cell key (ncl - 1, -1 off the grid) of the particles of pbuf[i]
+    float* pfr[2] = {nullptr, nullptr};    // their cell fractions du, dt, dz: SoA [3][cap]
+    bool have_keys = false;                // pkey/pfr[cur] match pbuf[cur]
     double* p64 = nullptr;                 // SoA [2*ndim][cap] (FP64 path)
     int32_t* key64 = nullptr;
     double* w64 = nullptr;                 // [8][cap]
@@ -87,6 +89,8 @@ struct GxCtx {
     float4* specO = nullptr;               // convolved [4][nact][nkz][nr]
     float* syntab = nullptr;               // synthesis twiddle tables (gx_synth.cu)
     float* synR = nullptr;                 // vertically synthesised rows [4][nr][ngz][ncp]
+    float* fwdtab = nullptr;               // forward twiddles: azimuthal [na][ncp], vertical [ru4(2nkz)][ngz]
+    float* fwdC1 = nullptr;                // azimuthal spectra of every ring-plane row [nrow][ncp]
     double* spec64 = nullptr;
     double* out64 = nullptr;
     bool have_mass = false;
@@ -312,7 +316,7 @@ int gx_fp64_masset(GxCtx* c);
 int gx_fp64_findf(GxCtx* c, int lpot, bool polcat);
 int gx_fp64_getacc(GxCtx* c, float* acc, float* pot);
 int gx_fp64_step(GxCtx* c, int nsteps, int phys);
-int gx_deposit_rows(GxCtx* c, const float* P, const uint32_t* rowkey, int32_t* perm_out);
+int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* perm_out);
 int gx_comm_reduce_range(GxCtx* c);
 int gx_synthesis(GxCtx* c, int tmask, float* polar);
 int gx_comm_reduce_spectrum(GxCtx* c);

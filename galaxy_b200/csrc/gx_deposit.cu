@@ -9,8 +9,8 @@
 //      k_row_scan turns the counts into row starts, k_place gives every
 //      particle its slot in the row-ordered permutation;
 //   2. owner-computes deposit: a work item is up to DEP_CH particles of one
-//      base row; the CTA recomputes each particle's cell and weights and adds
-//      them, as 2^-20 fixed-point integers, into shared-memory bins of the 4
+//      base row; the CTA forms each particle's weights from the cell key and
+//      fractions the particle pass stored and adds them, as 2^-20 fixed-point integers, into shared-memory bins of the 4
 //      (2D: 2) output rows the base row feeds (same row, plane above, ring
 //      above, both); bins are staged per item as int32 rows;
 //   3. k_mass_combine sums, per mesh row, the staged rows of the base rows
@@ -136,7 +136,7 @@ __global__ void k_row_scan(int nrow, int ngz, int nr, const uint32_t* __restrict
 }
 
 // slot of every particle in the row-ordered permutation: perm[slot] = t
-__global__ void k_place(const uint32_t* __restrict__ rowkey, int64_t n, int nrow,
+__global__ void k_place(const int32_t* __restrict__ keys, int64_t n, int nrow, int na,
                         const int32_t* __restrict__ rowstart, const uint32_t* __restrict__ rowbase,
                         uint32_t* __restrict__ rowfill, int32_t* __restrict__ perm) {
     // same block -> counter-copy map as the pass that counted the rows
@@ -144,7 +144,11 @@ __global__ void k_place(const uint32_t* __restrict__ rowkey, int64_t n, int nrow
     rowfill += co;
     const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const bool act = t < n;
-    const uint32_t row = act ? rowkey[t] : 0xffffffffu;
+    uint32_t row = 0xffffffffu;
+    if (act) {
+        const int32_t key = keys[t];
+        row = (key >= 0) ? (uint32_t)(key / na) : (uint32_t)nrow;
+    }
     const uint32_t am = __ballot_sync(0xffffffffu, act);
     const uint32_t peers = __match_any_sync(0xffffffffu, row) & am;
     const int leader = __ffs(peers) - 1;
@@ -154,11 +158,13 @@ __global__ void k_place(const uint32_t* __restrict__ rowkey, int64_t n, int nrow
     if (act) perm[rowstart[row] + rowbase[co + row] + base + __popc(peers & lanemask_lt())] = (int32_t)t;
 }
 
-// owner-computes deposit of one work item per CTA iteration
+// owner-computes deposit of one work item per CTA iteration, from the cell
+// keys and fractions the particle pass stored
 template <int NW>
 __global__ void __launch_bounds__(256) k_deposit(DevGeo g, const int32_t* __restrict__ items,
                                                  const int32_t* __restrict__ nitems,
-                                                 const float* __restrict__ P, int64_t cap,
+                                                 const int32_t* __restrict__ keys,
+                                                 const float* __restrict__ fr, int64_t cap,
                                                  const int32_t* __restrict__ perm,
                                                  int32_t* __restrict__ stage,
                                                  int32_t* __restrict__ errword) {
@@ -166,17 +172,17 @@ __global__ void __launch_bounds__(256) k_deposit(DevGeo g, const int32_t* __rest
     const int na = g.na;
     constexpr int NQ = NW / 2;
     const int nit = *nitems;
-    const float* X = P;
-    const float* Y = P + cap;
-    const float* Z = (g.ndim == 3) ? P + 2 * cap : nullptr;
     for (int item = blockIdx.x; item < nit; item += gridDim.x) {
         const int row = items[3 * item], s0 = items[3 * item + 1], s1 = items[3 * item + 2];
         for (int i = threadIdx.x; i < NW * na; i += blockDim.x) bins[i] = 0;
         __syncthreads();
         for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
             const int p = perm[s];
-            const float z = Z ? Z[p] : 0.f;
-            const CellW cw = gx_cell(g, X[p], Y[p], z, false);
+            CellW cw;
+            cw.key = keys[p];
+            cw.du = fr[p];
+            cw.dt = fr[cap + p];
+            cw.dz = (NW == 8) ? fr[2 * cap + p] : 0.f;
             if (cw.key < 0 || cw.key / na != row) {
                 atomicExch(errword, 1);
                 continue;
@@ -217,8 +223,10 @@ __global__ void k_mass_combine(DevGeo g, const int32_t* __restrict__ stage,
     mass[i] = (float)((double)v * (1.0 / (double)FIXQ)) * g.pmass;
 }
 
+// cell keys and fractions of the stored particles, rows counted (masset)
 __global__ void k_row_keys(DevGeo g, const float* __restrict__ P, int64_t cap, int64_t n,
-                           uint32_t* __restrict__ rowkey, uint32_t* __restrict__ rowcnt) {
+                           int32_t* __restrict__ keys, float* __restrict__ fr,
+                           uint32_t* __restrict__ rowcnt) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const bool act = i < n;
     uint32_t row = 0;
@@ -226,13 +234,16 @@ __global__ void k_row_keys(DevGeo g, const float* __restrict__ P, int64_t cap, i
         const float z = (g.ndim == 3) ? P[2 * cap + i] : 0.f;
         const CellW c = gx_cell(g, P[i], P[cap + i], z, false);
         row = (c.key >= 0) ? (uint32_t)(c.key / g.na) : (uint32_t)g.nrow;
-        rowkey[i] = row;
+        keys[i] = c.key;
+        fr[i] = c.du;
+        fr[cap + i] = c.dt;
+        if (g.ndim == 3) fr[2 * cap + i] = c.dz;
     }
     gx_row_count(row, act, rowcnt + (size_t)(blockIdx.x & (NCOPY - 1)) * (g.nrow + 1));
 }
 
 // rows counted by the caller's pass -> permutation, deposit, mass
-int gx_deposit_rows(GxCtx* c, const float* P, const uint32_t* rowkey, int32_t* perm_out) {
+int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* perm_out) {
     const DevGeo& g = c->g;
     const int64_t n = c->n;
     int rc = gx_phase_mark(c, PH_SORT);
@@ -244,7 +255,7 @@ int gx_deposit_rows(GxCtx* c, const float* P, const uint32_t* rowkey, int32_t* p
                                           c->items, c->nitems_d, c->jrk_d);
     GX_LAUNCHED(c);
     if (n > 0) {
-        k_place<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(rowkey, n, g.nrow, c->rowstart,
+        k_place<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(keys, n, g.nrow, g.na, c->rowstart,
                                                                   c->rowbase, c->rowfill, perm_out);
         GX_LAUNCHED(c);
     }
@@ -254,11 +265,11 @@ int gx_deposit_rows(GxCtx* c, const float* P, const uint32_t* rowkey, int32_t* p
     const size_t sm = sizeof(int32_t) * (size_t)nw * g.na;
     const int grid = std::min(c->maxitems, 148 * 16);
     if (nw == 8)
-        k_deposit<8><<<grid, 256, sm, c->stream>>>(g, c->items, c->nitems_d, P, c->cap, perm_out,
-                                                   c->stage, c->errword);
+        k_deposit<8><<<grid, 256, sm, c->stream>>>(g, c->items, c->nitems_d, keys, fr, c->cap,
+                                                   perm_out, c->stage, c->errword);
     else
-        k_deposit<4><<<grid, 256, sm, c->stream>>>(g, c->items, c->nitems_d, P, c->cap, perm_out,
-                                                   c->stage, c->errword);
+        k_deposit<4><<<grid, 256, sm, c->stream>>>(g, c->items, c->nitems_d, keys, fr, c->cap,
+                                                   perm_out, c->stage, c->errword);
     GX_LAUNCHED(c);
     rc = gx_phase_mark(c, PH_COMBINE);
     if (rc) return rc;
@@ -273,11 +284,12 @@ int gx_mixed_masset(GxCtx* c) {
     const DevGeo& g = c->g;
     const int64_t n = c->n;
     if (n > 0) {
-        k_row_keys<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(g, c->pbuf[c->cur], c->cap, n,
-                                                                      c->pkey, c->rowcnt);
+        k_row_keys<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+            g, c->pbuf[c->cur], c->cap, n, c->pkey[c->cur], c->pfr[c->cur], c->rowcnt);
         GX_LAUNCHED(c);
     }
-    int rc = gx_deposit_rows(c, c->pbuf[c->cur], c->pkey, c->perm);
+    int rc = gx_deposit_rows(c, c->pkey[c->cur], c->pfr[c->cur], c->perm);
     if (rc) return rc;
+    c->have_keys = true;
     return gx_phase_end(c);
 }

@@ -1,12 +1,15 @@
 // gx_solve.cu -- field solve of the mixed-precision path (findf).
 //
-//   k_fwd3 / k_fwd2   p3manl.f:62-109 / p2manl.f:32-45: per ring, the
-//                     azimuthal real DFT of every plane restricted to the
-//                     active harmonics (the m = 0 term summed in FP64), then
-//                     (3D) the zero-padded length-2 ngz vertical DFT.  Both
-//                     are small GEMMs against twiddle matrices held in
-//                     shared memory; only the active harmonics are formed.
-//   k_conv            p3conv.f:137-230 / p2conv.f:114-181: for every
+//   k_fwd_az, k_fwd_z (3D) / k_fwd2 (2D)   p3manl.f:62-109 / p2manl.f:32-45:
+//                     the azimuthal real DFT of every ring-plane row
+//                     restricted to the active harmonics (the m = 0 term
+//                     summed in FP64), then (3D) per ring the zero-padded
+//                     length-2 ngz vertical DFT.  Both are small GEMMs
+//                     against twiddle tables staged in shared memory, with
+//                     the K sum split over lanes; only the active harmonics
+//                     are formed.
+//   k_conv            p3conv.f:137-230 / p2conv.f:114-181 (2D, and 3D grids
+//                     that gx_conv.cu's bulk-copy kernel does not take): for every
 //                     (harmonic, vertical wavenumber) the dense radial
 //                     contraction with the FP32 Green table of each field
 //                     type, the Green matrix streamed from HBM once per step.
@@ -68,77 +71,168 @@ __device__ void build_taz(float* T, int na, int nact, int ncp) {
     }
 }
 
-// ---------------------------------------------------------------------------
-// 3D forward transform, one CTA per active source ring.
-__global__ void k_fwd3(DevGeo g, int nact, int ncp, const int32_t* __restrict__ jrk,
-                       const float* __restrict__ mass, float4* __restrict__ S) {
-    extern __shared__ __align__(16) float sm[];
-    const int na = g.na, ngz = g.ngz, nkz = g.nkz, nr = g.nr;
-    const int ir = blockIdx.x;
-    // only the rings that hold mass are transformed (p3fndf.f:44-57); the
-    // others get a zero spectrum so that the sum over ranks stays exact
-    if (ir < jrk[0] - 1 || ir > min(jrk[1], nr) - 1) {
-        for (int i = threadIdx.x; i < nact * nkz; i += blockDim.x)
-            S[(size_t)i * nr + ir] = make_float4(0.f, 0.f, 0.f, 0.f);
-        return;
-    }
-    const int ldx = na + 1;
-    const int r0sz = max(ru4(ngz) * ldx, ru4(2 * nkz) * ngz);
-    float* X = sm;                       // [ru4(ngz)][na + 1], later Tz [ru4(2 nkz)][ngz]
-    float* T = X + r0sz;                 // [na][ncp]
-    float* C1 = T + na * ncp;            // [ru4(ngz)][ncp]
-    const float* src = mass + (size_t)ir * ngz * na;
-    for (int i = threadIdx.x; i < ngz * na; i += blockDim.x) {
-        int z = i / na, j = i - z * na;
-        X[z * ldx + j] = src[i];
-    }
-    for (int i = ngz * ldx + threadIdx.x; i < ru4(ngz) * ldx; i += blockDim.x) X[i] = 0.f;
-    build_taz(T, na, nact, ncp);
-    __syncthreads();
-    sgemm44(ngz, ncp, na, X, ldx, T, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
+// C[M][N] = A[M][K] * B[K][N] in shared memory, 4x4 register tiles with the
+// K sum split over KS adjacent lanes (lane ks takes k = ks, ks + KS, ...) and
+// reduced by shuffles; epi(r0, c0, acc) runs on the lane with ks == 0.  The
+// tile loop has the same trip count on every thread (the shuffles need the
+// whole warp); blockDim.x must be a multiple of 32.
+template <int KS, class Epi>
+__device__ __forceinline__ void sgemm44_sk(int M, int N, int K, const float* A, int lda,
+                                           const float* B, int ldb, Epi epi) {
+    const int tilesN = (N + 3) >> 2, tilesM = (M + 3) >> 2, nt = tilesM * tilesN;
+    const int per = blockDim.x / KS, ks = threadIdx.x % KS;
+    for (int t0 = 0; t0 < nt; t0 += per) {
+        const int t = t0 + threadIdx.x / KS;
+        const bool act = t < nt;
+        const int tm = act ? t / tilesN : 0, tn = act ? t - tm * tilesN : 0;
+        const int r0 = tm * 4, c0 = tn * 4;
+        float acc[4][4];
 #pragma unroll
         for (int i = 0; i < 4; i++)
 #pragma unroll
-            for (int j = 0; j < 4; j++) C1[(r0 + i) * ncp + c0 + j] = acc[i][j];
-    });
-    __syncthreads();
-    // m = 0 (when active) in FP64
-    if (c_act_m[0] == 0) {
-        for (int z = threadIdx.x; z < ngz; z += blockDim.x) {
-            double s = 0.0;
-            for (int j = 0; j < na; j++) s += (double)X[z * ldx + j];
-            C1[z * ncp] = (float)s;
+            for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+        if (act) {
+            const float* ap = A + (size_t)r0 * lda;
+            const float* bp = B + c0;
+#pragma unroll 4
+            for (int k = ks; k < K; k += KS) {
+                const float4 b = *reinterpret_cast<const float4*>(bp + (size_t)k * ldb);
+                const float a0 = ap[k], a1 = ap[lda + k], a2 = ap[2 * lda + k], a3 = ap[3 * lda + k];
+                acc[0][0] += a0 * b.x; acc[0][1] += a0 * b.y; acc[0][2] += a0 * b.z; acc[0][3] += a0 * b.w;
+                acc[1][0] += a1 * b.x; acc[1][1] += a1 * b.y; acc[1][2] += a1 * b.z; acc[1][3] += a1 * b.w;
+                acc[2][0] += a2 * b.x; acc[2][1] += a2 * b.y; acc[2][2] += a2 * b.z; acc[2][3] += a2 * b.w;
+                acc[3][0] += a3 * b.x; acc[3][1] += a3 * b.y; acc[3][2] += a3 * b.z; acc[3][3] += a3 * b.w;
+            }
         }
+#pragma unroll
+        for (int o = 1; o < KS; o <<= 1)
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] += __shfl_xor_sync(0xffffffffu, acc[i][j], o);
+        if (act && ks == 0) epi(r0, c0, acc);
     }
-    __syncthreads();
-    // vertical twiddles Tz[2k][z] = cos(pi k z / ngz), Tz[2k+1][z] = -sin(...)
-    float* Tz = X;
-    for (int i = threadIdx.x; i < ru4(2 * nkz) * ngz; i += blockDim.x) {
-        int r = i / ngz, z = i - r * ngz;
-        int k = r >> 1;
+}
+
+// forward twiddle tables, built once per context:
+//   Taz[j][2a] = cos(2 pi m_a j / na), Taz[j][2a+1] = -sin(...)   [na][ncp]
+//   Tz[2k][z] = cos(pi k z / ngz), Tz[2k+1][z] = -sin(...)       [ru4(2 nkz)][ngz]
+__global__ void k_fwdtab(DevGeo g, int nact, int ncp, float* __restrict__ Taz, float* __restrict__ Tz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int na = g.na, ngz = g.ngz, nkz = g.nkz;
+    if (i < na * ncp) {
+        const int j = i / ncp, c = i - j * ncp;
+        float v = 0.f;
+        if (c < 2 * nact) {
+            const int m = c_act_m[c >> 1];
+            const int idx = (int)(((int64_t)m * j) % na);
+            float sn, co;
+            sincospif(2.0f * (float)idx / (float)na, &sn, &co);
+            v = (c & 1) ? -sn : co;
+        }
+        Taz[i] = v;
+    }
+    if (g.ndim == 3 && i < ru4(2 * nkz) * ngz) {
+        const int r = i / ngz, z = i - r * ngz, k = r >> 1;
         float v = 0.f;
         if (k < nkz) {
-            int idx = (int)(((int64_t)k * z) % (2 * ngz));
-            float s, co;
-            sincospif((float)idx / (float)ngz, &s, &co);
-            v = (r & 1) ? -s : co;
+            const int idx = (int)(((int64_t)k * z) % (2 * ngz));
+            float sn, co;
+            sincospif((float)idx / (float)ngz, &sn, &co);
+            v = (r & 1) ? -sn : co;
         }
         Tz[i] = v;
     }
+}
+
+// 3D forward, azimuthal part (p3manl.f:62-83): the active-harmonic DFT of
+// FWD_RB ring-plane rows per CTA, C1[row][2a, 2a+1] = (a_m, b_m); the m = 0
+// column summed in FP64.  Rows of rings without mass are skipped (the
+// vertical part zeroes their spectrum).
+#define FWD_RB 32
+__global__ void __launch_bounds__(288) k_fwd_az(DevGeo g, int ncp, const int32_t* __restrict__ jrk,
+                                                const float* __restrict__ mass,
+                                                const float* __restrict__ Taz,
+                                                float* __restrict__ C1) {
+    extern __shared__ __align__(16) float sm[];
+    const int na = g.na, ngz = g.ngz, nr = g.nr;
+    const int row0 = blockIdx.x * FWD_RB;
+    const int rlo = (max(jrk[0], 1) - 1) * ngz, rhi = min(jrk[1], nr) * ngz;  // active rows [rlo, rhi)
+    if (row0 + FWD_RB <= rlo || row0 >= rhi) return;
+    const int nrows = min(FWD_RB, g.nrow - row0);
+    const int ldx = na + 1;
+    float* X = sm;                 // [FWD_RB][na + 1]
+    float* T = X + FWD_RB * ldx;   // [na][ncp]
+    for (int i = threadIdx.x; i < FWD_RB * na; i += blockDim.x) {
+        const int r = i / na, j = i - r * na;
+        X[r * ldx + j] = (r < nrows) ? mass[(size_t)(row0 + r) * na + j] : 0.f;
+    }
+    for (int i = threadIdx.x; i < na * ncp / 4; i += blockDim.x)
+        reinterpret_cast<float4*>(T)[i] = reinterpret_cast<const float4*>(Taz)[i];
     __syncthreads();
-    sgemm44(2 * nkz, ncp, ngz, Tz, ngz, C1, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
-        // rows r0 = 2k, 2k+1, 2k+2, 2k+3; cols c0 = 2a, 2a+1, 2a+2, 2a+3
+    sgemm44_sk<4>(FWD_RB, ncp, na, X, ldx, T, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            if (r0 + i >= nrows) continue;
+            *reinterpret_cast<float4*>(C1 + (size_t)(row0 + r0 + i) * ncp + c0) =
+                make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+        }
+    });
+    if (c_act_m[0] == 0) {
+        __syncthreads();  // column 0 of the GEMM is written before the FP64 sum replaces it
+        // 8 lanes per row, FP64 partial sums over na / 8 points each
+        const int r = threadIdx.x >> 3, q = threadIdx.x & 7;
+        double s = 0.0;
+        if (r < FWD_RB)
+            for (int j = q; j < na; j += 8) s += (double)X[r * ldx + j];
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (r < nrows && q == 0) C1[(size_t)(row0 + r) * ncp] = (float)s;
+    }
+}
+
+// 3D forward, vertical part (p3manl.f:84-109): per ring, the zero-padded
+// length-2 ngz DFT of the azimuthal spectra, FWD_KR output rows (2 per kz)
+// per CTA.  S[(a nkz + k) nr + ir] = (A_c, B_c, A_s, B_s).
+#define FWD_KR 32
+__global__ void __launch_bounds__(288) k_fwd_z(DevGeo g, int nact, int ncp,
+                                               const int32_t* __restrict__ jrk,
+                                               const float* __restrict__ C1,
+                                               const float* __restrict__ Tz, float4* __restrict__ S) {
+    extern __shared__ __align__(16) float sm[];
+    const int ngz = g.ngz, nkz = g.nkz, nr = g.nr;
+    const int ir = blockIdx.x, kr0 = blockIdx.y * FWD_KR;   // first output row (2 kz0)
+    const int nrow_out = min(FWD_KR, 2 * nkz - kr0);
+    if (ir < jrk[0] - 1 || ir > min(jrk[1], nr) - 1) {
+        // only the rings that hold mass are transformed (p3fndf.f:44-57); the
+        // others get a zero spectrum so that the sum over ranks stays exact
+        for (int i = threadIdx.x; i < nact * (nrow_out / 2); i += blockDim.x) {
+            const int a = i / (nrow_out / 2), k = kr0 / 2 + (i - a * (nrow_out / 2));
+            S[((size_t)a * nkz + k) * nr + ir] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+        return;
+    }
+    float* B = sm;                      // [ngz][ncp]
+    float* Tk = B + ngz * ncp;          // [FWD_KR][ngz]
+    const float* src = C1 + (size_t)ir * ngz * ncp;
+    for (int i = threadIdx.x; i < ngz * ncp / 4; i += blockDim.x)
+        reinterpret_cast<float4*>(B)[i] = reinterpret_cast<const float4*>(src)[i];
+    for (int i = threadIdx.x; i < FWD_KR * ngz; i += blockDim.x)
+        Tk[i] = (i < nrow_out * ngz) ? Tz[(size_t)kr0 * ngz + i] : 0.f;
+    __syncthreads();
+    sgemm44_sk<4>(nrow_out, ncp, ngz, Tk, ngz, B, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
+        // rows r0 = 2k, 2k+1, 2k+2, 2k+3 (relative to kr0); cols c0 = 2a .. 2a+3
 #pragma unroll
         for (int dk = 0; dk < 2; dk++) {
-            int k = (r0 >> 1) + dk;
-            if (k >= nkz) continue;
+            const int k = (kr0 + r0) / 2 + dk;
+            if (k >= nkz || r0 + 2 * dk >= nrow_out) continue;
 #pragma unroll
             for (int da = 0; da < 2; da++) {
-                int a = (c0 >> 1) + da;
+                const int a = (c0 >> 1) + da;
                 if (a >= nact) continue;
-                float4 v = make_float4(acc[2 * dk][2 * da], acc[2 * dk + 1][2 * da],
-                                       acc[2 * dk][2 * da + 1], acc[2 * dk + 1][2 * da + 1]);
-                S[((size_t)a * nkz + k) * nr + ir] = v;
+                S[((size_t)a * nkz + k) * nr + ir] =
+                    make_float4(acc[2 * dk][2 * da], acc[2 * dk + 1][2 * da], acc[2 * dk][2 * da + 1],
+                                acc[2 * dk + 1][2 * da + 1]);
             }
         }
     });
@@ -264,6 +358,9 @@ __global__ void __launch_bounds__(256) k_conv(DevGeo g, int nact, int tmask,
     }
 }
 
+bool gx_conv_bulk_ok(const DevGeo& g);
+int gx_conv_bulk(GxCtx* c, int nact, int tmask);
+
 // ---------------------------------------------------------------------------
 static int set_act(GxCtx* c) {
     GX_CUDA(c, cudaMemcpyToSymbolAsync(c_act_m, c->spec.m, sizeof(int) * 260, 0,
@@ -271,11 +368,6 @@ static int set_act(GxCtx* c) {
     return GX_OK;
 }
 
-static size_t fwd3_smem(const DevGeo& g, int ncp) {
-    int ldx = g.na + 1;
-    int r0sz = std::max(ru4(g.ngz) * ldx, ru4(2 * g.nkz) * g.ngz);
-    return sizeof(float) * ((size_t)r0sz + (size_t)g.na * ncp + (size_t)ru4(g.ngz) * ncp);
-}
 // findf for the mixed path: mass -> field (and optional polar copy)
 int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
     const DevGeo& g = c->g;
@@ -296,9 +388,25 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
     rc = gx_comm_reduce_range(c);
     if (rc) return rc;
     if (g.ndim == 3) {
-        size_t sm = fwd3_smem(g, ncp);
-        GX_CUDA(c, cudaFuncSetAttribute(k_fwd3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_fwd3<<<g.nr, 512, sm, c->stream>>>(g, nact, ncp, c->jrk_d, c->mass, c->specS);
+        const size_t ntaz = (size_t)g.na * ncp, ntz = (size_t)ru4(2 * g.nkz) * g.ngz;
+        if (!c->fwdtab) {
+            GX_CUDA(c, cudaMalloc((void**)&c->fwdtab, sizeof(float) * (ntaz + ntz)));
+            const size_t mx = std::max(ntaz, ntz);
+            k_fwdtab<<<(unsigned)((mx + 255) / 256), 256, 0, c->stream>>>(g, nact, ncp, c->fwdtab,
+                                                                          c->fwdtab + ntaz);
+            GX_LAUNCHED(c);
+        }
+        if (!c->fwdC1) GX_CUDA(c, cudaMalloc((void**)&c->fwdC1, sizeof(float) * (size_t)g.nrow * ncp));
+        size_t sm = sizeof(float) * ((size_t)FWD_RB * (g.na + 1) + ntaz);
+        GX_CUDA(c, cudaFuncSetAttribute(k_fwd_az, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_fwd_az<<<(g.nrow + FWD_RB - 1) / FWD_RB, 288, sm, c->stream>>>(g, ncp, c->jrk_d, c->mass,
+                                                                         c->fwdtab, c->fwdC1);
+        GX_LAUNCHED(c);
+        sm = sizeof(float) * ((size_t)g.ngz * ncp + (size_t)FWD_KR * g.ngz);
+        GX_CUDA(c, cudaFuncSetAttribute(k_fwd_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        dim3 gz(g.nr, (2 * g.nkz + FWD_KR - 1) / FWD_KR);
+        k_fwd_z<<<gz, 288, sm, c->stream>>>(g, nact, ncp, c->jrk_d, c->fwdC1, c->fwdtab + ntaz,
+                                            c->specS);
         GX_LAUNCHED(c);
     } else {
         size_t sm = sizeof(float) * ((size_t)RB2 * (g.na + 1) + (size_t)g.na * ncp);
@@ -311,7 +419,10 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
     if (rc) return rc;
     rc = gx_phase_mark(c, PH_CONV);
     if (rc) return rc;
-    {
+    if (gx_conv_bulk_ok(g)) {
+        rc = gx_conv_bulk(c, nact, tmask);
+        if (rc) return rc;
+    } else {
         size_t sm = sizeof(float4) * (size_t)g.nr * 9;
         dim3 grid(nact, g.nkz);
         bool vec = (g.nr % 4) == 0;

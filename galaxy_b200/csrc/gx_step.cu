@@ -1,14 +1,16 @@
 // gx_step.cu -- particle side of the mixed-precision path.
 //
 //   k_push         one pass per step over the particles in row-sorted order
-//                  (getacc + stpgrp + the new cell key of massgn's weight
-//                  call): old cell and weights (weight.f:61-101, 196-250),
+//                  (getacc + stpgrp + the new cell of massgn's weight
+//                  call): weights of the stored cell (weight.f:61-101, 196-250),
 //                  gather of the float4 field at the 4/8 corners
 //                  (grdacc.f:40-84, 189-218), rigid halo (getacc.f:103-122,
 //                  frhalo.f:55-56), v += a, x += v (stpgrp.f:26-32), off-grid
-//                  test (offgrd.f:51-77), new ring-plane row of the key.
-//                  The pass also counts the new rows for the deposit's
-//                  counting sort (gx_deposit.cu).
+//                  test (offgrd.f:51-77), the new cell key and fractions
+//                  (stored for the deposit and the next step: the cell of
+//                  each position is computed once).  The pass also counts
+//                  the new rows for the deposit's counting sort
+//                  (gx_deposit.cu).
 #include <algorithm>
 
 #include "gx_common.cuh"
@@ -19,24 +21,25 @@ __device__ __forceinline__ uint32_t row_of(const DevGeo& g, const CellW& c) {
     return (c.key >= 0) ? (uint32_t)(c.key / g.na) : (uint32_t)g.nrow;
 }
 
-// interpolated acceleration and potential at (x, y, z): grdacc + halfrc
-__device__ __forceinline__ void gx_accel(const DevGeo& g, const float4* __restrict__ F, float x,
-                                         float y, float z, float& ax, float& ay, float& az,
-                                         float& ph) {
+// interpolated acceleration and potential of a particle at (x, y, z) whose
+// interpolation cell is cw: grdacc + halfrc
+__device__ __forceinline__ void gx_accel_cell(const DevGeo& g, const float4* __restrict__ F,
+                                              const CellW& cw, float x, float y, float z, float& ax,
+                                              float& ay, float& az, float& ph) {
     ax = ay = az = ph = 0.f;
-    CellW cw = gx_cell(g, x, y, z, true);
-    if (cw.key < 0) return;
-    float w[8];
-    int ic[8];
-    gx_weights(g, cw, w);
-    const int nc = gx_corners(g, cw.key, ic);
-    for (int k = 0; k < nc; k++) {
-        if (ic[k] < 0) continue;
-        const float4 f = __ldg(F + ic[k]);
-        ax += f.x * w[k];
-        ay += f.y * w[k];
-        az += f.z * w[k];
-        ph += f.w * w[k];
+    if (cw.key >= 0) {
+        float w[8];
+        int ic[8];
+        gx_weights(g, cw, w);
+        const int nc = gx_corners(g, cw.key, ic);
+        for (int k = 0; k < nc; k++) {
+            if (ic[k] < 0) continue;
+            const float4 f = __ldg(F + ic[k]);
+            ax += f.x * w[k];
+            ay += f.y * w[k];
+            az += f.z * w[k];
+            ph += f.w * w[k];
+        }
     }
     if (g.halo == 1) {
         // cored isothermal halo (frhalo.f:55-56): F(r) = -v^2 r / (r^2 + rc^2)
@@ -53,15 +56,27 @@ __device__ __forceinline__ void gx_accel(const DevGeo& g, const float4* __restri
     }
 }
 
-// the fused particle pass of one step; counts the new rows for the
-// deposit's counting sort
+__device__ __forceinline__ void gx_accel(const DevGeo& g, const float4* __restrict__ F, float x,
+                                         float y, float z, float& ax, float& ay, float& az,
+                                         float& ph) {
+    const CellW cw = gx_cell(g, x, y, z, true);
+    gx_accel_cell(g, F, cw, x, y, z, ax, ay, az, ph);
+}
+
+// the fused particle pass of one step.  The interpolation cell of the
+// current position is the one the previous pass (or masset) stored; the
+// pass stores the cell of the new position for the deposit and the next
+// step, and counts the new rows for the deposit's counting sort.
 __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict__ Pin,
                                               float* __restrict__ Pout, int64_t cap, int64_t n,
                                               const int32_t* __restrict__ perm,
                                               const int32_t* __restrict__ orig_in,
                                               int32_t* __restrict__ orig_out,
                                               const float4* __restrict__ F,
-                                              uint32_t* __restrict__ rowkey,
+                                              const int32_t* __restrict__ key_in,
+                                              const float* __restrict__ fr_in,
+                                              int32_t* __restrict__ key_out,
+                                              float* __restrict__ fr_out,
                                               uint32_t* __restrict__ rowcnt,
                                               float* __restrict__ pot) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -81,8 +96,18 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
             vy = Pin[3 * cap + p];
         }
         const int32_t o = orig_in[p];
+        CellW cw;
+        if (g.nsect > 1) {
+            // the stored cell is folded into the first sector; interpolation is not
+            cw = gx_cell(g, x, y, z, true);
+        } else {
+            cw.key = key_in[p];
+            cw.du = fr_in[p];
+            cw.dt = fr_in[cap + p];
+            cw.dz = d3 ? fr_in[2 * cap + p] : 0.f;
+        }
         float ax, ay, az, ph;
-        gx_accel(g, F, x, y, z, ax, ay, az, ph);
+        gx_accel_cell(g, F, cw, x, y, z, ax, ay, az, ph);
         vx += ax;
         vy += ay;
         x += vx;
@@ -105,8 +130,11 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
         orig_out[s] = o;
         if (pot) pot[s] = ph;
         const CellW cn = gx_cell(g, x, y, z, false);
+        key_out[s] = cn.key;
+        fr_out[s] = cn.du;
+        fr_out[cap + s] = cn.dt;
+        if (d3) fr_out[2 * cap + s] = cn.dz;
         row = row_of(g, cn);
-        rowkey[s] = row;
     }
     gx_row_count(row, act, rowcnt + (size_t)(blockIdx.x & (NCOPY - 1)) * (g.nrow + 1));
 }
@@ -128,10 +156,30 @@ __global__ void k_getacc(DevGeo g, const float* __restrict__ P, int64_t cap, int
     if (pot) pot[o] = ph;
 }
 
+// cell keys and fractions of the stored particles (when the mass array came
+// from gx_set_mass rather than a deposit of these particles)
+__global__ void k_cell_keys(DevGeo g, const float* __restrict__ P, int64_t cap, int64_t n,
+                            int32_t* __restrict__ keys, float* __restrict__ fr) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float z = (g.ndim == 3) ? P[2 * cap + i] : 0.f;
+    const CellW cw = gx_cell(g, P[i], P[cap + i], z, false);
+    keys[i] = cw.key;
+    fr[i] = cw.du;
+    fr[cap + i] = cw.dt;
+    if (g.ndim == 3) fr[2 * cap + i] = cw.dz;
+}
+
 // ---------------------------------------------------------------------------
 int gx_mixed_step(GxCtx* c, int nsteps, int phys) {
     const DevGeo& g = c->g;
     const int64_t n = c->n;
+    if (!c->have_keys && n > 0) {
+        k_cell_keys<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(g, c->pbuf[c->cur], c->cap, n,
+                                                                       c->pkey[c->cur], c->pfr[c->cur]);
+        GX_LAUNCHED(c);
+        c->have_keys = true;
+    }
     for (int s = 0; s < nsteps; s++) {
         const bool last = (s == nsteps - 1);
         int rc = gx_mixed_findf(c, phys && last, true);
@@ -142,14 +190,15 @@ int gx_mixed_step(GxCtx* c, int nsteps, int phys) {
         if (n > 0) {
             k_push<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
                 g, c->pbuf[c->cur], c->pbuf[nxt], c->cap, n, c->perm, c->origin, c->origin_tmp,
-                c->field, c->pkey, c->rowcnt, (phys && last) ? c->ppot : nullptr);
+                c->field, c->pkey[c->cur], c->pfr[c->cur], c->pkey[nxt], c->pfr[nxt], c->rowcnt,
+                (phys && last) ? c->ppot : nullptr);
             GX_LAUNCHED(c);
         }
         std::swap(c->origin, c->origin_tmp);
         c->cur = nxt;
         // the pass wrote particles in processing order; the new permutation
         // orders them by their new rows
-        rc = gx_deposit_rows(c, c->pbuf[c->cur], c->pkey, c->perm_next);
+        rc = gx_deposit_rows(c, c->pkey[c->cur], c->pfr[c->cur], c->perm_next);
         if (rc) return rc;
         std::swap(c->perm, c->perm_next);
     }

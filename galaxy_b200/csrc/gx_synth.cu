@@ -87,7 +87,9 @@ __global__ void k_syntab(DevGeo g, ActList act, int nact, float scale, float* WA
 }
 
 // vertical synthesis, one CTA per (ring, field type); R[t][ir][z][ncp]
-__global__ void __launch_bounds__(128) k_synz(DevGeo g, int nact, int ncp, int tmask,
+#define SYNZ_KS 2
+#define SYNZ_THREADS 288
+__global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int ncp, int tmask,
                                              const float4* __restrict__ O, SynTab tb,
                                              float* __restrict__ R) {
     extern __shared__ __align__(16) float sm[];
@@ -149,17 +151,22 @@ __global__ void __launch_bounds__(128) k_synz(DevGeo g, int nact, int ncp, int t
         }
     }
     __syncthreads();
-    const int tilesN = ncp >> 2, tilesM = nz4 >> 2;
-    for (int tile = threadIdx.x; tile < tilesM * tilesN; tile += blockDim.x) {
-        const int tm = tile / tilesN, tn = tile - tm * tilesN;
+    // 4x4 tiles of (z, column); the k sums split over SYNZ_KS adjacent lanes
+    const int tilesN = ncp >> 2, tilesM = nz4 >> 2, nt = tilesM * tilesN;
+    const int per = blockDim.x / SYNZ_KS, ks = threadIdx.x % SYNZ_KS;
+    for (int t0 = 0; t0 < nt; t0 += per) {
+        const int tile = t0 + threadIdx.x / SYNZ_KS;
+        const bool act = tile < nt;
+        const int tm = act ? tile / tilesN : 0, tn = act ? tile - tm * tilesN : 0;
         const int z0 = tm * 4, c0 = tn * 4;
         float EA[4][4], EB[4][4], OA[4][4], OB[4][4];
 #pragma unroll
         for (int r = 0; r < 4; r++)
 #pragma unroll
             for (int q = 0; q < 4; q++) EA[r][q] = EB[r][q] = OA[r][q] = OB[r][q] = 0.f;
+        const int ke = act ? KE : 0, ko = act ? KO : 0;
 #pragma unroll 2
-        for (int i = 0; i < KE; i++) {
+        for (int i = ks; i < ke; i += SYNZ_KS) {
             const float4 a4 = *reinterpret_cast<const float4*>(Ae + i * ncp + c0);
             const float4 b4 = *reinterpret_cast<const float4*>(Be + i * ncp + c0);
 #pragma unroll
@@ -170,7 +177,7 @@ __global__ void __launch_bounds__(128) k_synz(DevGeo g, int nact, int ncp, int t
             }
         }
 #pragma unroll 2
-        for (int i = 0; i < KO; i++) {
+        for (int i = ks; i < ko; i += SYNZ_KS) {
             const float4 a4 = *reinterpret_cast<const float4*>(Ao + i * ncp + c0);
             const float4 b4 = *reinterpret_cast<const float4*>(Bo + i * ncp + c0);
 #pragma unroll
@@ -180,6 +187,18 @@ __global__ void __launch_bounds__(128) k_synz(DevGeo g, int nact, int ncp, int t
                 OB[r][0] += wb * b4.x; OB[r][1] += wb * b4.y; OB[r][2] += wb * b4.z; OB[r][3] += wb * b4.w;
             }
         }
+#pragma unroll
+        for (int o = 1; o < SYNZ_KS; o <<= 1)
+#pragma unroll
+            for (int r = 0; r < 4; r++)
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    EA[r][q] += __shfl_xor_sync(0xffffffffu, EA[r][q], o);
+                    EB[r][q] += __shfl_xor_sync(0xffffffffu, EB[r][q], o);
+                    OA[r][q] += __shfl_xor_sync(0xffffffffu, OA[r][q], o);
+                    OB[r][q] += __shfl_xor_sync(0xffffffffu, OB[r][q], o);
+                }
+        if (!act || ks != 0) continue;
 #pragma unroll
         for (int r = 0; r < 4; r++) {
             const int z = z0 + r;
@@ -311,7 +330,7 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar) {
         const size_t sm = sizeof(float) * (2 * nWe + 2 * nWo + (size_t)(KE + KO) * 2 * ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_synz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         dim3 grid(g.nr, 4);
-        k_synz<<<grid, 128, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, tb, c->synR);
+        k_synz<<<grid, SYNZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, tb, c->synR);
         GX_LAUNCHED(c);
     }
     {
