@@ -7,7 +7,7 @@
 // mixing of the type.  Each Green entry is used for 4 MACs and read once per
 // step, so the kernel's job is to keep the HBM pipe full.
 //
-// Persistent CTAs of 8 consumer warps and 1 producer warp.  Work items are
+// Persistent CTAs of 16 consumer warps and 1 producer warp.  Work items are
 // (m, kz) pairs dealt round-robin to CTAs.  The producer walks the same tile
 // sequence as the consumers -- items, then valid types, then chunks of rows
 // (source rings js..ks) of the nr x nr matrix -- and copies each tile, a
@@ -23,7 +23,7 @@
 #include "gx_common.cuh"
 
 namespace {
-constexpr int NCW = 8;                        // consumer warps
+constexpr int NCW = 16;                       // consumer warps
 constexpr int MAXST = 8;                      // most stages in the ring
 constexpr uint32_t SPIN_LIMIT = 1u << 22;     // try_wait polls before giving up
 
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) k_conv_bulk(ConvArgs A) {
 }
 
 // host side: true when the bulk path handles this geometry
-bool gx_conv_bulk_ok(const DevGeo& g) { return g.ndim == 3 && g.nr % 4 == 0 && g.nr <= 256; }
+bool gx_conv_bulk_ok(const DevGeo& g) { return g.ndim == 3 && g.nr % 4 == 0 && g.nr <= 128; }
 
 int gx_conv_bulk(GxCtx* c, int nact, int tmask) {
     const DevGeo& g = c->g;
@@ -256,10 +256,10 @@ int gx_conv_bulk(GxCtx* c, int nact, int tmask) {
     GX_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->dev));
     GX_CUDA(c, cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
     const size_t fixed = sizeof(float4) * (size_t)g.nr * (NCW + 2) + (2 * MAXST + 4) * sizeof(uint64_t);
-    // rows per tile: the whole matrix or 32 KB of it; as many stages as fit in 192 KB
+    // rows per tile: the whole matrix or 32 KB of it; as many stages as fit in 160 KB
     const int R = std::min(g.nr, (int)(32768 / (g.nr * sizeof(float))));
     const size_t stage_bytes = (size_t)R * g.nr * sizeof(float);
-    const size_t budget = std::min<size_t>((size_t)smem_max - fixed, 196608);
+    const size_t budget = std::min<size_t>((size_t)smem_max - fixed, 163840);
     int nst = (int)std::min<size_t>(MAXST, budget / stage_bytes);
     if (nst < 2) return c->err = "radial contraction: shared memory too small", GX_ERR_ARG;
     const size_t smem = nst * stage_bytes + fixed;
@@ -277,13 +277,8 @@ int gx_conv_bulk(GxCtx* c, int nact, int tmask) {
     A.errword = c->errword;
     for (int i = 0; i < 260; i++) A.act_m[i] = (i < nact) ? c->spec.m[i] : 0;
     const int grid = std::min(A.nitems, dev_sms);
-    if (g.nr <= 128) {
-        GX_CUDA(c, cudaFuncSetAttribute(k_conv_bulk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_conv_bulk<1><<<grid, (NCW + 1) * 32, smem, c->stream>>>(A);
-    } else {
-        GX_CUDA(c, cudaFuncSetAttribute(k_conv_bulk<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_conv_bulk<2><<<grid, (NCW + 1) * 32, smem, c->stream>>>(A);
-    }
+    GX_CUDA(c, cudaFuncSetAttribute(k_conv_bulk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_conv_bulk<1><<<grid, (NCW + 1) * 32, smem, c->stream>>>(A);
     GX_LAUNCHED(c);
     return GX_OK;
 }

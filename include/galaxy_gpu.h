@@ -289,6 +289,53 @@ int gx_sfp_acc(GxSfp* sfp, const double* coeff, float* acc, float* pot);
 /* Device ms and kernel launches of the last gx_sfp_sum. */
 int gx_sfp_last_ms(const GxSfp* sfp, float* ms, int64_t* launches);
 
+/* Ensemble of independent 2D discs sharing one grid geometry (one Green
+ * table), advanced together: every step is one persistent cooperative
+ * launch for all discs (field solve per disc, then push + deposit of every
+ * particle), and batches of 16 step launches are replayed from a CUDA graph.
+ * Each disc follows the single-disc run of SRC/progs/galaxy.f:107-148
+ * (findf, getacc + stpgrp, massgn: the same cell keys, weights and integer
+ * deposit; FP32 transforms summed in a different order, so fields agree to
+ * FP32 rounding, not bitwise).  No single reference routine: it batches the
+ * reference's per-run loop over runs.
+ *  - cfg: the shared 2D grid (ndim 2, mixed precision; cfg->pmass ignored);
+ *    at most 12800 cells (16 B per cell of shared memory).
+ *  - counts[ndisc], pmass[ndisc]: particles and particle mass of each disc;
+ *    coords: sum(counts) records (x, y, vx, vy) in grid units, disc after
+ *    disc.  max_steps bounds the recorded A2 series.
+ *  - create builds the Green table, deposits the initial mass (masset) and
+ *    records A2 at step 0. */
+typedef struct GxEnsemble GxEnsemble;
+int gx_ensemble_create(const GxConfig* cfg, int ndisc, const int64_t* counts, const float* pmass,
+                       const float* coords, int max_steps, GxEnsemble** out);
+void gx_ensemble_destroy(GxEnsemble* ens);
+const char* gx_ensemble_last_error(const GxEnsemble* ens);
+
+/* Autotuner: times each (threads per CTA, particles per chunk) candidate
+ * over a few steps from a snapshot of the state, restores the state and
+ * keeps the fastest; returns the choice. */
+int gx_ensemble_tune(GxEnsemble* ens, int* threads, int* chunk);
+
+/* Current launch shape: threads per CTA, particles per chunk, CTAs, and
+ * whether the steps are replayed from a CUDA graph (1) or launched one by
+ * one (0). */
+int gx_ensemble_config(const GxEnsemble* ens, int* threads, int* chunk, int* grid, int* graph);
+
+/* Advance every disc nsteps leapfrog steps. */
+int gx_ensemble_step(GxEnsemble* ens, int nsteps);
+int gx_ensemble_steps_done(const GxEnsemble* ens, int64_t* n);
+
+/* m = 2 amplitude of every disc after every step:
+ * out[(s * ndisc + d) * 2 + {0, 1}] = mean over the disc's particles on the
+ * grid of (cos 2 phi, sin 2 phi), s = 0 .. steps_done (FP64 sums). */
+int gx_ensemble_a2(GxEnsemble* ens, double* out, int64_t cap);
+
+/* Particle records (x, y, vx, vy) of all discs, in the order of create. */
+int gx_ensemble_unload(GxEnsemble* ens, float* coords);
+
+/* Device ms and kernel launches of the last gx_ensemble_step. */
+int gx_ensemble_last_ms(const GxEnsemble* ens, float* ms, int64_t* launches);
+
 /* Page-locked host buffers for gx_loadup/gx_unload (cudaMallocHost in the
  * library's own runtime).  No reference counterpart. */
 int gx_host_alloc(int64_t bytes, void** ptr);
