@@ -316,6 +316,66 @@ def run_sfp(n=20_000_000, reps=5):
     return out
 
 
+def run_ensemble(ndisc=64, steps=1000, loop_steps=20, seed=12345):
+    """Batched ensemble: ndisc seeded Kuzmin-Toomre discs (seeds 0..ndisc-1),
+    particle counts log-uniform in [2e4, 2e6], each on its own 64 x 128 2D
+    grid (log rings 0.05..5, m = 0..8, Plummer 0.1), dt = 0.025; one
+    persistent launch per step under a CUDA graph after the autotuner.
+    Against the plain per-run loop (one single-disc context per disc, the
+    same arithmetic), timed over loop_steps steps per disc."""
+    from galaxy_b200 import Galaxy, make_config, GX_RMAP_LOG
+    from galaxy_b200.disk import kt_disk
+    from galaxy_b200.ensemble import Ensemble
+    rng = np.random.default_rng(seed)
+    counts = np.round(np.exp(rng.uniform(np.log(2e4), np.log(2e6), ndisc))).astype(np.int64)
+
+    def cfg():
+        return make_config(2, 64, 128, ng=9, rmap=GX_RMAP_LOG, rmap_a=float(np.log(100.0) / 63),
+                           rmap_r0=0.05, softl=0.1, tsoft=1, pmass=1.0)
+    recs, pms = [], []
+    for d in range(ndisc):
+        r, pm = kt_disk(int(counts[d]), seed=d, rmax=4.8, ndim=2, dt=0.025)
+        recs.append(r.astype(np.float32))
+        pms.append(pm)
+    ntot = int(counts.sum())
+    ens = Ensemble(cfg(), recs, np.array(pms, np.float32), max_steps=loop_steps + 16 + steps)
+    threads, chunk = ens.tune()
+    ens.step(loop_steps)
+    p_ens = ens.unload()
+    ens.step(16)
+    ens.step(steps)
+    ms, launches = ens.last_ms()
+    conf = ens.config()
+    a2 = ens.a2()
+    ens.close()
+    # plain per-run loop
+    t_loop = 0.0
+    err = 0.0
+    for d in range(ndisc):
+        c = cfg()
+        c.pmass = float(pms[d])
+        with Galaxy(c) as gal:
+            gal.greenm()
+            gal.loadup(recs[d])
+            gal.masset()
+            gal.step(loop_steps)
+            t_loop += gal.last_step_ms()
+            pos = gal.unload()
+        ref = pos[:, :2].astype(np.float64)
+        err = max(err, float(np.abs(p_ens[d][:, :2] - ref).max() / np.abs(ref).max()))
+    rate = ntot * steps / (ms * 1e-3)
+    rate_loop = ntot * loop_steps / (t_loop * 1e-3)
+    return {"workload": f"ensemble2d-{ndisc}x64x128-{ntot}", "discs": ndisc, "particles": ntot,
+            "steps": steps, "ms_per_step": round(ms / steps, 4), "particle_steps_per_s": rate,
+            "launches_per_step": launches / steps, "cuda_graph": conf["graph"],
+            "tuned": {"threads": threads, "chunk": chunk, "ctas": conf["grid"]},
+            "per_run_loop": {"particle_steps_per_s": rate_loop, "steps": loop_steps,
+                             "ms_per_step_all_discs": round(t_loop / loop_steps, 4)},
+            "speedup_vs_per_run_loop": round(rate / rate_loop, 2),
+            "max_pos_rel_diff_vs_per_run_loop": err,
+            "a2_final_abs_mean": float(np.abs(a2[-1]).mean())}
+
+
 def cpu_rate(w, rec, pm, steps, budget_s, threads):
     """CPU restatement of one step (oracle, FP32 mirror) on the host cores:
     the field solve on the full grid, the particle loop on a sample, the
@@ -387,6 +447,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=30.0)
     ap.add_argument("--no-sfp", action="store_true")
+    ap.add_argument("--no-ens", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     w = WORKLOADS[args.workload]
@@ -428,6 +489,7 @@ def main():
     if rank == 0:
         e2e = run_e2e(args, w, rec, pm, cfg.device) if world == 1 else None
         sfp = run_sfp() if (world == 1 and not args.no_sfp) else None
+        ens = run_ensemble() if (world == 1 and not args.no_ens) else None
         cpu = None
         if world == 1 and not args.no_cpu:
             cpu = cpu_rate(w, rec, pm, 3, args.cpu_budget, os.cpu_count() or 1)
@@ -441,7 +503,8 @@ def main():
                 "fp64_path": out.get("fp64_path"),
                 "speedup_vs_fp64_path": out.get("speedup_vs_fp64_path"),
                 "force_rel_err": out.get("force_rel_err"),
-                "step_roofline": out["step_roofline"], "phases": out["phases"], "sfp": sfp}
+                "step_roofline": out["step_roofline"], "phases": out["phases"], "sfp": sfp,
+                "ensemble": ens}
         print(json.dumps(line))
     if comm is not None:
         comm.dist.destroy_process_group()
