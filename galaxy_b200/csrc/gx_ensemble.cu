@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(1024) k_ens_step(EnsArgs A) {
                         ay += f.y * w[k];
                     }
                 }
-                if (g.halo == 1) {
+                if (g.halo == 1 && cw.key >= 0) {
                     const float r2 = x * x + y * y;
                     const float rr = sqrtf(r2);
                     float fr = -g.halo_v2 * rr / (r2 + g.halo_rc2);

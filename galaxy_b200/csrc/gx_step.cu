@@ -27,7 +27,10 @@ __device__ __forceinline__ void gx_accel_cell(const DevGeo& g, const float4* __r
                                               const CellW& cw, float x, float y, float z, float& ax,
                                               float& ay, float& az, float& ph) {
     ax = ay = az = ph = 0.f;
-    if (cw.key >= 0) {
+    // particles off the grid feel no force (getacc.f:103-122 acts on the
+    // particles inside the grid)
+    if (cw.key < 0) return;
+    {
         float w[8];
         int ic[8];
         gx_weights(g, cw, w);

@@ -163,6 +163,7 @@ int64_t ox_direct_size(const GxConfig* c) {
 #define FMOD fmod
 #define POW pow
 #include "gx_oracle_tmpl.h"
+#include "gx_oracle_adj.h"
 #undef R
 #undef S
 #undef MIRROR

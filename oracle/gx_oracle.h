@@ -73,6 +73,14 @@ int ox_sfp_coeffs(const GxSfpBasis* b, int64_t n, const double* pos, int stride,
 int ox_sfp_acc(const GxSfpBasis* b, const double* coeff, int64_t n, const double* pos, int stride,
                double maxr, double* acc, double* pot);
 
+/* adjoint of the 2D step in FP64 (gx_oracle_adj.h): J = |A2(x_T)| over
+ * all particles; pos records (x, y, vx, vy); grad [n][4]; dtheta = dJ/d
+ * (halo_rc, halo_v2) */
+int ox_adj_forward(const GxConfig* cfg, const double* G, int64_t n, double* pos, int nsteps,
+                   double* a2, double* J);
+int ox_adj_gradient(const GxConfig* cfg, const double* G, int64_t n, const double* pos0,
+                    int nsteps, double* grad, double* dtheta, double* J);
+
 /* icheck-style integrals in FP64 from FP64 particle records and potentials */
 int ox_icheck(const GxConfig* cfg, int64_t n, const double* pos,
               const double* acc, const double* pot, double pmass_phys,

@@ -65,6 +65,8 @@ def _setup(L):
     L.ox_sfp_coeffs.argtypes = [C.POINTER(GxSfpBasis), i64, P, C.c_int, C.c_double, C.c_double, P]
     L.ox_sfp_acc.argtypes = [C.POINTER(GxSfpBasis), P, i64, P, C.c_int, C.c_double, P, P]
     L.ox_icheck.argtypes = [C.POINTER(GxConfig), i64, P, P, P, C.c_double, C.POINTER(GxDiag)]
+    L.ox_adj_forward.argtypes = [C.POINTER(GxConfig), P, i64, P, C.c_int, P, P]
+    L.ox_adj_gradient.argtypes = [C.POINTER(GxConfig), P, i64, P, C.c_int, P, P, P]
 
 
 def _p(a):
@@ -246,3 +248,29 @@ def sfp_acc(basis, coeff, pos, maxr):
     _chk(lib().ox_sfp_acc(C.byref(basis.c), _p(coeff), pos.shape[0], _p(pos), pos.shape[1],
                           float(maxr), _p(acc), _p(pot)), "sfp_acc")
     return acc, pot
+
+
+def adj_forward(cfg, G, pos, nsteps):
+    """J = |A2| after masset + nsteps FP64 steps of the records pos (n x 4,
+    2D), A2 = mean e^{2 i phi} over all particles (gx_oracle_adj.h)."""
+    L = lib()
+    q = np.ascontiguousarray(pos, np.float64).copy()
+    G = np.ascontiguousarray(G, np.float64)
+    a2 = np.zeros(2)
+    J = np.zeros(1)
+    _chk(L.ox_adj_forward(C.byref(cfg), _p(G), len(q), _p(q), int(nsteps), _p(a2), _p(J)),
+         "ox_adj_forward")
+    return float(J[0]), complex(a2[0], a2[1]), q
+
+
+def adj_gradient(cfg, G, pos, nsteps):
+    """(J, grad [n][4] = dJ/d(x, y, vx, vy), dJ/d(halo_rc, halo_v2)) in FP64"""
+    L = lib()
+    q = np.ascontiguousarray(pos, np.float64)
+    G = np.ascontiguousarray(G, np.float64)
+    grad = np.zeros((len(q), 4))
+    dth = np.zeros(2)
+    J = np.zeros(1)
+    _chk(L.ox_adj_gradient(C.byref(cfg), _p(G), len(q), _p(q), int(nsteps), _p(grad), _p(dth),
+                           _p(J)), "ox_adj_gradient")
+    return float(J[0]), grad, dth
