@@ -70,6 +70,7 @@ def lib():
         L.gx_host_free.argtypes = [P]
         L.gx_set_profile.argtypes = [P, C.c_int]
         L.gx_phase_ms.argtypes = [P, P, P]
+        L.gx_adjoint.argtypes = [P, C.c_int, C.c_int, P, P, P, P]
         _lib = L
     return _lib
 
@@ -224,6 +225,21 @@ class Galaxy:
 
     def step(self, nsteps=1, phys=False):
         self._chk(self._L.gx_step(self._h, nsteps, int(phys)))
+
+    def adjoint(self, nsteps, ckpt_every=50):
+        """Gradient of J = |A2(t_final)| after nsteps steps (2D, mixed path)
+        with respect to the loaded records and the halo parameters:
+        returns (J, grad [n, 4] = dJ/d(x, y, vx, vy) in load order,
+        dJ/d(halo_rc, halo_v2), reversal drift).  The context keeps its
+        initial particles."""
+        n = self.n
+        J = np.zeros(1, np.float64)
+        grad = np.zeros((n, 4), np.float32)
+        dth = np.zeros(2, np.float64)
+        drift = np.zeros(1, np.float32)
+        self._chk(self._L.gx_adjoint(self._h, int(nsteps), int(ckpt_every), _ptr(J), _ptr(grad),
+                                     _ptr(dth), _ptr(drift)))
+        return float(J[0]), grad, dth, float(drift[0])
 
     def tmcent(self, start=True):
         self._chk(self._L.gx_tmcent(self._h, int(start)))

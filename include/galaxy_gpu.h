@@ -289,6 +289,24 @@ int gx_sfp_acc(GxSfp* sfp, const double* coeff, float* acc, float* pot);
 /* Device ms and kernel launches of the last gx_sfp_sum. */
 int gx_sfp_last_ms(const GxSfp* sfp, float* ms, int64_t* launches);
 
+/* Adjoint of nsteps mixed-path steps (2D, one sector) of the loaded
+ * particles for the objective J = |A2(t_final)|, A2 = (1/n) sum_p
+ * e^{2 i phi_p} over all particles.  The forward sweep (the arithmetic of
+ * gx_step: massgn, findf + polcat, getacc with the ISOT halo, stpgrp) keeps
+ * a checkpoint every ckpt_every steps; the reverse sweep recomputes the
+ * trajectory backwards by time reversal (reset at each checkpoint) and
+ * applies the transposed step: interpolation slopes, halo Jacobian, and the
+ * transposed field solve (forward DFT, radial contraction with the same
+ * Green table, synthesis, polcat, all transposed).  Outputs: J, grad[n][4] =
+ * dJ/d(x, y, vx, vy) of the initial records in load order, dtheta[2] =
+ * dJ/d(halo_rc, halo_v2) in config units, drift (may be NULL) = largest
+ * |position difference| between the time-reversed trajectory and the
+ * checkpoints.  Afterwards the context holds the initial particles and
+ * their mass again.  No reference counterpart (the reference has no
+ * gradients); its forward arithmetic is step.f:135-290 / stpgrp.f:26-32. */
+int gx_adjoint(GxCtx* ctx, int nsteps, int ckpt_every, double* J, float* grad, double* dtheta,
+               float* drift);
+
 /* Ensemble of independent 2D discs sharing one grid geometry (one Green
  * table), advanced together: every step is one persistent cooperative
  * launch for all discs (field solve per disc, then push + deposit of every
