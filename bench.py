@@ -471,27 +471,6 @@ def cpu_rate(w, rec, pm, steps, budget_s, threads):
             "t_step_s": t_step, "steps_timed": len(times)}
 
 
-class Comm:
-    """Per-step mass-grid sum across ranks over NCCL (torch.distributed)."""
-
-    def __init__(self):
-        import torch
-        import torch.distributed as dist
-        self.torch, self.dist = torch, dist
-        self.rank, self.world = dist.get_rank(), dist.get_world_size()
-
-    def attach(self, gal):
-        gal.set_comm(self)
-
-    def barrier(self):
-        self.dist.barrier()
-
-    def max(self, v):
-        t = self.torch.tensor([float(v)], device="cuda")
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
-
-
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -540,7 +519,8 @@ def main():
         import datetime
         torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-        comm = Comm()
+        from galaxy_b200.dist import RankComm
+        comm = RankComm()
     out, rec, pm, cfg = run_ours(args, w, rank, world, comm)
     if comm is not None:
         comm.barrier()

@@ -181,9 +181,12 @@ class Galaxy:
         buf = C.create_string_buffer(128)
         if rank == 0:
             self._chk(self._L.gx_comm_unique_id(buf))
-        obj = [bytes(buf.raw)]
-        dist.broadcast_object_list(obj, src=0)
-        self._chk(self._L.gx_comm_init(self._h, obj[0], world, rank))
+        uid = comm.broadcast_bytes(buf.raw) if hasattr(comm, "broadcast_bytes") else None
+        if uid is None:
+            obj = [bytes(buf.raw)]
+            dist.broadcast_object_list(obj, src=0)
+            uid = obj[0]
+        self._chk(self._L.gx_comm_init(self._h, uid, world, rank))
 
     def unload(self):
         out = np.zeros((self.n, 2 * self.ndim), np.float32)
