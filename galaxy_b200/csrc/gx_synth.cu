@@ -87,8 +87,7 @@ __global__ void k_syntab(DevGeo g, ActList act, int nact, float scale, float* WA
 }
 
 // vertical synthesis, one CTA per (ring, field type); R[t][ir][z][ncp]
-#define SYNZ_KS 2
-#define SYNZ_THREADS 288
+#define SYNZ_THREADS 576
 __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int ncp, int tmask,
                                              const float4* __restrict__ O, SynTab tb,
                                              float* __restrict__ R) {
@@ -151,71 +150,66 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
         }
     }
     __syncthreads();
-    // 4x4 tiles of (z, column); the k sums split over SYNZ_KS adjacent lanes
+    // 4x4 tiles of (z, column); the four sums of a tile (even/odd kz x A/B
+    // part) go to four adjacent lanes, recombined by shuffles:
+    // lo = EA + OA + EB + OB, hi = EA - OA - EB + OB
     const int tilesN = ncp >> 2, tilesM = nz4 >> 2, nt = tilesM * tilesN;
-    const int per = blockDim.x / SYNZ_KS, ks = threadIdx.x % SYNZ_KS;
+    const int per = blockDim.x / 4, role = threadIdx.x & 3;
+    const float* Sp = (role == 0) ? Ae : (role == 1) ? Be : (role == 2) ? Ao : Bo;
+    const float* Wp = (role == 0) ? sWAe : (role == 1) ? sWBe : (role == 2) ? sWAo : sWBo;
+    const int KR = (role < 2) ? KE : KO;
+    const float hs = (role == 0 || role == 3) ? 1.f : -1.f;
     for (int t0 = 0; t0 < nt; t0 += per) {
-        const int tile = t0 + threadIdx.x / SYNZ_KS;
+        const int tile = t0 + threadIdx.x / 4;
         const bool act = tile < nt;
         const int tm = act ? tile / tilesN : 0, tn = act ? tile - tm * tilesN : 0;
         const int z0 = tm * 4, c0 = tn * 4;
-        float EA[4][4], EB[4][4], OA[4][4], OB[4][4];
+        float acc[4][4];
 #pragma unroll
         for (int r = 0; r < 4; r++)
 #pragma unroll
-            for (int q = 0; q < 4; q++) EA[r][q] = EB[r][q] = OA[r][q] = OB[r][q] = 0.f;
-        const int ke = act ? KE : 0, ko = act ? KO : 0;
-#pragma unroll 2
-        for (int i = ks; i < ke; i += SYNZ_KS) {
-            const float4 a4 = *reinterpret_cast<const float4*>(Ae + i * ncp + c0);
-            const float4 b4 = *reinterpret_cast<const float4*>(Be + i * ncp + c0);
+            for (int q = 0; q < 4; q++) acc[r][q] = 0.f;
+        const int kr = act ? KR : 0;
+#pragma unroll 4
+        for (int i = 0; i < kr; i++) {
+            const float4 v = *reinterpret_cast<const float4*>(Sp + i * ncp + c0);
 #pragma unroll
             for (int r = 0; r < 4; r++) {
-                const float wa = sWAe[(z0 + r) * KE + i], wb = sWBe[(z0 + r) * KE + i];
-                EA[r][0] += wa * a4.x; EA[r][1] += wa * a4.y; EA[r][2] += wa * a4.z; EA[r][3] += wa * a4.w;
-                EB[r][0] += wb * b4.x; EB[r][1] += wb * b4.y; EB[r][2] += wb * b4.z; EB[r][3] += wb * b4.w;
+                const float w = Wp[(z0 + r) * KR + i];
+                acc[r][0] += w * v.x; acc[r][1] += w * v.y; acc[r][2] += w * v.z; acc[r][3] += w * v.w;
             }
         }
-#pragma unroll 2
-        for (int i = ks; i < ko; i += SYNZ_KS) {
-            const float4 a4 = *reinterpret_cast<const float4*>(Ao + i * ncp + c0);
-            const float4 b4 = *reinterpret_cast<const float4*>(Bo + i * ncp + c0);
+        float lo[4][4], hi[4][4];
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const float wa = sWAo[(z0 + r) * KO + i], wb = sWBo[(z0 + r) * KO + i];
-                OA[r][0] += wa * a4.x; OA[r][1] += wa * a4.y; OA[r][2] += wa * a4.z; OA[r][3] += wa * a4.w;
-                OB[r][0] += wb * b4.x; OB[r][1] += wb * b4.y; OB[r][2] += wb * b4.z; OB[r][3] += wb * b4.w;
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                lo[r][q] = acc[r][q];
+                hi[r][q] = hs * acc[r][q];
             }
-        }
 #pragma unroll
-        for (int o = 1; o < SYNZ_KS; o <<= 1)
+        for (int o = 1; o < 4; o <<= 1)
 #pragma unroll
             for (int r = 0; r < 4; r++)
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
-                    EA[r][q] += __shfl_xor_sync(0xffffffffu, EA[r][q], o);
-                    EB[r][q] += __shfl_xor_sync(0xffffffffu, EB[r][q], o);
-                    OA[r][q] += __shfl_xor_sync(0xffffffffu, OA[r][q], o);
-                    OB[r][q] += __shfl_xor_sync(0xffffffffu, OB[r][q], o);
+                    lo[r][q] += __shfl_xor_sync(0xffffffffu, lo[r][q], o);
+                    hi[r][q] += __shfl_xor_sync(0xffffffffu, hi[r][q], o);
                 }
-        if (!act || ks != 0) continue;
+        if (!act || role > 1) continue;
+        // role 0 writes the planes z, role 1 the mirrored planes ngz - z
 #pragma unroll
         for (int r = 0; r < 4; r++) {
             const int z = z0 + r;
             if (z >= Z0) continue;
-            float4 lo, hi;
-            lo.x = EA[r][0] + OA[r][0] + EB[r][0] + OB[r][0];
-            lo.y = EA[r][1] + OA[r][1] + EB[r][1] + OB[r][1];
-            lo.z = EA[r][2] + OA[r][2] + EB[r][2] + OB[r][2];
-            lo.w = EA[r][3] + OA[r][3] + EB[r][3] + OB[r][3];
-            *reinterpret_cast<float4*>(Rt + (size_t)z * ncp + c0) = lo;
-            const int zm = ngz - z;
-            if (z >= 1 && zm != z && zm < ngz) {
-                hi.x = EA[r][0] - OA[r][0] - EB[r][0] + OB[r][0];
-                hi.y = EA[r][1] - OA[r][1] - EB[r][1] + OB[r][1];
-                hi.z = EA[r][2] - OA[r][2] - EB[r][2] + OB[r][2];
-                hi.w = EA[r][3] - OA[r][3] - EB[r][3] + OB[r][3];
-                *reinterpret_cast<float4*>(Rt + (size_t)zm * ncp + c0) = hi;
+            if (role == 0) {
+                *reinterpret_cast<float4*>(Rt + (size_t)z * ncp + c0) =
+                    make_float4(lo[r][0], lo[r][1], lo[r][2], lo[r][3]);
+            } else {
+                const int zm = ngz - z;
+                if (z >= 1 && zm != z && zm < ngz)
+                    *reinterpret_cast<float4*>(Rt + (size_t)zm * ncp + c0) =
+                        make_float4(hi[r][0], hi[r][1], hi[r][2], hi[r][3]);
             }
         }
     }
