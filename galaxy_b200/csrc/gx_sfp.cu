@@ -106,135 +106,163 @@ __device__ __forceinline__ void mma_tf32(float* d, const uint32_t* a, const uint
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
 }
 
-// Features of one particle for the lane's fragment slots: T_d for
-// d = q + 8 j (j < 2 MT) and g_n for n = q + 8 u (u < NT):
-// g_0 = 1, g_{2m-1} = p^e cos m phi, g_{2m} = p^e sin m phi, e = m mod 2.
-template <int MT, int NT>
-__device__ __forceinline__ void sfp_features(float x, float y, float inv_maxr, int q, int maxm,
-                                             float* T, float* G) {
-    const float px = x * inv_maxr, py = y * inv_maxr;
-    const float p2 = px * px + py * py;
-    const bool act = p2 <= 1.0f;
-    const float xc = 2.f * p2 - 1.f;
-    // T_0 .. T_8 by the three-term recurrence
-    float t[9];
-    t[0] = 1.f;
-    t[1] = xc;
-#pragma unroll
-    for (int i = 2; i <= 8; i++) t[i] = 2.f * xc * t[i - 1] - t[i - 2];
-    float tq = 0.f, tm = 0.f;  // T_q, T_{8-q}
-#pragma unroll
-    for (int i = 0; i <= 8; i++) {
-        if (i == q) tq = t[i];
-        if (i == 8 - q) tm = t[i];
-    }
-    // T_{d+8} = 2 T_8 T_d - T_{|d-8|}
-    float prev = tm, cur = tq;
-#pragma unroll
-    for (int j = 0; j < 2 * MT; j++) {
-        T[j] = act ? cur : 0.f;
-        float nx = 2.f * t[8] * cur - prev;
-        prev = cur;
-        cur = nx;
-    }
-    // e^{i m phi} by repeated multiplication
-    const float pr = sqrtf(p2);
-    const float cr = pr > 0.f ? px / pr : 1.f, ci = pr > 0.f ? py / pr : 0.f;
-    float zr = 1.f, zi = 0.f;
-#pragma unroll
-    for (int u = 0; u < NT; u++) G[u] = 0.f;
-    for (int m = 0; m <= maxm; m++) {
-        if (m > 0) {
-            float nr = zr * cr - zi * ci;
-            zi = zr * ci + zi * cr;
-            zr = nr;
-        }
-        const float f = (m & 1) ? pr : 1.f;
-#pragma unroll
-        for (int u = 0; u < NT; u++) {
-            const int n = q + 8 * u;
-            if (m == 0 && n == 0) G[u] = 1.f;
-            if (m > 0 && n == 2 * m - 1) G[u] = zr * f;
-            if (m > 0 && n == 2 * m) G[u] = zi * f;
-        }
-    }
-    if (!act)
-#pragma unroll
-        for (int u = 0; u < NT; u++) G[u] = 0.f;
-}
-
-// moments of one SFP_CHUNK of particles per warp; part[warp][d][c]
-template <int MT, int NT>
+// Moments of one SFP_CHUNK of particles per warp; part[warp][d][c].
+// Rounds of 32 particles: lane l computes the features of particle l once --
+// T_d(x) for d < D by the three-term recurrence, and g_n (n >= 1) =
+// p^e cos m phi, p^e sin m phi (e = m mod 2) from repeated multiplication of
+// (x, y) / r -- into the warp's shared-memory tiles Ts[32][D + 8] and
+// Gs[32][GSTR] (padded so that the fragment loads below hit 32 distinct
+// banks).  Column c = 0 (g_0 = 1) is the plain sum of T_d, taken on the CUDA
+// cores (lane d); columns 1 .. NB*8 come from mma.sync m16n8k8 TF32 with the
+// operands split hi/lo (3 products), FP32 accumulation over the chunk.
+#define SFP_GSTR 24  // >= 8 NB, and 24 p mod 32 spreads c4 over banks
+template <int MT, int NB>
 __global__ void __launch_bounds__(256) k_sfp_moments(const float* __restrict__ X,
                                                      const float* __restrict__ Y, int64_t n,
-                                                     float inv_maxr, int maxm,
+                                                     float inv_maxr, int maxm, int NCP,
                                                      float* __restrict__ part) {
-    const int lane = threadIdx.x & 31;
+    constexpr int D = MT * 16, TSTR = D + 8;
+    extern __shared__ __align__(16) float sfs[];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    float* Ts = sfs + (size_t)wib * 32 * (TSTR + SFP_GSTR);
+    float* Gs = Ts + 32 * TSTR;
     const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t base = wid * SFP_CHUNK;
     if (base >= n) return;
     const int q = lane >> 2, c4 = lane & 3;
-    float acc[MT][NT][4];
+    float acc[MT][NB][4];
 #pragma unroll
     for (int a = 0; a < MT; a++)
 #pragma unroll
-        for (int u = 0; u < NT; u++)
+        for (int u = 0; u < NB; u++)
 #pragma unroll
             for (int i = 0; i < 4; i++) acc[a][u][i] = 0.f;
+    float col0[MT / 2 > 0 ? MT / 2 : 1];  // lane d (+32): sum of T_d
+#pragma unroll
+    for (int h = 0; h < (MT / 2 > 0 ? MT / 2 : 1); h++) col0[h] = 0.f;
     const int64_t end = min(base + (int64_t)SFP_CHUNK, n);
-    for (int64_t k0 = base; k0 < end; k0 += 8) {
-        float T[2][2 * MT], G[2][NT];
-#pragma unroll
-        for (int e = 0; e < 2; e++) {
-            const int64_t i = k0 + c4 + 4 * e;
-            float x = 2.f / inv_maxr, y = 0.f;  // outside the basis edge: no contribution
+    for (int64_t r0 = base; r0 < end; r0 += 32) {
+        // ---- features of particle r0 + lane
+        {
+            const int64_t i = r0 + lane;
+            float px = 2.f, py = 0.f;  // outside the basis edge: no contribution
             if (i < end) {
-                x = __ldg(X + i);
-                y = __ldg(Y + i);
+                px = __ldg(X + i) * inv_maxr;
+                py = __ldg(Y + i) * inv_maxr;
             }
-            sfp_features<MT, NT>(x, y, inv_maxr, q, maxm, T[e], G[e]);
+            const float p2 = px * px + py * py;
+            const bool act = p2 <= 1.0f;
+            const float xc = 2.f * p2 - 1.f;
+            float* tr = Ts + lane * TSTR;
+            float tm2 = 1.f, tm1 = xc;
+            float4 v;
+#pragma unroll
+            for (int d = 0; d < D; d += 4) {
+                float t4[4];
+#pragma unroll
+                for (int k = 0; k < 4; k++) {
+                    const int dd = d + k;
+                    float t;
+                    if (dd == 0) t = 1.f;
+                    else if (dd == 1) t = xc;
+                    else {
+                        t = 2.f * xc * tm1 - tm2;
+                        tm2 = tm1;
+                        tm1 = t;
+                    }
+                    t4[k] = act ? t : 0.f;
+                }
+                v = make_float4(t4[0], t4[1], t4[2], t4[3]);
+                *reinterpret_cast<float4*>(tr + d) = v;
+            }
+            const float pr = sqrtf(p2);
+            const float cr = pr > 0.f ? px / pr : 1.f, ci = pr > 0.f ? py / pr : 0.f;
+            float* gr = Gs + lane * SFP_GSTR;
+            float zr = 1.f, zi = 0.f;
+#pragma unroll
+            for (int u = 0; u < NB * 8; u += 2) {
+                const int m = u / 2 + 1;
+                float gc = 0.f, gs = 0.f;
+                if (m <= maxm) {
+                    const float nr = zr * cr - zi * ci;
+                    zi = zr * ci + zi * cr;
+                    zr = nr;
+                    const float f = (m & 1) ? pr : 1.f;
+                    gc = act ? zr * f : 0.f;
+                    gs = act ? zi * f : 0.f;
+                }
+                gr[u] = gc;
+                gr[u + 1] = gs;
+            }
         }
-        // split operands: hi = tf32(v), lo = tf32(v - hi)
-        uint32_t bh[NT][2], bl[NT][2];
+        __syncwarp();
+        // ---- column 0 on the CUDA cores
+#pragma unroll 8
+        for (int pp = 0; pp < 32; pp++) {
 #pragma unroll
-        for (int u = 0; u < NT; u++)
+            for (int h = 0; h < (MT / 2 > 0 ? MT / 2 : 1); h++) col0[h] += Ts[pp * TSTR + lane + 32 * h];
+        }
+        // ---- columns 1 .. 8 NB on the tensor cores, 4 k-blocks of 8 particles
 #pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const float v = G[e][u];
-                bh[u][e] = f2tf32(v);
-                bl[u][e] = f2tf32(v - __uint_as_float(bh[u][e]));
+        for (int kb = 0; kb < 4; kb++) {
+            const float* t0 = Ts + (8 * kb + c4) * TSTR;
+            const float* t1 = t0 + 4 * TSTR;
+            const float* g0 = Gs + (8 * kb + c4) * SFP_GSTR;
+            const float* g1 = g0 + 4 * SFP_GSTR;
+            uint32_t bh[NB][2], bl[NB][2];
+#pragma unroll
+            for (int u = 0; u < NB; u++) {
+                const float v0 = g0[8 * u + q], v1 = g1[8 * u + q];
+                bh[u][0] = f2tf32(v0);
+                bl[u][0] = f2tf32(v0 - __uint_as_float(bh[u][0]));
+                bh[u][1] = f2tf32(v1);
+                bl[u][1] = f2tf32(v1 - __uint_as_float(bh[u][1]));
             }
 #pragma unroll
-        for (int a = 0; a < MT; a++) {
-            // a0 = A[q][c4], a1 = A[q+8][c4], a2 = A[q][c4+4], a3 = A[q+8][c4+4]
-            const float v[4] = {T[0][2 * a], T[0][2 * a + 1], T[1][2 * a], T[1][2 * a + 1]};
-            uint32_t ah[4], al[4];
+            for (int a = 0; a < MT; a++) {
+                // a0 = A[q][c4], a1 = A[q+8][c4], a2 = A[q][c4+4], a3 = A[q+8][c4+4]
+                const float v[4] = {t0[16 * a + q], t0[16 * a + q + 8], t1[16 * a + q], t1[16 * a + q + 8]};
+                uint32_t ah[4], al[4];
 #pragma unroll
-            for (int i = 0; i < 4; i++) {
-                ah[i] = f2tf32(v[i]);
-                al[i] = f2tf32(v[i] - __uint_as_float(ah[i]));
-            }
+                for (int i = 0; i < 4; i++) {
+                    ah[i] = f2tf32(v[i]);
+                    al[i] = f2tf32(v[i] - __uint_as_float(ah[i]));
+                }
 #pragma unroll
-            for (int u = 0; u < NT; u++) {
-                mma_tf32(acc[a][u], al, bh[u]);
-                mma_tf32(acc[a][u], ah, bl[u]);
-                mma_tf32(acc[a][u], ah, bh[u]);
+                for (int u = 0; u < NB; u++) {
+                    mma_tf32(acc[a][u], al, bh[u]);
+                    mma_tf32(acc[a][u], ah, bl[u]);
+                    mma_tf32(acc[a][u], ah, bh[u]);
+                }
             }
         }
+        __syncwarp();
     }
-    // c0 = D[q][2c4], c1 = D[q][2c4+1], c2 = D[q+8][2c4], c3 = D[q+8][2c4+1]
-    const int NCP = NT * 8;
-    float* dst = part + wid * (size_t)(MT * 16) * NCP;
+    // c0 = D[q][2c4], c1 = D[q][2c4+1], c2 = D[q+8][2c4], c3 = D[q+8][2c4+1]; column
+    // n of the product is feature column n + 1
+    float* dst = part + wid * (size_t)D * NCP;
 #pragma unroll
     for (int a = 0; a < MT; a++)
 #pragma unroll
-        for (int u = 0; u < NT; u++) {
-            const int r0 = a * 16 + q, c0 = u * 8 + 2 * c4;
-            dst[r0 * NCP + c0] = acc[a][u][0];
-            dst[r0 * NCP + c0 + 1] = acc[a][u][1];
-            dst[(r0 + 8) * NCP + c0] = acc[a][u][2];
-            dst[(r0 + 8) * NCP + c0 + 1] = acc[a][u][3];
+        for (int u = 0; u < NB; u++) {
+            const int r0 = a * 16 + q, cc = u * 8 + 2 * c4 + 1;
+            if (cc < NCP) {
+                dst[r0 * NCP + cc] = acc[a][u][0];
+                dst[(r0 + 8) * NCP + cc] = acc[a][u][2];
+            }
+            if (cc + 1 < NCP) {
+                dst[r0 * NCP + cc + 1] = acc[a][u][1];
+                dst[(r0 + 8) * NCP + cc + 1] = acc[a][u][3];
+            }
         }
+#pragma unroll
+    for (int h = 0; h < (MT / 2 > 0 ? MT / 2 : 1); h++)
+        if (lane + 32 * h < D) dst[(lane + 32 * h) * NCP] = col0[h];
+    // columns past the products
+    for (int i = lane; i < D * (NCP - 1 - 8 * NB); i += 32) {
+        const int d = i / (NCP - 1 - 8 * NB), c = 1 + 8 * NB + (i - d * (NCP - 1 - 8 * NB));
+        dst[d * NCP + c] = 0.f;
+    }
 }
 
 // FP64 sum of the per-warp partials: one block per moment, each thread a
@@ -476,16 +504,14 @@ static int sfp_moments(GxSfp* s, int precision) {
     const int64_t nw = (n + SFP_CHUNK - 1) / SFP_CHUNK;
     const unsigned grid = (unsigned)((nw * 32 + 255) / 256);
     const float inv = (float)(1.0 / s->maxr);
-    const int NT = NCP / 8;
-    if (D == 32) {
-        if (NT == 1) k_sfp_moments<2, 1><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
-        else if (NT == 2) k_sfp_moments<2, 2><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
-        else k_sfp_moments<2, 3><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
-    } else {
-        if (NT == 1) k_sfp_moments<4, 1><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
-        else if (NT == 2) k_sfp_moments<4, 2><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
-        else k_sfp_moments<4, 3><<<grid, 256, 0, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->part);
-    }
+    // feature columns 1 .. NC - 1 in blocks of 8
+    const int NB = (s->NC - 1 + 7) / 8;
+    if (NB > 3) return s->err = "more than 11 harmonics on the tensor-core path", GX_ERR_RANGE;
+    const size_t sm = sizeof(float) * 8 * 32 * ((size_t)(D + 8) + SFP_GSTR);
+    auto k = (D == 32) ? ((NB <= 1) ? k_sfp_moments<2, 1> : (NB == 2) ? k_sfp_moments<2, 2> : k_sfp_moments<2, 3>)
+                       : ((NB <= 1) ? k_sfp_moments<4, 1> : (NB == 2) ? k_sfp_moments<4, 2> : k_sfp_moments<4, 3>);
+    SFP_CUDA(s, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k<<<grid, 256, sm, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, NCP, s->part);
     SFP_CUDA(s, cudaGetLastError());
     k_sfp_reduce<float><<<nmom, 256, 0, s->stream>>>(s->part, nw, nmom, s->mom);
     SFP_CUDA(s, cudaGetLastError());
