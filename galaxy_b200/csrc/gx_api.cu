@@ -168,6 +168,7 @@ static int alloc_grids(GxCtx* c) {
         DALLOC(c, c->rowfill, (size_t)NCOPY * (g.nrow + 1));
         DALLOC(c, c->rowbase, (size_t)NCOPY * (g.nrow + 1));
         DALLOC(c, c->rowtot, (size_t)g.nrow + 1);
+        DALLOC(c, c->rowtile, (size_t)4 * ((g.nrow + 1 + ROW_TILE - 1) / ROW_TILE));
         DALLOC(c, c->nitems_d, 4);
         GX_CUDA(c, cudaMemsetAsync(c->rowcnt, 0, sizeof(uint32_t) * NCOPY * (g.nrow + 1), c->stream));
     }
@@ -227,7 +228,7 @@ void gx_destroy(GxCtx* c) {
                     c->origin_tmp, c->pkey[0], c->pkey[1], c->pfr[0], c->pfr[1], c->p64, c->key64, c->w64, c->acc64, c->ppot,
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
                     c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->perm_next, c->rowstart,
-                    c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->stage, c->jrk_d,
+                    c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->rowtile, c->stage, c->jrk_d,
                     c->errword, c->dsum};
     for (void* p : ptrs)
         if (p) cudaFree(p);

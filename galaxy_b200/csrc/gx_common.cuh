@@ -108,6 +108,7 @@ struct GxCtx {
     uint32_t* rowfill = nullptr;           // [NCOPY][nrow + 1] slots handed out per row
     uint32_t* rowbase = nullptr;           // [NCOPY][nrow + 1] offset of each copy in its row
     uint32_t* rowtot = nullptr;            // [nrow + 1] particles per row
+    int32_t* rowtile = nullptr;            // [tiles of ROW_TILE rows][4]: particles, items, first and last occupied row
     int maxitems = 0;
     int32_t* jrk_d = nullptr;              // device min/max ring
     int32_t* errword = nullptr;            // device error word
@@ -293,6 +294,8 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
 }
+
+#define ROW_TILE 256  // rows per block of the row reduce / scan
 
 // warp-aggregated count of row (all 32 lanes must call)
 __device__ __forceinline__ void gx_row_count(uint32_t row, bool act, uint32_t* __restrict__ cnt) {

@@ -27,103 +27,140 @@
 
 #define FIXQ 1048576.0f  // 2^20
 
-// per row: total over the counter copies, each copy's offset in the row;
-// clears the counters for the next pass
-__global__ void k_row_reduce(int nrow, uint32_t* __restrict__ rowcnt, uint32_t* __restrict__ rowfill,
-                             uint32_t* __restrict__ rowbase, uint32_t* __restrict__ rowtot) {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r > nrow) return;
-    const size_t st = (size_t)nrow + 1;
-    uint32_t run = 0;
-#pragma unroll 8
-    for (int c = 0; c < NCOPY; c++) {
-        const uint32_t v = rowcnt[c * st + r];
-        rowbase[c * st + r] = run;
-        run += v;
-        rowcnt[c * st + r] = 0;
-        rowfill[c * st + r] = 0;
+// block-wide sums / extremes of one value per thread (ROW_TILE threads)
+__device__ __forceinline__ void tile_reduce(int& a, int& b, int& lo, int& hi, int* sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        a += __shfl_xor_sync(0xffffffffu, a, o);
+        b += __shfl_xor_sync(0xffffffffu, b, o);
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
     }
-    rowtot[r] = run;
-}
-
-// row totals -> row starts, deposit work items, active ring range.  One CTA.
-__global__ void k_row_scan(int nrow, int ngz, int nr, const uint32_t* __restrict__ rowcnt,
-                           int32_t* __restrict__ rowstart,
-                           int32_t* __restrict__ rowitem, int32_t* __restrict__ items,
-                           int32_t* __restrict__ nitems, int32_t* __restrict__ jrk) {
-    __shared__ int32_t ws_a[32], ws_b[32];
-    __shared__ int32_t carry_a, carry_b, rmin, rmax;
-    if (threadIdx.x == 0) {
-        carry_a = carry_b = 0;
-        rmin = 0x7fffffff;
-        rmax = -1;
+    if (lane == 0) {
+        sh[4 * warp] = a;
+        sh[4 * warp + 1] = b;
+        sh[4 * warp + 2] = lo;
+        sh[4 * warp + 3] = hi;
     }
     __syncthreads();
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    // rows 0 .. nrow (row nrow collects particles off the grid)
-    for (int base = 0; base <= nrow; base += blockDim.x) {
-        const int r = base + threadIdx.x;
-        const int cnt = (r <= nrow) ? (int)rowcnt[r] : 0;
-        const int nit = (r < nrow) ? (cnt + DEP_CH - 1) / DEP_CH : 0;
-        if (r < nrow && cnt > 0) {
-            atomicMin(&rmin, r);
-            atomicMax(&rmax, r);
-        }
-        int xa = cnt, xb = nit;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            int ya = __shfl_up_sync(0xffffffffu, xa, o);
-            int yb = __shfl_up_sync(0xffffffffu, xb, o);
-            if (lane >= o) {
-                xa += ya;
-                xb += yb;
-            }
-        }
-        if (lane == 31) {
-            ws_a[warp] = xa;
-            ws_b[warp] = xb;
-        }
-        __syncthreads();
-        if (warp == 0) {
-            int sa = (lane < nw) ? ws_a[lane] : 0, sb = (lane < nw) ? ws_b[lane] : 0;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                int ya = __shfl_up_sync(0xffffffffu, sa, o);
-                int yb = __shfl_up_sync(0xffffffffu, sb, o);
-                if (lane >= o) {
-                    sa += ya;
-                    sb += yb;
-                }
-            }
-            if (lane < nw) {
-                ws_a[lane] = sa;
-                ws_b[lane] = sb;
-            }
-        }
-        __syncthreads();
-        const int ea = carry_a + ((warp > 0) ? ws_a[warp - 1] : 0) + xa - cnt;
-        const int eb = carry_b + ((warp > 0) ? ws_b[warp - 1] : 0) + xb - nit;
-        if (r <= nrow) rowstart[r] = ea;
-        if (r < nrow) {
-            rowitem[r] = eb;
-            for (int q = 0; q < nit; q++) {
-                int it = eb + q;
-                items[3 * it + 0] = r;
-                items[3 * it + 1] = ea + q * DEP_CH;
-                items[3 * it + 2] = min(ea + (q + 1) * DEP_CH, ea + cnt);
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            carry_a += ws_a[nw - 1];
-            carry_b += ws_b[nw - 1];
-        }
-        __syncthreads();
-    }
     if (threadIdx.x == 0) {
-        rowstart[nrow + 1] = carry_a;
-        rowitem[nrow] = carry_b;
-        *nitems = carry_b;
+        for (int w = 1; w < nw; w++) {
+            a += sh[4 * w];
+            b += sh[4 * w + 1];
+            lo = min(lo, sh[4 * w + 2]);
+            hi = max(hi, sh[4 * w + 3]);
+        }
+    }
+}
+
+// per row: total over the counter copies, each copy's offset in the row;
+// clears the counters for the next pass.  Per tile of ROW_TILE rows: the
+// particles, the deposit work items and the occupied row range.
+__global__ void __launch_bounds__(ROW_TILE) k_row_reduce(int nrow, uint32_t* __restrict__ rowcnt,
+                                                         uint32_t* __restrict__ rowfill,
+                                                         uint32_t* __restrict__ rowbase,
+                                                         uint32_t* __restrict__ rowtot,
+                                                         int32_t* __restrict__ tile) {
+    __shared__ int sh[4 * (ROW_TILE / 32)];
+    const int r = blockIdx.x * ROW_TILE + threadIdx.x;
+    const size_t st = (size_t)nrow + 1;
+    uint32_t run = 0;
+    if (r <= nrow) {
+#pragma unroll 8
+        for (int c = 0; c < NCOPY; c++) {
+            const uint32_t v = rowcnt[c * st + r];
+            rowbase[c * st + r] = run;
+            run += v;
+            rowcnt[c * st + r] = 0;
+            rowfill[c * st + r] = 0;
+        }
+        rowtot[r] = run;
+    }
+    int a = (int)run, b = (r < nrow) ? (int)((run + DEP_CH - 1) / DEP_CH) : 0;
+    int lo = (r < nrow && run > 0) ? r : 0x7fffffff, hi = (r < nrow && run > 0) ? r : -1;
+    tile_reduce(a, b, lo, hi, sh);
+    if (threadIdx.x == 0) {
+        tile[4 * blockIdx.x] = a;
+        tile[4 * blockIdx.x + 1] = b;
+        tile[4 * blockIdx.x + 2] = lo;
+        tile[4 * blockIdx.x + 3] = hi;
+    }
+}
+
+// row totals -> row starts, deposit work items, active ring range; one
+// block per tile of ROW_TILE rows, the carry-in from the tile sums
+__global__ void __launch_bounds__(ROW_TILE) k_row_scan(int nrow, int ngz, int nr,
+                                                       const uint32_t* __restrict__ rowcnt,
+                                                       const int32_t* __restrict__ tile,
+                                                       int32_t* __restrict__ rowstart,
+                                                       int32_t* __restrict__ rowitem,
+                                                       int32_t* __restrict__ items,
+                                                       int32_t* __restrict__ nitems,
+                                                       int32_t* __restrict__ jrk) {
+    __shared__ int ws_a[ROW_TILE / 32], ws_b[ROW_TILE / 32];
+    __shared__ int carry_a, carry_b;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int b = blockIdx.x;
+    if (warp == 0) {
+        int ca = 0, cb = 0;
+        for (int t = lane; t < b; t += 32) {
+            ca += tile[4 * t];
+            cb += tile[4 * t + 1];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ca += __shfl_xor_sync(0xffffffffu, ca, o);
+            cb += __shfl_xor_sync(0xffffffffu, cb, o);
+        }
+        if (lane == 0) {
+            carry_a = ca;
+            carry_b = cb;
+        }
+    }
+    const int r = b * ROW_TILE + threadIdx.x;
+    const int cnt = (r <= nrow) ? (int)rowcnt[r] : 0;
+    const int nit = (r < nrow) ? (cnt + DEP_CH - 1) / DEP_CH : 0;
+    int xa = cnt, xb = nit;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int ya = __shfl_up_sync(0xffffffffu, xa, o), yb = __shfl_up_sync(0xffffffffu, xb, o);
+        if (lane >= o) {
+            xa += ya;
+            xb += yb;
+        }
+    }
+    if (lane == 31) {
+        ws_a[warp] = xa;
+        ws_b[warp] = xb;
+    }
+    __syncthreads();
+    int pa = carry_a, pb = carry_b;
+    for (int w = 0; w < warp; w++) {
+        pa += ws_a[w];
+        pb += ws_b[w];
+    }
+    const int ea = pa + xa - cnt, eb = pb + xb - nit;
+    if (r <= nrow) rowstart[r] = ea;
+    if (r <= nrow) rowitem[r] = eb;
+    if (r < nrow) {
+        for (int q = 0; q < nit; q++) {
+            const int it = eb + q;
+            items[3 * it + 0] = r;
+            items[3 * it + 1] = ea + q * DEP_CH;
+            items[3 * it + 2] = min(ea + (q + 1) * DEP_CH, ea + cnt);
+        }
+    }
+    if (r == nrow) {
+        // the off-grid row closes the arrays: totals and the active ring range
+        rowstart[nrow + 1] = ea + cnt;
+        *nitems = eb;
+        const int ntile = nrow / ROW_TILE + 1;
+        int rmin = 0x7fffffff, rmax = -1;
+        for (int t = 0; t < ntile; t++) {
+            rmin = min(rmin, tile[4 * t + 2]);
+            rmax = max(rmax, tile[4 * t + 3]);
+        }
         // 1-based ring range as massgn tracks it (jrad = j + 1, krad = j + 2)
         if (rmax >= 0) {
             jrk[0] = rmin / ngz + 1;
@@ -133,6 +170,7 @@ __global__ void k_row_scan(int nrow, int ngz, int nr, const uint32_t* __restrict
             jrk[1] = 0;
         }
     }
+    (void)nw;
 }
 
 // slot of every particle in the row-ordered permutation: perm[slot] = t
@@ -248,11 +286,12 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
     const int64_t n = c->n;
     int rc = gx_phase_mark(c, PH_SORT);
     if (rc) return rc;
-    k_row_reduce<<<(g.nrow + 1 + 255) / 256, 256, 0, c->stream>>>(g.nrow, c->rowcnt, c->rowfill,
-                                                                  c->rowbase, c->rowtot);
+    const int ntile = (g.nrow + 1 + ROW_TILE - 1) / ROW_TILE;
+    k_row_reduce<<<ntile, ROW_TILE, 0, c->stream>>>(g.nrow, c->rowcnt, c->rowfill, c->rowbase, c->rowtot,
+                                                     c->rowtile);
     GX_LAUNCHED(c);
-    k_row_scan<<<1, 1024, 0, c->stream>>>(g.nrow, g.ngz, g.nr, c->rowtot, c->rowstart, c->rowitem,
-                                          c->items, c->nitems_d, c->jrk_d);
+    k_row_scan<<<ntile, ROW_TILE, 0, c->stream>>>(g.nrow, g.ngz, g.nr, c->rowtot, c->rowtile, c->rowstart,
+                                                   c->rowitem, c->items, c->nitems_d, c->jrk_d);
     GX_LAUNCHED(c);
     if (n > 0) {
         k_place<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(keys, n, g.nrow, g.na, c->rowstart,
