@@ -7,7 +7,7 @@
 // mixing of the type.  Each Green entry is used for 4 MACs and read once per
 // step, so the kernel's job is to keep the HBM pipe full.
 //
-// Persistent CTAs of 16 consumer warps and 1 producer warp.  Work items are
+// Persistent CTAs of 8 consumer warps and 1 producer warp.  Work items are
 // (m, kz) pairs dealt round-robin to CTAs.  The producer walks the same tile
 // sequence as the consumers -- items, then valid types, then chunks of rows
 // (source rings js..ks) of the nr x nr matrix -- and copies each tile, a
@@ -23,7 +23,6 @@
 #include "gx_common.cuh"
 
 namespace {
-constexpr int NCW = 16;                       // consumer warps
 constexpr int MAXST = 8;                      // most stages in the ring
 constexpr uint32_t SPIN_LIMIT = 1u << 22;     // try_wait polls before giving up
 
@@ -63,6 +62,7 @@ __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t by
         "l"(src), "r"(bytes), "r"(su32(b))
         : "memory");
 }
+template <int NCW>
 __device__ __forceinline__ void consumer_sync() {
     asm volatile("bar.sync 1, %0;" ::"n"(NCW * 32) : "memory");
 }
@@ -87,8 +87,8 @@ __device__ __forceinline__ bool type_valid(const DevGeo& g, int t, int m, int k)
 }  // namespace
 
 // NJ = ceil(nr / 128): groups of 128 output rings per lane (4 per lane each)
-template <int NJ>
-__global__ void __launch_bounds__((NCW + 1) * 32, 1) k_conv_bulk(ConvArgs A) {
+template <int NJ, int NCW, int MINB>
+__global__ void __launch_bounds__((NCW + 1) * 32, MINB) k_conv_bulk(ConvArgs A) {
     extern __shared__ __align__(128) unsigned char smraw[];
     const DevGeo& g = A.g;
     const int nr = g.nr, nkz = g.nkz;
@@ -230,7 +230,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) k_conv_bulk(ConvArgs A) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) part[warp * nr + ir0 + q] = acc[j][q];
             }
-            consumer_sync();
+            consumer_sync<NCW>();
             for (int i = threadIdx.x; i < nr; i += NCW * 32) {
                 float4 v = part[i];
 #pragma unroll
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 1) k_conv_bulk(ConvArgs A) {
                 }
                 out[i] = v;
             }
-            consumer_sync();
+            consumer_sync<NCW>();
         }
         __syncwarp();
         if (lane == 0 && !dead) mbar_arrive(&sempty[li & 1]);
@@ -255,11 +255,14 @@ int gx_conv_bulk(GxCtx* c, int nact, int tmask) {
     int dev_sms = 0, smem_max = 0;
     GX_CUDA(c, cudaDeviceGetAttribute(&dev_sms, cudaDevAttrMultiProcessorCount, c->dev));
     GX_CUDA(c, cudaDeviceGetAttribute(&smem_max, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dev));
-    const size_t fixed = sizeof(float4) * (size_t)g.nr * (NCW + 2) + (2 * MAXST + 4) * sizeof(uint64_t);
-    // rows per tile: the whole matrix or 32 KB of it; as many stages as fit in 160 KB
-    const int R = std::min(g.nr, (int)(32768 / (g.nr * sizeof(float))));
+    // 8 consumer warps; tiles of whole 64 KB matrices (or 64 KB of rows): a
+    // sweep on B200 found the contraction's rate set by the size of each bulk
+    // copy (16 KB: 2.9 TB/s, 32 KB: 3.5, 64 KB: 3.95), not by the stage count
+    constexpr int ncw = 8;
+    const size_t fixed = sizeof(float4) * (size_t)g.nr * (ncw + 2) + (2 * MAXST + 4) * sizeof(uint64_t);
+    const int R = std::min(g.nr, (int)(65536 / (g.nr * sizeof(float))));
     const size_t stage_bytes = (size_t)R * g.nr * sizeof(float);
-    const size_t budget = std::min<size_t>((size_t)smem_max - fixed, 163840);
+    const size_t budget = std::min<size_t>((size_t)smem_max - fixed, 204800);
     int nst = (int)std::min<size_t>(MAXST, budget / stage_bytes);
     if (nst < 2) return c->err = "radial contraction: shared memory too small", GX_ERR_ARG;
     const size_t smem = nst * stage_bytes + fixed;
@@ -277,8 +280,8 @@ int gx_conv_bulk(GxCtx* c, int nact, int tmask) {
     A.errword = c->errword;
     for (int i = 0; i < 260; i++) A.act_m[i] = (i < nact) ? c->spec.m[i] : 0;
     const int grid = std::min(A.nitems, dev_sms);
-    GX_CUDA(c, cudaFuncSetAttribute(k_conv_bulk<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_conv_bulk<1><<<grid, (NCW + 1) * 32, smem, c->stream>>>(A);
+    GX_CUDA(c, cudaFuncSetAttribute(k_conv_bulk<1, ncw, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_conv_bulk<1, ncw, 1><<<grid, (ncw + 1) * 32, smem, c->stream>>>(A);
     GX_LAUNCHED(c);
     return GX_OK;
 }
