@@ -49,7 +49,8 @@ int setgrd(const GxConfig* c, GxGeometry* g, std::string& err) {
     g->ng = std::min(std::max(c->ng, 1), g->mmax);
     g->nsect = c->nsect;
     int64_t mesh = (int64_t)c->nr * na * ngz;
-    if (mesh >= (int64_t)1 << 30) return err = "mesh too large", GX_ERR_RANGE;
+    // cell keys are divided by na in single precision (gx_div_na): below 2^24
+    if (mesh >= (int64_t)1 << 24) return err = "mesh too large (2^24 cells at most)", GX_ERR_RANGE;
     g->mesh = (int)mesh;
     g->alpha = (float)(2.0 * GX_PI / (double)(float)na);
     g->ua = (c->rmap_a > 0.f) ? c->rmap_a : g->alpha;
@@ -105,6 +106,7 @@ void fill_devgeo(GxCtx* c) {
     d.dzg = c->cfg.dzg;
     d.inv_dzg = (d.ndim == 3) ? 1.0f / c->cfg.dzg : 0.f;
     d.t_scale = (float)((double)G.na / (2.0 * GX_PI));
+    d.inv_na = 1.0f / (float)G.na;
     d.halo_v2 = c->cfg.halo_v2;
     d.halo_rc2 = c->cfg.halo_rc * c->cfg.halo_rc;
     d.pmass = c->cfg.pmass;

@@ -29,6 +29,7 @@ struct DevGeo {
     int rmap, tsoft, halo;
     float alpha, ua, inv_ua, uoffs, rinh, rgrid, zm, thmax, dzg, inv_dzg;
     float t_scale;  // na / (2 pi) in FP32
+    float inv_na;   // 1 / na (fast division of cell keys, gx_div_na)
     float halo_v2, halo_rc2;
     float pmass;
     // FP64 copies for the plain FP64 path
@@ -264,10 +265,28 @@ __device__ __forceinline__ void gx_weights(const DevGeo& g, const CellW& c, floa
     }
 }
 
+// q = v / na and r = v % na for 0 <= v < 2^24 (every cell key: the mesh is
+// checked against 2^24 at set-up): the float reciprocal is off by at most
+// one, fixed by one correction
+__device__ __forceinline__ int gx_div_na(const DevGeo& g, int v, int& r) {
+    int q = __float2int_rz((float)v * g.inv_na);
+    r = v - q * g.na;
+    if (r < 0) {
+        q--;
+        r += g.na;
+    } else if (r >= g.na) {
+        q++;
+        r -= g.na;
+    }
+    return q;
+}
+
 // corner cells of a key (grdacc.f:193-202); -1 for cells past the mesh end
 __device__ __forceinline__ int gx_corners(const DevGeo& g, int key, int* ic) {
     const int na = g.na;
-    int end = ((key + 1) % na) == 0;
+    int jt;
+    gx_div_na(g, key, jt);
+    const int end = (jt == na - 1);
     ic[0] = key;
     ic[1] = key + 1 - (end ? na : 0);
     ic[2] = key + na;

@@ -18,7 +18,8 @@
 // ---------------------------------------------------------------------------
 // row key of a cell (nrow for particles off the grid)
 __device__ __forceinline__ uint32_t row_of(const DevGeo& g, const CellW& c) {
-    return (c.key >= 0) ? (uint32_t)(c.key / g.na) : (uint32_t)g.nrow;
+    int r;
+    return (c.key >= 0) ? (uint32_t)gx_div_na(g, c.key, r) : (uint32_t)g.nrow;
 }
 
 // interpolated acceleration and potential of a particle at (x, y, z) whose
