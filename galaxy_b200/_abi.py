@@ -20,6 +20,7 @@ GX_SOFT_PLUMMER = 1
 GX_SOFT_SPLINE = 2
 GX_PREC_MIXED = 0
 GX_PREC_FP64 = 1
+GX_PREC_MIXED_TC05 = 2
 GX_FLAG_COMPENSATED = 1
 
 GX_GRID_MASS = 0

@@ -49,6 +49,9 @@ struct GxSfp {
     float* part = nullptr;      // per-warp partial moments
     double* mom = nullptr;      // [D][NCP] FP64 moments
     double* qc = nullptr;       // device force series [2][maxm+1][D]
+    double* upart = nullptr;    // per-CTA FP64 partial moments of the tcgen05 path
+    int32_t* errword = nullptr; // device error word (bounded waits)
+    int nsm = 0;
     float last_ms = 0.f;
     int64_t launches = 0;
 };
@@ -426,6 +429,10 @@ extern "C" int gx_sfp_init(const GxSfpBasis* b, double maxr, int device, GxSfp**
     if (e == cudaSuccess) e = cudaEventCreate(&s->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&s->e1);
     if (e == cudaSuccess) e = cudaMalloc((void**)&s->mom, sizeof(double) * 64 * 32);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s->upart, sizeof(double) * (size_t)s->nsm * 32 * 32);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s->errword, sizeof(int32_t));
+    if (e == cudaSuccess) e = cudaMemset(s->errword, 0, sizeof(int32_t));
     if (e != cudaSuccess) {
         g_sfp_err = std::string("CUDA: ") + cudaGetErrorString(e);
         delete s;
@@ -439,7 +446,7 @@ extern "C" void gx_sfp_destroy(GxSfp* s) {
     if (!s) return;
     cudaSetDevice(s->dev);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    void* p[] = {s->xy, s->part, s->mom, s->qc};
+    void* p[] = {s->xy, s->part, s->mom, s->qc, s->upart, s->errword};
     for (void* q : p)
         if (q) cudaFree(q);
     if (s->e0) cudaEventDestroy(s->e0);
@@ -485,6 +492,312 @@ extern "C" int gx_sfp_load(GxSfp* s, const float* coords, int64_t n, int stride)
     return GX_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Moments on the 5th-generation tensor cores (tcgen05, TMEM accumulator).
+//
+// One tcgen05.mma.cta_group::1.kind::tf32 per 8 particles, M = 128, N = 40,
+// K = 8, both operands K-major in shared memory without swizzle:
+//   A rows 0..31   T_d hi (TF32 part of T_d(x_p)), rows 32..63 T_d lo
+//   (T_d - hi); rows 64..127 are not used (the tile of the next K-block,
+//   read by the MMA, never read back).
+//   B rows  0      g_0 = 1, rows 1..16 g_n hi, rows 17..32 g_n lo, 33..39 0.
+// D[m][n] in TMEM then holds every product of the hi/lo split:
+//   M[d][0] = D[d][0] + D[d+32][0],
+//   M[d][c] = D[d][c] + D[d][c+16] + D[d+32][c] + D[d+32][c+16]  (c = 1..16).
+// Layout of a K-block tile (UMMA canonical K-major, no swizzle): core
+// matrices of 8 rows x 16 bytes; the two 16-byte halves of K are LBO = 144
+// bytes apart, 8-row groups SBO = 288 bytes apart; consecutive K-blocks of a
+// round are 2336 (A) / 1440 (B) bytes apart.  These strides put the 32
+// scalar stores of a warp (4 K-blocks x 8 particles) on 32 distinct banks.
+// A CTA of 256 threads takes rounds of 128 particles (two threads per
+// particle: one writes its T rows, the other its g rows),
+// triple-buffered; one thread issues the 16 MMAs of a round and commits
+// them to the buffer's mbarrier.  Every UM_DRAIN rounds the accumulator is
+// drained into FP64 shared memory (warps 0 and 1 read TMEM lanes 0..63)
+// and the next MMA starts it afresh.  Waits are bounded; on time-out the
+// CTA raises the error word, waits (bounded) for its MMAs, frees its TMEM.
+#define UM_T 128          // particles per round
+#define UM_THREADS 256    // threads 0..127 write the T rows, 128..255 the g rows
+#define UM_KB (UM_T / 8)  // K-blocks per round
+#define UM_N 40
+#define UM_LBO 144
+#define UM_SBO 288
+#define UM_SA 2336        // A bytes per K-block (8 groups x 288 + 32)
+#define UM_SB 1440        // B bytes per K-block (5 groups x 288)
+#define UM_ABYTES (UM_KB * UM_SA + 8 * UM_SBO)  // + the rows 64..127 of the last K-block
+#define UM_BUFBYTES (UM_ABYTES + UM_KB * UM_SB)
+#define UM_NBUF 3
+#define UM_DRAIN 8
+#define UM_TMEM_COLS 64
+#define UM_SPIN (1u << 22)
+
+__device__ __forceinline__ uint32_t um_smem(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ uint32_t um_off(int r, int k) {
+    return (uint32_t)((r >> 3) * UM_SBO + (k >> 2) * UM_LBO + (r & 7) * 16 + (k & 3) * 4);
+}
+// shared-memory matrix descriptor: start, LBO, SBO (16-byte units), version 1
+__device__ __forceinline__ uint64_t um_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+    d |= (uint64_t)((UM_LBO >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((UM_SBO >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;  // version
+    return d;                // base offset 0, legacy LBO mode, no swizzle
+}
+// instruction descriptor: D F32, A and B TF32, both K-major, N = 40, M = 128
+#define UM_IDESC ((1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(UM_N >> 3) << 17) | (8u << 24))
+
+__device__ __forceinline__ void um_mma(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %3, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %4, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "l"(ad), "l"(bd), "r"(accumulate), "r"(UM_IDESC), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+__device__ __forceinline__ void um_commit(uint64_t* mbar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     um_smem(mbar))
+                 : "memory");
+}
+__device__ __forceinline__ bool um_try(uint64_t* b, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(um_smem(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool um_wait(uint64_t* b, uint32_t parity) {
+    for (uint32_t i = 0; i < UM_SPIN; i++)
+        if (um_try(b, parity)) return true;
+    return false;
+}
+__device__ __forceinline__ void um_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void um_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+// 8 consecutive FP32 columns of this warp's 32 TMEM lanes
+__device__ __forceinline__ void um_ld8(uint32_t taddr, float* v) {
+    uint32_t r[8];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__global__ void __launch_bounds__(UM_THREADS + 64, 1) k_sfp_umma(const float* __restrict__ X,
+                                                                  const float* __restrict__ Y, int64_t n,
+                                                                  float inv_maxr, int maxm,
+                                                                  double* __restrict__ part, int NCP,
+                                                                  int32_t* __restrict__ errword) {
+    extern __shared__ __align__(1024) unsigned char um_sm[];
+    __shared__ __align__(8) uint64_t full[UM_NBUF], empty[UM_NBUF];
+    __shared__ uint32_t tmem_slot;
+    unsigned char* buf0 = um_sm;
+    double* drain = reinterpret_cast<double*>(um_sm + UM_NBUF * UM_BUFBYTES);  // [64][UM_N]
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int NG = 2 * maxm;  // harmonic columns g_1 .. g_NG
+    const int nthr = UM_THREADS + 64;
+    const int MMAW = UM_THREADS / 32;  // warps MMAW (issue + lanes 0..31), MMAW + 1 (lanes 32..63)
+    if (tid == 0) {
+        for (int b = 0; b < UM_NBUF; b++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(um_smem(&full[b])), "r"(UM_THREADS / 32)
+                         : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(um_smem(&empty[b])) : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int i = tid; i < 64 * UM_N; i += nthr) drain[i] = 0.0;
+    // zero every buffer once (B rows past the harmonics, the padding rows)
+    for (int i = tid; i < UM_NBUF * UM_BUFBYTES / 4; i += nthr) reinterpret_cast<float*>(um_sm)[i] = 0.f;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == MMAW) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(um_smem(&tmem_slot)),
+                     "r"(UM_TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    um_fence_before();
+    __syncthreads();
+    um_fence_after();
+    const uint32_t tmem = tmem_slot;
+    const int64_t rounds_total = (n + UM_T - 1) / UM_T;
+    const int64_t my_rounds = (blockIdx.x < rounds_total) ? (rounds_total - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+
+    if (warp < MMAW) {
+        // ------------------------------------------------------------ producers
+        const int pt = tid & (UM_T - 1), role = tid / UM_T;  // particle of the round, rows written
+        float nx = 0.f, ny = 0.f;
+        bool nv = false;
+        if (my_rounds > 0) {
+            const int64_t i = (int64_t)blockIdx.x * UM_T + pt;
+            if (i < n) {
+                nx = __ldg(X + i);
+                ny = __ldg(Y + i);
+                nv = true;
+            }
+        }
+        for (int64_t li = 0; li < my_rounds; li++) {
+            const int64_t rnd = blockIdx.x + li * gridDim.x;
+            const float cx = nx, cy = ny;
+            const bool cv = nv;
+            {
+                const int64_t i = (rnd + gridDim.x) * UM_T + pt;
+                nv = false;
+                if (li + 1 < my_rounds && i < n) {
+                    nx = __ldg(X + i);
+                    ny = __ldg(Y + i);
+                    nv = true;
+                }
+            }
+            const int b = (int)(li % UM_NBUF);
+            if (li >= UM_NBUF && !um_wait(&empty[b], (uint32_t)(((li / UM_NBUF) - 1) & 1))) {
+                atomicExch(errword, 5);
+                break;
+            }
+            unsigned char* A = buf0 + (size_t)b * UM_BUFBYTES;
+            unsigned char* B = A + UM_ABYTES;
+            // a slot past the last particle sits outside the basis edge
+            const float px = cv ? cx * inv_maxr : 2.f;
+            const float py = cv ? cy * inv_maxr : 0.f;
+            const float p2 = px * px + py * py;
+            const bool act = p2 <= 1.0f;
+            const float xc = 2.f * p2 - 1.f;
+            const int kb = pt >> 3, k = pt & 7;
+            if (role == 0) {
+                unsigned char* a = A + kb * UM_SA;
+                float tm2 = 1.f, tm1 = xc;
+#pragma unroll
+                for (int d = 0; d < 32; d++) {
+                    float t;
+                    if (d == 0) t = 1.f;
+                    else if (d == 1) t = xc;
+                    else {
+                        t = 2.f * xc * tm1 - tm2;
+                        tm2 = tm1;
+                        tm1 = t;
+                    }
+                    t = act ? t : 0.f;
+                    const float hi = __uint_as_float(f2tf32(t));
+                    *reinterpret_cast<float*>(a + um_off(d, k)) = hi;
+                    *reinterpret_cast<float*>(a + um_off(d + 32, k)) = t - hi;
+                }
+            } else {
+                unsigned char* bb = B + kb * UM_SB;
+                *reinterpret_cast<float*>(bb + um_off(0, k)) = act ? 1.f : 0.f;
+                const float pr = sqrtf(p2);
+                const float cr = pr > 0.f ? px / pr : 1.f, ci = pr > 0.f ? py / pr : 0.f;
+                float zr = 1.f, zi = 0.f;
+#pragma unroll
+                for (int u = 0; u < 16; u += 2) {
+                    const int m = u / 2 + 1;
+                    float gc = 0.f, gs = 0.f;
+                    if (u < NG) {
+                        const float nr = zr * cr - zi * ci;
+                        zi = zr * ci + zi * cr;
+                        zr = nr;
+                        const float f = (m & 1) ? pr : 1.f;
+                        gc = act ? zr * f : 0.f;
+                        gs = act ? zi * f : 0.f;
+                    }
+                    const float hc = __uint_as_float(f2tf32(gc)), hs = __uint_as_float(f2tf32(gs));
+                    *reinterpret_cast<float*>(bb + um_off(1 + u, k)) = hc;
+                    *reinterpret_cast<float*>(bb + um_off(2 + u, k)) = hs;
+                    *reinterpret_cast<float*>(bb + um_off(17 + u, k)) = gc - hc;
+                    *reinterpret_cast<float*>(bb + um_off(18 + u, k)) = gs - hs;
+                }
+            }
+            // generic-proxy stores -> async proxy (the tensor core reads shared memory)
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(um_smem(&full[b])) : "memory");
+        }
+    } else {
+        // ------------------------------------------------- MMA issue and drain
+        // both warps take every iteration and every named barrier; after a
+        // failed wait a warp only skips work (never the barrier)
+        const bool issuer = (warp == MMAW);
+        bool ok = true;
+        int since = 0;
+        for (int64_t li = 0; li < my_rounds; li++) {
+            const int b = (int)(li % UM_NBUF);
+            if (issuer && ok) {
+                if (!um_wait(&full[b], (uint32_t)((li / UM_NBUF) & 1))) {
+                    atomicExch(errword, 5);
+                    ok = false;
+                }
+                um_fence_after();
+                if (ok && lane == 0) {
+                    const uint32_t a0 = um_smem(buf0 + (size_t)b * UM_BUFBYTES), b0 = a0 + UM_ABYTES;
+#pragma unroll 1
+                    for (int kb = 0; kb < UM_KB; kb++)
+                        um_mma(tmem, um_desc(a0 + kb * UM_SA), um_desc(b0 + kb * UM_SB),
+                               (since == 0 && kb == 0) ? 0u : 1u);
+                    um_commit(&empty[b]);
+                }
+                __syncwarp();
+            }
+            since++;
+            if (since == UM_DRAIN || li + 1 == my_rounds) {
+                // both drain warps meet once the issuer has committed this round
+                // (a parity wait must not start more than one phase early), then
+                // wait for its MMAs (and all before)
+                asm volatile("bar.sync 1, 64;" ::: "memory");
+                if (ok && !um_wait(&empty[b], (uint32_t)((li / UM_NBUF) & 1))) {
+                    atomicExch(errword, 5);
+                    ok = false;
+                }
+                um_fence_after();
+                if (ok) {
+                    float v[UM_N];
+                    const int q = warp - MMAW;  // TMEM lanes 32 q .. 32 q + 31
+#pragma unroll
+                    for (int c = 0; c < UM_N; c += 8) um_ld8(tmem + ((uint32_t)(32 * q) << 16) + c, v + c);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                    double* dr = drain + (32 * q + lane) * UM_N;
+#pragma unroll
+                    for (int c = 0; c < UM_N; c++) dr[c] += (double)v[c];
+                }
+                um_fence_before();
+                asm volatile("bar.sync 1, 64;" ::: "memory");  // the next MMA may overwrite
+                um_fence_after();
+                since = 0;
+            }
+        }
+        if (!ok && issuer && lane == 0 && my_rounds > 0) {
+            // wait (bounded) for whatever was committed before freeing TMEM
+            for (int bb = 0; bb < UM_NBUF; bb++) um_wait(&empty[bb], 0u);
+        }
+    }
+    um_fence_before();
+    __syncthreads();
+    um_fence_after();
+    if (warp == MMAW)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UM_TMEM_COLS)
+                     : "memory");
+    // combine the hi/lo quadrants: part[cta][d][c], c < NCP
+    double* dst = part + (size_t)blockIdx.x * 32 * NCP;
+    for (int i = tid; i < 32 * NCP; i += nthr) {
+        const int d = i / NCP, c = i - d * NCP;
+        double v = 0.0;
+        if (c == 0) v = drain[d * UM_N] + drain[(d + 32) * UM_N];
+        else if (c <= NG && c <= 16)
+            v = drain[d * UM_N + c] + drain[d * UM_N + c + 16] + drain[(d + 32) * UM_N + c] +
+                drain[(d + 32) * UM_N + c + 16];
+        dst[i] = v;
+    }
+}
+
 // moments on the device (precision GX_PREC_MIXED: tensor cores; GX_PREC_FP64: CUDA cores)
 static int sfp_moments(GxSfp* s, int precision) {
     const int D = s->D, NCP = (s->NC + 7) / 8 * 8, nmom = D * NCP;
@@ -501,9 +814,25 @@ static int sfp_moments(GxSfp* s, int precision) {
         s->launches += 2;
         return GX_OK;
     }
+    const float inv = (float)(1.0 / s->maxr);
+    if (precision == GX_PREC_MIXED_TC05) {
+        if (D != 32 || s->NC > 17)
+            return s->err = "the tcgen05 path takes at most 32 Chebyshev terms and maxm <= 8", GX_ERR_RANGE;
+        // tcgen05: one CTA per SM (at most), FP64 partial per CTA
+        const int64_t rounds = (n + UM_T - 1) / UM_T;
+        const int grid = (int)std::min<int64_t>(rounds, s->nsm);
+        const size_t sm = (size_t)UM_NBUF * UM_BUFBYTES + sizeof(double) * 64 * UM_N;
+        SFP_CUDA(s, cudaFuncSetAttribute(k_sfp_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_sfp_umma<<<grid, UM_THREADS + 64, sm, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->upart, NCP,
+                                                  s->errword);
+        SFP_CUDA(s, cudaGetLastError());
+        k_sfp_reduce<double><<<32 * NCP, 256, 0, s->stream>>>(s->upart, grid, 32 * NCP, s->mom);
+        SFP_CUDA(s, cudaGetLastError());
+        s->launches += 2;
+        return GX_OK;
+    }
     const int64_t nw = (n + SFP_CHUNK - 1) / SFP_CHUNK;
     const unsigned grid = (unsigned)((nw * 32 + 255) / 256);
-    const float inv = (float)(1.0 / s->maxr);
     // feature columns 1 .. NC - 1 in blocks of 8
     const int NB = (s->NC - 1 + 7) / 8;
     if (NB > 3) return s->err = "more than 11 harmonics on the tensor-core path", GX_ERR_RANGE;
@@ -522,7 +851,8 @@ static int sfp_moments(GxSfp* s, int precision) {
 // sfpsum + scaled: coeff[n * (2 maxm + 1) + m + maxm] (cosine +m, sine -m)
 extern "C" int gx_sfp_sum(GxSfp* s, int precision, double pmass, double* coeff) {
     if (!s || !coeff) return GX_ERR_ARG;
-    if (precision != GX_PREC_MIXED && precision != GX_PREC_FP64) return GX_ERR_ARG;
+    if (precision != GX_PREC_MIXED && precision != GX_PREC_FP64 && precision != GX_PREC_MIXED_TC05)
+        return GX_ERR_ARG;
     cudaSetDevice(s->dev);
     const int D = s->D, NCP = (s->NC + 7) / 8 * 8;
     const int ngx = 2 * s->b.maxm + 1, maxm = s->b.maxm;
@@ -538,6 +868,14 @@ extern "C" int gx_sfp_sum(GxSfp* s, int precision, double pmass, double* coeff) 
         SFP_CUDA(s, cudaMemcpyAsync(mom.data(), s->mom, sizeof(double) * D * NCP, cudaMemcpyDeviceToHost, s->stream));
     SFP_CUDA(s, cudaStreamSynchronize(s->stream));
     SFP_CUDA(s, cudaEventElapsedTime(&s->last_ms, s->e0, s->e1));
+    {
+        int32_t ew = 0;
+        SFP_CUDA(s, cudaMemcpy(&ew, s->errword, sizeof ew, cudaMemcpyDeviceToHost));
+        if (ew) {
+            cudaMemset(s->errword, 0, sizeof ew);
+            return s->err = "device check raised the error word", GX_ERR_DEVICE;
+        }
+    }
     memset(coeff, 0, sizeof(double) * (size_t)(s->b.maxn + 1) * ngx);
     const double fac = pmass / (s->maxr * s->maxr);
     for (int f = 0; f < s->nfun; f++) {

@@ -53,6 +53,7 @@ extern "C" {
 /* arithmetic of the step */
 #define GX_PREC_MIXED       0   /* FP32 bulk, FP64 Green table/diagnostics  */
 #define GX_PREC_FP64        1   /* plain FP64 path (the comparison baseline) */
+#define GX_PREC_MIXED_TC05  2   /* gx_sfp_sum only: the tcgen05 (TMEM) tensor path */
 
 /* flags */
 #define GX_FLAG_COMPENSATED 1   /* compensated (two-float) position update  */
@@ -276,9 +277,13 @@ int gx_sfp_load(GxSfp* sfp, const float* coords, int64_t n, int stride);
 /* sfpsum/sfpadd + scaled: coefficients of the loaded particles with
  * r <= maxr, x pmass / maxr^2, into coeff[n * (2 maxm + 1) + m + maxm]
  * (cosine terms at +m, sine terms at -m).  precision GX_PREC_MIXED runs the
- * moment sum on the tensor cores (3xTF32, FP32 accumulate per chunk, FP64
- * across chunks); GX_PREC_FP64 on the CUDA cores in FP64.
- * SRC/lib15/sfpsum.f:26-47, sfpadd.f:37-93, scaled.f:53-72. */
+ * moment contraction on the tensor cores with warp-level mma.sync TF32
+ * (operands split hi/lo, 3 products, FP32 accumulate per 1024-particle
+ * chunk, FP64 across chunks); GX_PREC_MIXED_TC05 on the tcgen05 tensor cores
+ * (all four hi/lo products in one MMA of M = 128, N = 40, K = 8 per 8
+ * particles, accumulator in TMEM drained to FP64 every 1024 particles per
+ * CTA; at most 32 Chebyshev terms and maxm <= 8); GX_PREC_FP64 on the CUDA
+ * cores in FP64.  SRC/lib15/sfpsum.f:26-47, sfpadd.f:37-93, scaled.f:53-72. */
 int gx_sfp_sum(GxSfp* sfp, int precision, double pmass, double* coeff);
 
 /* sfpacc: Cartesian accelerations [n][2] and potentials [n] (pot may be
