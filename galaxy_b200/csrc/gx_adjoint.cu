@@ -516,6 +516,8 @@ extern "C" int gx_adjoint(GxCtx* c, int nsteps, int ckpt_every, double* J_out, f
     // the context again holds the initial particles (load order) and their mass
     k_adj_scatter<<<nb, ADJ_BS, 0, st>>>(b.ck, n, c->pbuf[c->cur], c->cap, c->origin, c->perm);
     GX_LAUNCHED(c);
+    if (g.comp)  // the low parts of compensated positions start at zero, as after gx_loadup
+        GX_CUDA(c, cudaMemsetAsync(c->pbuf[c->cur] + (size_t)4 * c->cap, 0, sizeof(float) * 2 * c->cap, st));
     c->have_keys = false;
     int rc = gx_mixed_masset(c);
     if (rc) return rc;

@@ -107,6 +107,7 @@ void fill_devgeo(GxCtx* c) {
     d.inv_dzg = (d.ndim == 3) ? 1.0f / c->cfg.dzg : 0.f;
     d.t_scale = (float)((double)G.na / (2.0 * GX_PI));
     d.inv_na = 1.0f / (float)G.na;
+    d.comp = (c->cfg.flags & GX_FLAG_COMPENSATED) ? 1 : 0;
     d.halo_v2 = c->cfg.halo_v2;
     d.halo_rc2 = c->cfg.halo_rc * c->cfg.halo_rc;
     d.pmass = c->cfg.pmass;
@@ -374,8 +375,11 @@ static int alloc_particles(GxCtx* c, int64_t n) {
         DALLOC(c, c->acc64, 3 * cap);
         return GX_OK;
     }
-    DALLOC(c, c->pbuf[0], nw * cap);
-    DALLOC(c, c->pbuf[1], nw * cap);
+    // compensated positions keep a low part of every coordinate after the
+    // 2 ndim planes of the records
+    const int planes = nw + (c->g.comp ? c->g.ndim : 0);
+    DALLOC(c, c->pbuf[0], planes * cap);
+    DALLOC(c, c->pbuf[1], planes * cap);
     DALLOC(c, c->perm, cap);
     DALLOC(c, c->origin, cap);
     DALLOC(c, c->origin_tmp, cap);
@@ -417,6 +421,9 @@ int gx_loadup(GxCtx* c, const float* coords, int64_t n) {
         c->cur = 0;
         k_aos_to_soa<<<nb, bs, 0, c->stream>>>(staging, c->pbuf[0], n, c->cap, nw);
         GX_LAUNCHED(c);
+        if (c->g.comp)
+            GX_CUDA(c, cudaMemsetAsync(c->pbuf[0] + (size_t)nw * c->cap, 0,
+                                       sizeof(float) * c->g.ndim * c->cap, c->stream));
         k_iota<<<nb, bs, 0, c->stream>>>(c->origin, n);
         GX_LAUNCHED(c);
         k_iota<<<nb, bs, 0, c->stream>>>(c->perm, n);

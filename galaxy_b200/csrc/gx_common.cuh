@@ -30,6 +30,7 @@ struct DevGeo {
     float alpha, ua, inv_ua, uoffs, rinh, rgrid, zm, thmax, dzg, inv_dzg;
     float t_scale;  // na / (2 pi) in FP32
     float inv_na;   // 1 / na (fast division of cell keys, gx_div_na)
+    int comp;       // compensated positions: planes 2 ndim .. 3 ndim - 1 hold the low parts
     float halo_v2, halo_rc2;
     float pmass;
     // FP64 copies for the plain FP64 path
@@ -240,6 +241,19 @@ __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, floa
         c.key = (ju * g.ngz + jz) * g.na + jt;
     }
     return c;
+}
+
+// x + v with the rounding error of the sum carried in a low part (the
+// compensated drift): Knuth's two-sum of hi and v, then the error folded
+// into lo and (hi, lo) renormalised so that |lo| <= ulp(hi) / 2
+__device__ __forceinline__ void gx_comp_add(float& hi, float& lo, float v) {
+    const float s = __fadd_rn(hi, v);
+    const float bp = __fsub_rn(s, hi);
+    const float err = __fadd_rn(__fsub_rn(hi, __fsub_rn(s, bp)), __fsub_rn(v, bp));
+    const float l = __fadd_rn(lo, err);
+    const float t = __fadd_rn(s, l);
+    lo = __fsub_rn(l, __fsub_rn(t, s));
+    hi = t;
 }
 
 // 8 (3D) or 4 (2D) weights in the reference order (weight.f:92-99, 241-248)

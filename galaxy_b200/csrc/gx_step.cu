@@ -114,11 +114,24 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
         gx_accel_cell(g, F, cw, x, y, z, ax, ay, az, ph);
         vx += ax;
         vy += ay;
-        x += vx;
-        y += vy;
-        if (d3) {
-            vz += az;
-            z += vz;
+        if (d3) vz += az;
+        if (g.comp) {
+            // compensated drift: the low parts travel with the particle
+            const int nw = 2 * g.ndim;
+            float xl = Pin[nw * cap + p], yl = Pin[(nw + 1) * cap + p];
+            gx_comp_add(x, xl, vx);
+            gx_comp_add(y, yl, vy);
+            Pout[nw * cap + s] = xl;
+            Pout[(nw + 1) * cap + s] = yl;
+            if (d3) {
+                float zl = Pin[(nw + 2) * cap + p];
+                gx_comp_add(z, zl, vz);
+                Pout[(nw + 2) * cap + s] = zl;
+            }
+        } else {
+            x += vx;
+            y += vy;
+            if (d3) z += vz;
         }
         Pout[s] = x;
         Pout[cap + s] = y;

@@ -174,3 +174,36 @@ def test_mixed_force_error_vs_fp64_path():
     perr = np.linalg.norm(p32 - p64) / np.linalg.norm(p64)
     assert err < 1e-5, err
     assert perr < 1e-5, perr
+
+
+def test_compensated_drift_tracks_the_exact_sum():
+    """GX_FLAG_COMPENSATED: the drift x += v carries its rounding error in a
+    low part.  With no mass the step is a pure drift, so after T steps the
+    stored (FP32) position must be the FP32 rounding of x0 + T v (summed
+    exactly), while the plain FP32 drift accumulates one rounding per step."""
+    from galaxy_b200 import GX_FLAG_COMPENSATED
+    rng = np.random.default_rng(5)
+    n, T = 4000, 3000
+    r = rng.uniform(0.5, 3.0, n)
+    th = rng.uniform(0, 2 * np.pi, n)
+    rec = np.zeros((n, 4), np.float32)
+    rec[:, 0] = r * np.cos(th)
+    rec[:, 1] = r * np.sin(th)
+    rec[:, 2:] = rng.uniform(-1e-3, 1e-3, (n, 2))
+    exact = rec[:, :2].astype(np.float64) + T * rec[:, 2:].astype(np.float64)
+    err = {}
+    for flags in (0, GX_FLAG_COMPENSATED):
+        cfg = cfg2()
+        cfg.pmass = 0.0
+        cfg.flags = flags
+        with Galaxy(cfg) as gal:
+            gal.greenm()
+            gal.loadup(rec)
+            gal.masset()
+            gal.step(T)
+            out = gal.unload()
+        assert np.array_equal(out[:, 2:], rec[:, 2:])  # no force: velocities unchanged
+        ulp = np.spacing(np.abs(exact).astype(np.float32)).astype(np.float64)
+        err[flags] = np.max(np.abs(out[:, :2] - exact) / ulp)
+    assert err[GX_FLAG_COMPENSATED] <= 1.0, err
+    assert err[0] > 8 * err[GX_FLAG_COMPENSATED], err
