@@ -229,6 +229,24 @@ def run_ours(args, w, rank, world, comm):
                             "frac": round(sb / (out["ms_per_step"] * 1e-3) / 1e9 / peak, 4)}
     out["phases"] = phases
     gal.close()
+    # the same step with the compensated position update (GX_FLAG_COMPENSATED)
+    if rank == 0 and not args.no_fp64:
+        from galaxy_b200 import GX_FLAG_COMPENSATED
+        cfgc = make_cfg(w, GX_PREC_MIXED)
+        cfgc.pmass = pm / world
+        cfgc.device = cfg.device
+        cfgc.flags = GX_FLAG_COMPENSATED
+        with Galaxy(cfgc) as gc:
+            gc.greenm()
+            gc.loadup(rec)
+            gc.masset()
+            gc.tmcent(True)
+            gc.step(3)
+            kc = 50
+            gc.step(kc)
+            msc = gc.last_step_ms() / kc
+        out["compensated_step"] = {"ms_per_step": round(msc, 4), "value": n / (msc * 1e-3),
+                                   "what": "GX_FLAG_COMPENSATED: two-float positions (+12 B per particle per step)"}
     # plain FP64 path on the same particles: rate and force error
     if rank == 0 and not args.no_fp64:
         cfg64 = make_cfg(w, GX_PREC_FP64)
@@ -550,6 +568,7 @@ def main():
                 "fp64_path": out.get("fp64_path"),
                 "speedup_vs_fp64_path": out.get("speedup_vs_fp64_path"),
                 "force_rel_err": out.get("force_rel_err"),
+                "compensated_step": out.get("compensated_step"),
                 "step_roofline": out["step_roofline"], "phases": out["phases"], "sfp": sfp,
                 "ensemble": ens, "adjoint": adj}
         print(json.dumps(line))
