@@ -71,6 +71,8 @@ def lib():
         L.gx_set_profile.argtypes = [P, C.c_int]
         L.gx_phase_ms.argtypes = [P, P, P]
         L.gx_adjoint.argtypes = [P, C.c_int, C.c_int, P, P, P, P]
+        L.gx_set_zones.argtypes = [P, C.c_int32, P, P]
+        L.gx_zone_info.argtypes = [P, P, P]
         _lib = L
     return _lib
 
@@ -243,6 +245,23 @@ class Galaxy:
         self._chk(self._L.gx_adjoint(self._h, int(nsteps), int(ckpt_every), _ptr(J), _ptr(grad),
                                      _ptr(dth), _ptr(drift)))
         return float(J[0]), grad, dth, float(drift[0])
+
+    def set_zones(self, nstep, zbr):
+        """Multiple time-step zones (before loadup): zone i steps every
+        nstep[i] base steps and holds the particles at radius >= zbr[i]
+        (grid units; nstep[0] = 1, zbr[0] unused)."""
+        nstep = np.ascontiguousarray(nstep, np.int32)
+        zbr = np.ascontiguousarray(zbr, np.float32)
+        assert nstep.size == zbr.size
+        self._chk(self._L.gx_set_zones(self._h, int(nstep.size), _ptr(nstep), _ptr(zbr)))
+
+    def zone_info(self):
+        """(zone code of every particle in load order, 1..nzones or
+        nzones + 1 off the grid; the step counter)"""
+        zone = np.zeros(self.n, np.int32)
+        istep = np.zeros(1, np.int32)
+        self._chk(self._L.gx_zone_info(self._h, _ptr(zone), _ptr(istep)))
+        return zone, int(istep[0])
 
     def tmcent(self, start=True):
         self._chk(self._L.gx_tmcent(self._h, int(start)))

@@ -404,6 +404,8 @@ extern "C" int gx_adjoint(GxCtx* c, int nsteps, int ckpt_every, double* J_out, f
     if (!c || nsteps < 0 || ckpt_every < 1 || !J_out || !grad || !dtheta) return GX_ERR_ARG;
     if (c->fp64 || c->g.ndim != 2 || c->g.nsect != 1)
         return c->err = "the adjoint runs 2D one-sector grids on the mixed path", GX_ERR_ARG;
+    if (c->nzones > 1) return c->err = "the adjoint runs a single time-step zone", GX_ERR_ARG;
+    if (c->g.halo > 1) return c->err = "the adjoint differentiates the ISOT halo only", GX_ERR_ARG;
     if (!c->have_green) return c->err = "no Green table (call gx_greenm)", GX_ERR_STATE;
     if (c->spec.nact > 64) return c->err = "more than 64 active harmonics", GX_ERR_RANGE;
     const int64_t n = c->n;

@@ -40,6 +40,8 @@ int setgrd(const GxConfig* c, GxGeometry* g, std::string& err) {
     if (!(c->softl > 0.f)) return err = "Softening length must be greater than 0", GX_ERR_ARG;
     if (c->rmap != GX_RMAP_STDPOL && c->rmap != GX_RMAP_LOG) return err = "unknown radial map", GX_ERR_ARG;
     if (c->rmap == GX_RMAP_LOG && !(c->rmap_r0 > 0.f)) return err = "log map needs rmap_r0 > 0", GX_ERR_ARG;
+    if (c->halo < 0 || c->halo > 2) return err = "unknown rigid force (halo)", GX_ERR_ARG;
+    if (c->halo > 0 && !(c->halo_rc > 0.f)) return err = "halo_rc must be positive", GX_ERR_ARG;
     if (c->precision != GX_PREC_MIXED && c->precision != GX_PREC_FP64)
         return err = "unknown precision", GX_ERR_ARG;
     g->nr = c->nr;
@@ -232,7 +234,7 @@ void gx_destroy(GxCtx* c) {
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
                     c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->perm_next, c->rowstart,
                     c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->rowtile, c->stage, c->jrk_d,
-                    c->errword, c->dsum};
+                    c->errword, c->dsum, c->pzone[0], c->pzone[1], c->zbuf, c->zjrk_d};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i <= GX_NPHASE; i++)
@@ -350,13 +352,15 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     // grow: free old
     void* old[] = {c->pbuf[0], c->pbuf[1], c->perm, c->origin, c->origin_tmp, c->pkey[0], c->pkey[1],
                    c->pfr[0], c->pfr[1], c->p64,
-                   c->key64, c->w64, c->acc64, c->ppot, c->pacc, c->perm_next, c->items, c->stage};
+                   c->key64, c->w64, c->acc64, c->ppot, c->pacc, c->perm_next, c->items, c->stage,
+                   c->pzone[0], c->pzone[1]};
     for (void* p : old)
         if (p) cudaFree(p);
     c->pbuf[0] = c->pbuf[1] = nullptr;
     c->perm = c->origin = c->origin_tmp = nullptr;
     c->pkey[0] = c->pkey[1] = nullptr;
     c->pfr[0] = c->pfr[1] = nullptr;
+    c->pzone[0] = c->pzone[1] = nullptr;
     c->p64 = nullptr;
     c->key64 = nullptr;
     c->w64 = c->acc64 = nullptr;
@@ -407,7 +411,7 @@ int gx_loadup(GxCtx* c, const float* coords, int64_t n) {
     c->n = n;
     c->have_mass = c->have_field = c->have_keys = false;
     const int nw = 2 * c->g.ndim;
-    if (n == 0) return GX_OK;
+    if (n == 0) return (c->nzones > 1 && !c->fp64) ? gx_zone_loadup(c) : GX_OK;
     float* staging = nullptr;
     GX_CUDA(c, cudaMallocAsync((void**)&staging, sizeof(float) * nw * n, c->stream));
     GX_CUDA(c, cudaMemcpyAsync(staging, coords, sizeof(float) * nw * n, cudaMemcpyHostToDevice,
@@ -428,6 +432,10 @@ int gx_loadup(GxCtx* c, const float* coords, int64_t n) {
         GX_LAUNCHED(c);
         k_iota<<<nb, bs, 0, c->stream>>>(c->perm, n);
         GX_LAUNCHED(c);
+        if (c->nzones > 1) {
+            rc = gx_zone_loadup(c);
+            if (rc) return rc;
+        }
     }
     GX_CUDA(c, cudaFreeAsync(staging, c->stream));
     GX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -447,6 +455,10 @@ int gx_unload(GxCtx* c, float* coords) {
     if (c->fp64) k_soa64_to_aos<<<nb, bs, 0, c->stream>>>(c->p64, staging, n, c->cap, nw);
     else k_soa_to_aos<<<nb, bs, 0, c->stream>>>(c->pbuf[c->cur], c->origin, staging, n, c->cap, nw);
     GX_LAUNCHED(c);
+    if (c->nzones > 1) {
+        int rc = gx_zone_unload(c, staging);
+        if (rc) return rc;
+    }
     GX_CUDA(c, cudaMemcpyAsync(coords, staging, sizeof(float) * nw * n, cudaMemcpyDeviceToHost,
                                c->stream));
     GX_CUDA(c, cudaFreeAsync(staging, c->stream));
@@ -457,7 +469,7 @@ int gx_unload(GxCtx* c, float* coords) {
 int gx_masset(GxCtx* c) {
     if (!c) return GX_ERR_ARG;
     cudaSetDevice(c->dev);
-    int rc = c->fp64 ? gx_fp64_masset(c) : gx_mixed_masset(c);
+    int rc = c->fp64 ? gx_fp64_masset(c) : (c->nzones > 1 ? gx_zone_masset(c) : gx_mixed_masset(c));
     if (rc) return rc;
     GX_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_mass = true;
@@ -504,7 +516,8 @@ int gx_step(GxCtx* c, int nsteps, int phys) {
     cudaSetDevice(c->dev);
     c->launches = 0;
     GX_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    int rc = c->fp64 ? gx_fp64_step(c, nsteps, phys) : gx_mixed_step(c, nsteps, phys);
+    int rc = c->fp64 ? gx_fp64_step(c, nsteps, phys)
+                     : (c->nzones > 1 ? gx_zone_step(c, nsteps, phys) : gx_mixed_step(c, nsteps, phys));
     if (rc) return rc;
     GX_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     GX_CUDA(c, cudaEventSynchronize(c->ev1));

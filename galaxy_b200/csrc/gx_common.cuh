@@ -37,6 +37,15 @@ struct DevGeo {
     double ua_d, uoffs_d, rinh_d, rgrid_d, zm_d, thmax_d, dzg_d, halo_v2_d, halo_rc2_d;
 };
 
+// Time-step zones (gx_zones.cu): zone i (1-based) steps every nstep[i-1]
+// base steps and holds the particles at radius >= zbr[i-1]; code nz + 1
+// marks a particle off the grid.
+struct ZoneTab {
+    int nz;
+    int nstep[GX_MAX_ZONES];
+    float zbr[GX_MAX_ZONES];
+};
+
 // Spectral bookkeeping: active harmonics (lg false, m < ng).
 struct Spec {
     int nact;        // number of active harmonics
@@ -124,6 +133,18 @@ struct GxCtx {
     float phase_ms[GX_NPHASE] = {};
     int64_t phase_n[GX_NPHASE] = {};
     int open_phase = -1;
+
+    // time-step zones (gx_zones.cu); nzones = 1 is the single-zone step
+    int nzones = 1;
+    ZoneTab zt = {};
+    int32_t* pzone[2] = {nullptr, nullptr};  // zone code of the particles of pbuf[i]
+    float* zbuf = nullptr;                   // [2][nzones][mesh] mass arrays of zones 2..nzones
+    float* znew[GX_MAX_ZONES] = {};          // newest array of each zone (index >= 1)
+    float* zold[GX_MAX_ZONES] = {};          // the one before it
+    int32_t* zjrk_d = nullptr;               // [GX_MAX_ZONES][2] ring range of each zone's mass
+    int istep = 0;                           // step counter of the zone schedule
+    int lstep[GX_MAX_ZONES][2] = {};         // step numbers of zold, znew
+    bool zones_ready = false;                // zone arrays deposited (gx_masset)
 
     // multi-GPU (gx_comm.cu): NCCL communicator of the particle decomposition
     void* comm = nullptr;
@@ -337,6 +358,65 @@ __device__ __forceinline__ void gx_row_count(uint32_t row, bool act, uint32_t* _
     if (act && (peers & lanemask_lt()) == 0) atomicAdd(&cnt[row], (uint32_t)__popc(peers));
 }
 
+// fixed axisymmetric force of a softened Kuz'min-Toomre disc, applied to
+// every particle on the grid when the m = 0 harmonic is filtered out
+// (filset.f:3-5, getacc.f:118-121, axifrc.f, frdisc.f:27-29 'SOFT'):
+// F(r) = -K r / (r^2 + Rs^2)^1.5 with K = halo_v2 (the disc mass in
+// internal units, M lscale^3 ts^2) and Rs = halo_rc (grid units,
+// (1 + epsilon) rscale lscale, inimod.f:74); potential -K / sqrt(r^2 + Rs^2)
+// (phidsc.f:38).  Spherical radius in 3D, as getacc measures it.
+__device__ __forceinline__ void gx_disc_force(const DevGeo& g, float x, float y, float z, float& ax,
+                                              float& ay, float& az, float& ph) {
+    const float r2 = x * x + y * y + ((g.ndim == 3) ? z * z : 0.f);
+    const float d = r2 + g.halo_rc2;
+    const float sd = sqrtf(d);
+    const float f = -g.halo_v2 / (d * sd);
+    ax += f * x;
+    ay += f * y;
+    if (g.ndim == 3) az += f * z;
+    ph -= g.halo_v2 / sd;
+}
+
+// interpolated acceleration and potential of a particle at (x, y, z) whose
+// interpolation cell is cw: grdacc + halfrc (or the fixed disc force)
+__device__ __forceinline__ void gx_accel_cell(const DevGeo& g, const float4* __restrict__ F,
+                                              const CellW& cw, float x, float y, float z, float& ax,
+                                              float& ay, float& az, float& ph) {
+    ax = ay = az = ph = 0.f;
+    // particles off the grid feel no force (getacc.f:103-122 acts on the
+    // particles inside the grid)
+    if (cw.key < 0) return;
+    {
+        float w[8];
+        int ic[8];
+        gx_weights(g, cw, w);
+        const int nc = gx_corners(g, cw.key, ic);
+        for (int k = 0; k < nc; k++) {
+            if (ic[k] < 0) continue;
+            const float4 f = __ldg(F + ic[k]);
+            ax += f.x * w[k];
+            ay += f.y * w[k];
+            az += f.z * w[k];
+            ph += f.w * w[k];
+        }
+    }
+    if (g.halo == 1) {
+        // cored isothermal halo (frhalo.f:55-56): F(r) = -v^2 r / (r^2 + rc^2)
+        float r2 = x * x + y * y + ((g.ndim == 3) ? z * z : 0.f);
+        float rr = sqrtf(r2);
+        float fr = -g.halo_v2 * rr / (r2 + g.halo_rc2);
+        if (fr != 0.f) {
+            fr = fr / rr;
+            ax += fr * x;
+            ay += fr * y;
+            if (g.ndim == 3) az += fr * z;
+        }
+        ph += 0.5f * g.halo_v2 * logf(1.f + r2 / g.halo_rc2);
+    } else if (g.halo == 2) {
+        gx_disc_force(g, x, y, z, ax, ay, az, ph);
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host-side entry points implemented in the .cu files
 int setgrd(const GxConfig* c, GxGeometry* g, std::string& err);
@@ -352,7 +432,17 @@ int gx_fp64_masset(GxCtx* c);
 int gx_fp64_findf(GxCtx* c, int lpot, bool polcat);
 int gx_fp64_getacc(GxCtx* c, float* acc, float* pot);
 int gx_fp64_step(GxCtx* c, int nsteps, int phys);
-int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* perm_out);
+// rows counted by the caller's pass -> permutation, deposit, mass.  With
+// zone set, only particles whose zone code is zsel are deposited (the
+// counting pass filtered the same way); the mass goes to mass_out
+// (default c->mass), scaled by pm (default pmass).
+int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* perm_out,
+                    const int32_t* zone = nullptr, int zsel = 0, float* mass_out = nullptr,
+                    float pm = -1.f);
+int gx_zone_loadup(GxCtx* c);
+int gx_zone_unload(GxCtx* c, float* staging);
+int gx_zone_masset(GxCtx* c);
+int gx_zone_step(GxCtx* c, int nsteps, int phys);
 int gx_comm_reduce_range(GxCtx* c);
 int gx_synthesis(GxCtx* c, int tmask, float* polar);
 int gx_comm_reduce_spectrum(GxCtx* c);

@@ -176,7 +176,8 @@ __global__ void __launch_bounds__(ROW_TILE) k_row_scan(int nrow, int ngz, int nr
 // slot of every particle in the row-ordered permutation: perm[slot] = t
 __global__ void k_place(const int32_t* __restrict__ keys, int64_t n, int nrow, int na,
                         const int32_t* __restrict__ rowstart, const uint32_t* __restrict__ rowbase,
-                        uint32_t* __restrict__ rowfill, int32_t* __restrict__ perm) {
+                        uint32_t* __restrict__ rowfill, int32_t* __restrict__ perm,
+                        const int32_t* __restrict__ zone, int zsel) {
     // same block -> counter-copy map as the pass that counted the rows
     const size_t co = (size_t)(blockIdx.x & (NCOPY - 1)) * (nrow + 1);
     rowfill += co;
@@ -185,7 +186,7 @@ __global__ void k_place(const int32_t* __restrict__ keys, int64_t n, int nrow, i
     uint32_t row = 0xffffffffu;
     if (act) {
         const int32_t key = keys[t];
-        row = (key >= 0) ? (uint32_t)(key / na) : (uint32_t)nrow;
+        row = (key >= 0 && (!zone || zone[t] == zsel)) ? (uint32_t)(key / na) : (uint32_t)nrow;
     }
     const uint32_t am = __ballot_sync(0xffffffffu, act);
     const uint32_t peers = __match_any_sync(0xffffffffu, row) & am;
@@ -245,7 +246,8 @@ __global__ void __launch_bounds__(256) k_deposit(DevGeo g, const int32_t* __rest
 
 // mass[R][j] = pmass 2^-20 (sum over the base rows R, R-1, R-ngz, R-ngz-1)
 __global__ void k_mass_combine(DevGeo g, const int32_t* __restrict__ stage,
-                               const int32_t* __restrict__ rowitem, float* __restrict__ mass) {
+                               const int32_t* __restrict__ rowitem, float* __restrict__ mass,
+                               float pm) {
     const int na = g.na, nrow = g.nrow;
     const int NQ = (g.ndim == 3) ? 4 : 2;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -258,7 +260,7 @@ __global__ void k_mass_combine(DevGeo g, const int32_t* __restrict__ stage,
         if (B < 0) continue;
         for (int it = rowitem[B]; it < rowitem[B + 1]; it++) v += stage[((size_t)it * NQ + q) * na + j];
     }
-    mass[i] = (float)((double)v * (1.0 / (double)FIXQ)) * g.pmass;
+    mass[i] = (float)((double)v * (1.0 / (double)FIXQ)) * pm;
 }
 
 // cell keys and fractions of the stored particles, rows counted (masset)
@@ -281,7 +283,8 @@ __global__ void k_row_keys(DevGeo g, const float* __restrict__ P, int64_t cap, i
 }
 
 // rows counted by the caller's pass -> permutation, deposit, mass
-int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* perm_out) {
+int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* perm_out,
+                    const int32_t* zone, int zsel, float* mass_out, float pm) {
     const DevGeo& g = c->g;
     const int64_t n = c->n;
     int rc = gx_phase_mark(c, PH_SORT);
@@ -295,7 +298,8 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
     GX_LAUNCHED(c);
     if (n > 0) {
         k_place<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(keys, n, g.nrow, g.na, c->rowstart,
-                                                                  c->rowbase, c->rowfill, perm_out);
+                                                                  c->rowbase, c->rowfill, perm_out,
+                                                                  zone, zsel);
         GX_LAUNCHED(c);
     }
     rc = gx_phase_mark(c, PH_DEPOSIT);
@@ -313,8 +317,8 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
     rc = gx_phase_mark(c, PH_COMBINE);
     if (rc) return rc;
     const int64_t tot = (int64_t)g.nrow * g.na;
-    k_mass_combine<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(g, c->stage, c->rowitem,
-                                                                       c->mass);
+    k_mass_combine<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(
+        g, c->stage, c->rowitem, mass_out ? mass_out : c->mass, pm < 0.f ? g.pmass : pm);
     GX_LAUNCHED(c);
     return GX_OK;
 }

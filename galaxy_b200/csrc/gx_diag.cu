@@ -35,18 +35,39 @@ __device__ __forceinline__ void accel_parts(const DevGeo& g, const float4* __res
             if (g.ndim == 3) a[2] += fr * z;
         }
         phalo = 0.5f * g.halo_v2 * logf(1.f + r2 / g.halo_rc2);
+    } else if (g.halo == 2) {
+        gx_disc_force(g, x, y, z, a[0], a[1], a[2], phalo);
     }
+}
+
+// with time-step zones: the acceleration of a zone's own step
+// (getacc.f:141-150, x nstep^2); none off the grid.  Returns the zone's
+// step factor.
+__device__ __forceinline__ float zone_scale(const ZoneTab& zt, const int32_t* __restrict__ zone,
+                                            int64_t i, float* a, float& pg, float& ph) {
+    if (!zone) return 1.f;
+    const int iz = zone[i];
+    const float t = (float)zt.nstep[min(iz, zt.nz) - 1];
+    if (iz > zt.nz) {
+        a[0] = a[1] = a[2] = 0.f;
+        pg = ph = 0.f;
+    } else if (iz > 1) {
+        for (int d = 0; d < 3; d++) a[d] *= t * t;
+    }
+    return t;
 }
 
 // tmcgrp.f (RVLF): v <- v - fac * a, fac = +1/2 to start, -1/2 to undo
 __global__ void k_tmcent(DevGeo g, float* __restrict__ P, int64_t cap, int64_t n,
-                         const float4* __restrict__ F, float fac) {
+                         const float4* __restrict__ F, float fac, const int32_t* __restrict__ zone,
+                         ZoneTab zt) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int nd = g.ndim;
     float z = (nd == 3) ? P[2 * cap + i] : 0.f;
     float a[3], pg, ph;
     accel_parts(g, F, P[i], P[cap + i], z, a, pg, ph);
+    zone_scale(zt, zone, i, a, pg, ph);
     for (int d = 0; d < nd; d++) P[(nd + d) * cap + i] -= fac * a[d];
 }
 
@@ -55,7 +76,8 @@ __global__ void k_tmcent(DevGeo g, float* __restrict__ P, int64_t cap, int64_t n
 // a2_re, a2_im, mass, count
 #define NDSUM 8
 __global__ void k_icheck(DevGeo g, const float* __restrict__ P, int64_t cap, int64_t n,
-                         const float4* __restrict__ F, double pm, double* __restrict__ part) {
+                         const float4* __restrict__ F, double pm, double* __restrict__ part,
+                         const int32_t* __restrict__ zone, ZoneTab zt) {
     __shared__ double sh[NDSUM][256];
     double acc[NDSUM] = {0, 0, 0, 0, 0, 0, 0, 0};
     const int nd = g.ndim;
@@ -66,8 +88,13 @@ __global__ void k_icheck(DevGeo g, const float* __restrict__ P, int64_t cap, int
         accel_parts(g, F, x, y, z, a, pg, ph);
         CellW cw = gx_cell(g, x, y, z, true);
         if (cw.key < 0) continue;
+        // time-centred velocity in base-step units (cencds.f:26-35)
+        float az[3] = {a[0], a[1], a[2]};
+        const double t = zone_scale(zt, zone, i, az, pg, ph);
+        if (zone && zone[i] > zt.nz) a[0] = a[1] = a[2] = 0.f;
         double v[3], q[3] = {x, y, z};
-        for (int d = 0; d < nd; d++) v[d] = (double)P[(nd + d) * cap + i] + 0.5 * (double)a[d];
+        for (int d = 0; d < nd; d++)
+            v[d] = ((double)P[(nd + d) * cap + i] + 0.5 * (double)az[d]) / t;
         double ke = 0, vir = 0;
         for (int d = 0; d < nd; d++) {
             ke += v[d] * v[d];
@@ -120,8 +147,9 @@ extern "C" int gx_tmcent(GxCtx* c, int start) {
         k64_tmcent<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, c->p64, c->cap, n,
                                                                       c->acc64, (double)fac);
     } else {
-        k_tmcent<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, c->pbuf[c->cur], c->cap,
-                                                                    n, c->field, fac);
+        k_tmcent<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+            c->g, c->pbuf[c->cur], c->cap, n, c->field, fac,
+            c->nzones > 1 ? c->pzone[c->cur] : nullptr, c->zt);
     }
     GX_LAUNCHED(c);
     GX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -137,7 +165,8 @@ extern "C" int gx_icheck(GxCtx* c, GxDiag* d) {
     double* part = nullptr;
     GX_CUDA(c, cudaMallocAsync((void**)&part, sizeof(double) * NDSUM * nb, c->stream));
     k_icheck<<<nb, 256, 0, c->stream>>>(c->g, c->pbuf[c->cur], c->cap, c->n, c->field,
-                                        (double)c->cfg.pmass, part);
+                                        (double)c->cfg.pmass, part,
+                                        c->nzones > 1 ? c->pzone[c->cur] : nullptr, c->zt);
     GX_LAUNCHED(c);
     std::vector<double> h((size_t)NDSUM * nb);
     GX_CUDA(c, cudaMemcpyAsync(h.data(), part, sizeof(double) * NDSUM * nb, cudaMemcpyDeviceToHost,

@@ -307,6 +307,9 @@ __global__ void __launch_bounds__(1024) k_ens_step(EnsArgs A) {
                         ax += fr * x;
                         ay += fr * y;
                     }
+                } else if (g.halo == 2 && cw.key >= 0) {
+                    float az_ = 0.f, ph_ = 0.f;
+                    gx_disc_force(g, x, y, 0.f, ax, ay, az_, ph_);
                 }
                 // stpgrp.f:26-32
                 vx += ax;

@@ -302,6 +302,15 @@ __global__ void k64_gather(DevGeo g, const double* __restrict__ P, int64_t cap, 
                 if (nd == 3) a[2] += fr * z;
             }
             ph += 0.5 * g.halo_v2_d * log(1.0 + r2 / g.halo_rc2_d);
+        } else if (g.halo == 2) {
+            // fixed softened Kuz'min-Toomre disc force (frdisc.f:27-29)
+            const double d = x * x + y * y + ((nd == 3) ? z * z : 0.0) + g.halo_rc2_d;
+            const double sd = sqrt(d);
+            const double f = -g.halo_v2_d / (d * sd);
+            a[0] += f * x;
+            a[1] += f * y;
+            if (nd == 3) a[2] += f * z;
+            ph -= g.halo_v2_d / sd;
         }
     }
     for (int d = 0; d < nd; d++) acc[d * cap + i] = a[d];

@@ -520,6 +520,7 @@ extern "C" int gx_set_mass(GxCtx* c, const float* mass) {
             }
     c->jrs = jr;
     c->krs = kr;
+    c->zones_ready = false;  // the zone arrays no longer describe the mass
     int32_t jrk[2] = {jr, kr};
     GX_CUDA(c, cudaMemcpyAsync(c->jrk_d, jrk, sizeof jrk, cudaMemcpyHostToDevice, c->stream));
     if (c->fp64) {

@@ -22,44 +22,6 @@ __device__ __forceinline__ uint32_t row_of(const DevGeo& g, const CellW& c) {
     return (c.key >= 0) ? (uint32_t)gx_div_na(g, c.key, r) : (uint32_t)g.nrow;
 }
 
-// interpolated acceleration and potential of a particle at (x, y, z) whose
-// interpolation cell is cw: grdacc + halfrc
-__device__ __forceinline__ void gx_accel_cell(const DevGeo& g, const float4* __restrict__ F,
-                                              const CellW& cw, float x, float y, float z, float& ax,
-                                              float& ay, float& az, float& ph) {
-    ax = ay = az = ph = 0.f;
-    // particles off the grid feel no force (getacc.f:103-122 acts on the
-    // particles inside the grid)
-    if (cw.key < 0) return;
-    {
-        float w[8];
-        int ic[8];
-        gx_weights(g, cw, w);
-        const int nc = gx_corners(g, cw.key, ic);
-        for (int k = 0; k < nc; k++) {
-            if (ic[k] < 0) continue;
-            const float4 f = __ldg(F + ic[k]);
-            ax += f.x * w[k];
-            ay += f.y * w[k];
-            az += f.z * w[k];
-            ph += f.w * w[k];
-        }
-    }
-    if (g.halo == 1) {
-        // cored isothermal halo (frhalo.f:55-56): F(r) = -v^2 r / (r^2 + rc^2)
-        float r2 = x * x + y * y + ((g.ndim == 3) ? z * z : 0.f);
-        float rr = sqrtf(r2);
-        float fr = -g.halo_v2 * rr / (r2 + g.halo_rc2);
-        if (fr != 0.f) {
-            fr = fr / rr;
-            ax += fr * x;
-            ay += fr * y;
-            if (g.ndim == 3) az += fr * z;
-        }
-        ph += 0.5f * g.halo_v2 * logf(1.f + r2 / g.halo_rc2);
-    }
-}
-
 __device__ __forceinline__ void gx_accel(const DevGeo& g, const float4* __restrict__ F, float x,
                                          float y, float z, float& ax, float& ay, float& az,
                                          float& ph) {

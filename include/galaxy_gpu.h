@@ -75,6 +75,7 @@ extern "C" {
 #define GX_GREEN_POT        3
 
 #define GX_MAX_SKIP        16
+#define GX_MAX_ZONES        8   /* time-step zones (gx_set_zones)            */
 
 /* Grid and run parameters: the p2d/p3d cards of the reference
  * (SRC/lib15/p2dset.f:22-80, p3dset.f:22-101, filset.f:101-142) plus the
@@ -95,9 +96,15 @@ typedef struct GxConfig {
     float   softl;       /* softening length, grid units                      */
     int32_t tsoft;       /* GX_SOFT_*                                         */
     float   pmass;       /* particle mass in internal units (M lscale^3 ts^2) */
-    int32_t halo;        /* 0: none; 1: rigid cored isothermal halo (ISOT)    */
-    float   halo_v2;     /* ISOT asymptotic v^2 (M_h / r_c) in internal units */
-    float   halo_rc;     /* ISOT core radius, grid units                      */
+    int32_t halo;        /* rigid force on every particle on the grid: 0 none;
+                            1 cored isothermal halo (ISOT, frhalo.f:55-56);
+                            2 softened Kuz'min-Toomre disc, the analytic
+                            radial force of a run whose m = 0 harmonic is
+                            skipped (filset.f:3-5, axifrc.f, frdisc.f:27-29) */
+    float   halo_v2;     /* 1: asymptotic v^2 (M_h / r_c); 2: disc mass
+                            M lscale^3 ts^2; internal units                   */
+    float   halo_rc;     /* 1: core radius; 2: (1 + epsilon) rscale lscale;
+                            grid units                                        */
     int32_t precision;   /* GX_PREC_*                                         */
     int32_t flags;       /* GX_FLAG_*                                         */
     int32_t device;      /* CUDA device ordinal                               */
@@ -211,6 +218,27 @@ int gx_getacc(GxCtx* ctx, float* acc, float* pot);
  * requests potentials on the last step (analysis step).
  * SRC/lib15/step.f:135-290, SRC/progs/galaxy.f:107-148. */
 int gx_step(GxCtx* ctx, int nsteps, int phys);
+
+/* Multiple time-step zones (SRC/lib15/setrun.f:208-219, 770-790): zone i
+ * (1-based) holds the particles at radius >= zbr[i-1] (cylindrical in 2D,
+ * spherical in 3D; zbr[0] is ignored, zone 1 starts at the centre) and
+ * steps every nstep[i-1] base steps with that multiple of the base step
+ * (nstep[0] = 1, zbr ascending inside the grid, grid units).  Call before
+ * gx_loadup, which then gives every particle its zone (loadup.f:177-181,
+ * zoneno.f) and scales its velocity to its zone's step (adjvls.f); gx_unload
+ * undoes the scaling.  With more than one zone gx_step follows step.f: zone
+ * i moves at the steps divisible by nstep[i-1], accelerations scaled by
+ * nstep^2 (getacc.f:141-150), particles crossing a boundary change step
+ * (rezgrp.f, chstep.f) and particles leaving the grid move to the outer
+ * zone's step (addoff.f); each zone keeps its own mass array and the solve
+ * uses their linear interpolation in time (masscl.f:64-96, zoncmb.f:46-129),
+ * over the whole grid.  Mixed path; no compensated positions, ensembles,
+ * adjoint or guard zones.  nzones = 1 restores the single-zone step. */
+int gx_set_zones(GxCtx* ctx, int32_t nzones, const int32_t* nstep, const float* zbr);
+
+/* Zone of every particle in load order (1..nzones, nzones + 1 off the
+ * grid) and the step counter; zone may be NULL. */
+int gx_zone_info(GxCtx* ctx, int32_t* zone, int32_t* istep);
 
 /* tmcent: move velocities half a step back (start != 0) or forward using
  * the current fields.  SRC/lib15/tmcent.f:83-90, tmcgrp.f. */

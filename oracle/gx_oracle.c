@@ -164,6 +164,7 @@ int64_t ox_direct_size(const GxConfig* c) {
 #define POW pow
 #include "gx_oracle_tmpl.h"
 #include "gx_oracle_adj.h"
+#include "gx_oracle_zone.h"
 #undef R
 #undef S
 #undef MIRROR

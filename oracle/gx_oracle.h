@@ -81,6 +81,24 @@ int ox_adj_forward(const GxConfig* cfg, const double* G, int64_t n, double* pos,
 int ox_adj_gradient(const GxConfig* cfg, const double* G, int64_t n, const double* pos0,
                     int nsteps, double* grad, double* dtheta, double* J);
 
+/* multiple time-step zones of the p2d/p3d step in FP64 (gx_oracle_zone.h).
+ * Zone codes 1..nzones, nzones + 1 off the grid; zm, zo [nzones][mesh]. */
+typedef struct OxZones {
+    int32_t nzones;
+    int32_t nstep[GX_MAX_ZONES];
+    double zbr[GX_MAX_ZONES];      /* zbr[0] unused: zone 1 starts at the centre */
+    int32_t istep;
+    int32_t lstep[GX_MAX_ZONES][2];  /* step numbers of the older and newer arrays */
+    int32_t jrk[GX_MAX_ZONES][2];    /* 1-based ring range of each zone's mass */
+} OxZones;
+int ox_zone_setup(const GxConfig* cfg, OxZones* z, int64_t n, double* pos, int32_t* zone);
+int ox_zone_unscale(const GxConfig* cfg, const OxZones* z, int64_t n, double* pos,
+                    const int32_t* zone);
+int ox_zone_masset(const GxConfig* cfg, OxZones* z, int64_t n, const double* pos,
+                   const int32_t* zone, double* zm, double* zo, int32_t* jrk);
+int ox_zone_step(const GxConfig* cfg, OxZones* z, const double* G, int64_t n, double* pos,
+                 int32_t* zone, double* zm, double* zo, int32_t* jrk, int nsteps);
+
 /* icheck-style integrals in FP64 from FP64 particle records and potentials */
 int ox_icheck(const GxConfig* cfg, int64_t n, const double* pos,
               const double* acc, const double* pot, double pmass_phys,

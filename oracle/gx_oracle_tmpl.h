@@ -719,6 +719,19 @@ int F(ox_grdacc)(const GxConfig* c, int64_t n, const R* pos, const R* fields, in
                 if (phys)
                     ph = ph + (R)0.5 * g.halo_v2 * LOG((R)1 + rr * rr / (g.halo_rc * g.halo_rc));
             }
+            /* fixed axisymmetric force of a softened Kuz'min-Toomre disc
+             * (the 'skip 0' card: getacc.f:118-121, axifrc.f, frdisc.f:27-29):
+             * F(r) = -K r / (r^2 + Rs^2)^1.5, K = halo_v2, Rs = halo_rc;
+             * potential -K / sqrt(r^2 + Rs^2) */
+            if (g.halo == 2) {
+                R r2 = 0;
+                for (int i = 0; i < nd; i++) r2 = r2 + q[i] * q[i];
+                const R d = r2 + g.halo_rc * g.halo_rc;
+                const R sd = SQRT(d);
+                const R fr = -g.halo_v2 / (d * sd);
+                for (int i = 0; i < nd; i++) a[i] = a[i] + fr * q[i];
+                if (phys) ph = ph - g.halo_v2 / sd;
+            }
         }
         for (int i = 0; i < nd; i++) acc[p * nd + i] = a[i];
         if (pot) pot[p] = ph;

@@ -274,3 +274,63 @@ def adj_gradient(cfg, G, pos, nsteps):
     _chk(L.ox_adj_gradient(C.byref(cfg), _p(G), len(q), _p(q), int(nsteps), _p(grad), _p(dth),
                            _p(J)), "ox_adj_gradient")
     return float(J[0]), grad, dth
+
+
+class OxZones(C.Structure):
+    _fields_ = [("nzones", C.c_int32), ("nstep", C.c_int32 * 8), ("zbr", C.c_double * 8),
+                ("istep", C.c_int32), ("lstep", (C.c_int32 * 2) * 8),
+                ("jrk", (C.c_int32 * 2) * 8)]
+
+
+class ZoneRun:
+    """FP64 run with multiple time-step zones (gx_oracle_zone.h): loadup's
+    zone assignment and velocity scaling, masset, steps, unload.  pos holds
+    velocities in zone-step units between setup and records()."""
+
+    def __init__(self, cfg, G, pos, nstep, zbr):
+        L = lib()
+        for name, at in (("ox_zone_setup", [C.POINTER(GxConfig), C.POINTER(OxZones), C.c_int64,
+                                            C.c_void_p, C.c_void_p]),
+                         ("ox_zone_unscale", [C.POINTER(GxConfig), C.POINTER(OxZones),
+                                              C.c_int64, C.c_void_p, C.c_void_p]),
+                         ("ox_zone_masset", [C.POINTER(GxConfig), C.POINTER(OxZones), C.c_int64,
+                                             C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                             C.c_void_p]),
+                         ("ox_zone_step", [C.POINTER(GxConfig), C.POINTER(OxZones), C.c_void_p,
+                                           C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_int])):
+            getattr(L, name).argtypes = at
+        self.cfg = cfg
+        self.G = np.ascontiguousarray(G, np.float64)
+        self.z = OxZones()
+        self.z.nzones = len(nstep)
+        for i, (s, r) in enumerate(zip(nstep, zbr)):
+            self.z.nstep[i] = int(s)
+            self.z.zbr[i] = float(r)
+        self.pos = np.array(pos, np.float64, copy=True, order="C")
+        n = len(self.pos)
+        self.zone = np.zeros(n, np.int32)
+        g = geometry(cfg)
+        self.zm = np.zeros((len(nstep), g.mesh))
+        self.zo = np.zeros((len(nstep), g.mesh))
+        self.jrk = np.zeros(2, np.int32)
+        _chk(L.ox_zone_setup(C.byref(cfg), C.byref(self.z), n, _p(self.pos), _p(self.zone)),
+             "zone_setup")
+        _chk(L.ox_zone_masset(C.byref(cfg), C.byref(self.z), n, _p(self.pos), _p(self.zone),
+                              _p(self.zm), _p(self.zo), _p(self.jrk)), "zone_masset")
+
+    def step(self, nsteps):
+        _chk(lib().ox_zone_step(C.byref(self.cfg), C.byref(self.z), _p(self.G), len(self.pos),
+                                _p(self.pos), _p(self.zone), _p(self.zm), _p(self.zo),
+                                _p(self.jrk), int(nsteps)), "zone_step")
+
+    @property
+    def mass(self):
+        return self.zm[0]
+
+    def records(self):
+        """particle records with velocities in base-step units"""
+        q = self.pos.copy()
+        _chk(lib().ox_zone_unscale(C.byref(self.cfg), C.byref(self.z), len(q), _p(q),
+                                   _p(self.zone)), "zone_unscale")
+        return q

@@ -21,10 +21,14 @@ def gold():
 
 
 def cfg_run100(g):
-    # run100.dat: grid size 93 128, HASH 2, softl 3.67879 (Plummer), sectors 2
+    # run100.dat: grid size 93 128, HASH 2, softl 3.67879 (Plummer), sectors 2,
+    # 'skip 0': no m = 0 on the grid, the analytic force of the softened disc
+    # (mass 1, rstar = 1 + epsilon, epsilon = softl / lscale) instead
     gr = g["grid"]
+    L, ts = gr["lscale"], gr["ts"]
     return make_config(2, gr["nr"], gr["na"], ng=gr["hash"] + 1, nsect=gr["sectors"],
-                       rmap=GX_RMAP_STDPOL, softl=gr["softl"], tsoft=1)
+                       skip=(0,), rmap=GX_RMAP_STDPOL, softl=gr["softl"], tsoft=1, halo=2,
+                       halo_v2=L ** 3 * ts ** 2, halo_rc=(1.0 + gr["softl"] / L) * L)
 
 
 def test_pcs_reads_the_reference_layout(gold, tmp_path):
