@@ -18,7 +18,8 @@ from ._abi import (GxConfig, GxDiag, GxGeometry, make_config, GX_OK, GX_PREC_FP6
                    GX_PREC_MIXED, GX_RMAP_LOG, GX_RMAP_STDPOL, GX_SOFT_PLUMMER,
                    GX_SOFT_SPLINE, GX_GRID_MASS, GX_GRID_FR, GX_GRID_FT, GX_GRID_FZ,
                    GX_GRID_POT, GX_GRID_FX, GX_GRID_FY, GX_GREEN_FR, GX_GREEN_FT,
-                   GX_GREEN_FZ, GX_GREEN_POT, GX_FLAG_COMPENSATED)
+                   GX_GREEN_FZ, GX_GREEN_POT, GX_FLAG_COMPENSATED,
+                   GX_FLAG_QUADRATIC)
 
 __all__ = ["Galaxy", "GxError", "GxConfig", "GxDiag", "GxGeometry", "make_config", "lib",
            "LIB_PATH"]
@@ -199,7 +200,8 @@ class Galaxy:
         coords = np.ascontiguousarray(coords, dtype=np.float32)
         n = coords.shape[0]
         ncl = np.zeros(n, np.int32)
-        wt = np.zeros((n, 8), np.float32)
+        quad = self.ndim == 3 and (self.cfg.flags & GX_FLAG_QUADRATIC)
+        wt = np.zeros((n, 27 if quad else 8), np.float32)
         self._chk(self._L.gx_weight(self._h, _ptr(coords), n, int(old), _ptr(ncl), _ptr(wt)))
         return ncl, wt
 

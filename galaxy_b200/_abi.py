@@ -22,6 +22,7 @@ GX_PREC_MIXED = 0
 GX_PREC_FP64 = 1
 GX_PREC_MIXED_TC05 = 2
 GX_FLAG_COMPENSATED = 1
+GX_FLAG_QUADRATIC = 2
 
 GX_GRID_MASS = 0
 GX_GRID_FR = 1

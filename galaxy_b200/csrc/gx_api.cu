@@ -44,6 +44,10 @@ int setgrd(const GxConfig* c, GxGeometry* g, std::string& err) {
     if (c->halo > 0 && !(c->halo_rc > 0.f)) return err = "halo_rc must be positive", GX_ERR_ARG;
     if (c->precision != GX_PREC_MIXED && c->precision != GX_PREC_FP64)
         return err = "unknown precision", GX_ERR_ARG;
+    if ((c->flags & GX_FLAG_QUADRATIC) && c->ndim != 3)
+        return err = "quadratic interpolation is a p3d scheme", GX_ERR_ARG;
+    if ((c->flags & GX_FLAG_QUADRATIC) && c->precision == GX_PREC_FP64)
+        return err = "quadratic interpolation runs on the mixed path", GX_ERR_ARG;
     g->nr = c->nr;
     g->na = na;
     g->ngz = ngz;
@@ -110,6 +114,7 @@ void fill_devgeo(GxCtx* c) {
     d.t_scale = (float)((double)G.na / (2.0 * GX_PI));
     d.inv_na = 1.0f / (float)G.na;
     d.comp = (c->cfg.flags & GX_FLAG_COMPENSATED) ? 1 : 0;
+    d.quad = (c->cfg.ndim == 3 && (c->cfg.flags & GX_FLAG_QUADRATIC)) ? 1 : 0;
     d.halo_v2 = c->cfg.halo_v2;
     d.halo_rc2 = c->cfg.halo_rc * c->cfg.halo_rc;
     d.pmass = c->cfg.pmass;
@@ -395,7 +400,7 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     // deposit work items: every row once plus one per DEP_CH particles
     c->maxitems = c->g.nrow + 1 + (int)((cap + DEP_CH - 1) / DEP_CH);
     DALLOC(c, c->items, (size_t)3 * c->maxitems);
-    int nq = (c->g.ndim == 3) ? 4 : 2;
+    int nq = c->g.quad ? 9 : (c->g.ndim == 3) ? 4 : 2;
     DALLOC(c, c->stage, (size_t)c->maxitems * nq * c->g.na);
     return GX_OK;
 }

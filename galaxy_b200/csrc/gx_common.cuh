@@ -31,6 +31,7 @@ struct DevGeo {
     float t_scale;  // na / (2 pi) in FP32
     float inv_na;   // 1 / na (fast division of cell keys, gx_div_na)
     int comp;       // compensated positions: planes 2 ndim .. 3 ndim - 1 hold the low parts
+    int quad;       // 27-point quadratic interpolation (p3d jmass = 3)
     float halo_v2, halo_rc2;
     float pmass;
     // FP64 copies for the plain FP64 path
@@ -188,7 +189,7 @@ int gx_phase_end(GxCtx* c);
 
 struct CellW {
     int key;      // ncl - 1, or -1 when off the grid / in the hole
-    float du, dt, dz;
+    float du, dt, dz;  // fractions in the cell; quadratic: coord + 1/2 - index
 };
 
 __device__ __forceinline__ float gx_u_exact(const DevGeo& g, float rr) {
@@ -213,6 +214,30 @@ __device__ __forceinline__ bool gx_near_int(float v, float eps) {
     return (f < eps) || (f > 1.f - eps);
 }
 
+// quadratic (27-point) cell of p3d, jmass = 3 (weight.f:280-298): the
+// nearest node (ju, jz, jt) = int(coord + 1/2), ju in [1, nr - 2], jz in
+// [0, ngz - 2], jt = na wrapping to spoke 0 in the key; the fractions are
+// coord + 1/2 - index (outside [0, 1) where an index was clamped)
+__device__ __forceinline__ CellW gx_cell27(const DevGeo& g, float u, float t, float z, CellW c) {
+    const float uh = __fadd_rn(u, 0.5f), th = __fadd_rn(t, 0.5f);
+    int ju = (int)uh;
+    ju = min(max(ju, 1), g.nr - 2);
+    const int jt = (int)th;
+    float zz = (z + g.zm) * g.inv_dzg;
+    {
+        float eps = 4.0e-6f * ((float)g.ngz + 1.f);
+        if (gx_near_int(zz + 0.5f, eps)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
+    }
+    const float zh = __fadd_rn(zz, 0.5f);
+    int jz = (int)zh;
+    jz = min(max(jz, 0), g.ngz - 2);
+    c.du = uh - (float)ju;
+    c.dt = th - (float)jt;
+    c.dz = zh - (float)jz;
+    c.key = (ju * g.ngz + jz) * g.na + ((jt == g.na) ? 0 : jt);
+    return c;
+}
+
 // Cell of a particle; old != 0 for interpolation (no sector folding).
 __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, float z, bool old) {
     CellW c;
@@ -226,10 +251,12 @@ __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, floa
     float u;
     if (g.rmap == GX_RMAP_STDPOL) u = __logf(1.0f + rr) * g.inv_ua;
     else u = __logf(rr) * g.inv_ua + g.uoffs;
+    // the quadratic scheme truncates coord + 1/2: its boundaries sit at half-integers
+    const float sh = g.quad ? 0.5f : 0.f;
     {
         // __logf: 2^-21.41 absolute error on [0.5, 2], 3 ulp elsewhere
         float eps = 5.0e-7f * g.inv_ua + 2.0e-6f * (fabsf(u) + fabsf(g.uoffs) + 1.0f);
-        if (gx_near_int(u, eps) || u < eps) u = gx_u_exact(g, rr);
+        if (gx_near_int(u + sh, eps) || u < eps) u = gx_u_exact(g, rr);
     }
     // t
     float t;
@@ -237,11 +264,12 @@ __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, floa
         t = atan2f(y, x) * g.t_scale;
         if (t < 0.f) t += (float)g.na;
         float eps = 4.0e-6f * (float)(g.na + 1);
-        if (gx_near_int(t, eps) || t < eps || t > (float)g.na - eps) t = gx_t_exact(g, x, y);
+        if (gx_near_int(t + sh, eps) || t < eps || t > (float)g.na - eps) t = gx_t_exact(g, x, y);
     } else {
         t = 0.f;
     }
     if (!old && g.nsect > 1) t = fmodf(t, g.thmax);
+    if (g.quad) return gx_cell27(g, u, t, z, c);
     int ju = (int)u;
     if (ju > g.nr - 2) ju = g.nr - 2;
     int jt = (int)t;
@@ -317,6 +345,47 @@ __device__ __forceinline__ int gx_div_na(const DevGeo& g, int v, int& r) {
 }
 
 // corner cells of a key (grdacc.f:193-202); -1 for cells past the mesh end
+// 27 quadratic weights (weight.f:299-311): per axis (1 - 2dd + dd^2,
+// 1 + 2dd - 2dd^2, dd^2); weight l = 9 k + 3 j + i (theta i fastest, then z
+// j, then u k) = 1/8 f_theta(i) f_z(j) f_u(k)
+__device__ __forceinline__ void gx_weights27(const CellW& c, float* w) {
+    float f[3][3];
+    const float d[3] = {c.dt, c.dz, c.du};
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const float dd = d[a], d2 = dd * dd;
+        f[a][0] = (1.f - 2.f * dd) + d2;
+        f[a][1] = (1.f + 2.f * dd) - 2.f * d2;
+        f[a][2] = d2;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int i = 0; i < 3; i++) w[9 * k + 3 * j + i] = 0.125f * f[0][i] * f[1][j] * f[2][k];
+}
+
+// the 27 nodes of a quadratic cell in weight order (massgn.f:180-193,
+// grdacc.f:271-283): theta wraps, planes and rings are flat offsets of
+// na and ngz na; nodes outside the mesh are -1
+__device__ __forceinline__ void gx_corners27(const DevGeo& g, int key, int* ic) {
+    const int na = g.na, pl = g.ngz * na;
+    int r;
+    const int row = gx_div_na(g, key, r);
+    const int base = row * na;
+    const int mid[3] = {base + ((r == 0) ? na - 1 : r - 1), key, base + ((r == na - 1) ? 0 : r + 1)};
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                const int v = mid[i] + (j - 1) * na + (k - 1) * pl;
+                ic[9 * k + 3 * j + i] = (v < 0 || v >= g.mesh) ? -1 : v;
+            }
+}
+
 __device__ __forceinline__ int gx_corners(const DevGeo& g, int key, int* ic) {
     const int na = g.na;
     int jt;
@@ -379,14 +448,30 @@ __device__ __forceinline__ void gx_disc_force(const DevGeo& g, float x, float y,
 
 // interpolated acceleration and potential of a particle at (x, y, z) whose
 // interpolation cell is cw: grdacc + halfrc (or the fixed disc force)
-__device__ __forceinline__ void gx_accel_cell(const DevGeo& g, const float4* __restrict__ F,
-                                              const CellW& cw, float x, float y, float z, float& ax,
-                                              float& ay, float& az, float& ph) {
+template <bool Q>
+__device__ __forceinline__ void gx_accel_cell_t(const DevGeo& g, const float4* __restrict__ F,
+                                                const CellW& cw, float x, float y, float z,
+                                                float& ax, float& ay, float& az, float& ph) {
     ax = ay = az = ph = 0.f;
     // particles off the grid feel no force (getacc.f:103-122 acts on the
     // particles inside the grid)
     if (cw.key < 0) return;
-    {
+    if constexpr (Q) {
+        // grdacc.f:267-299
+        float w[27];
+        int ic[27];
+        gx_weights27(cw, w);
+        gx_corners27(g, cw.key, ic);
+#pragma unroll
+        for (int k = 0; k < 27; k++) {
+            if (ic[k] < 0) continue;
+            const float4 f = __ldg(F + ic[k]);
+            ax += f.x * w[k];
+            ay += f.y * w[k];
+            az += f.z * w[k];
+            ph += f.w * w[k];
+        }
+    } else {
         float w[8];
         int ic[8];
         gx_weights(g, cw, w);
@@ -415,6 +500,13 @@ __device__ __forceinline__ void gx_accel_cell(const DevGeo& g, const float4* __r
     } else if (g.halo == 2) {
         gx_disc_force(g, x, y, z, ax, ay, az, ph);
     }
+}
+
+__device__ __forceinline__ void gx_accel_cell(const DevGeo& g, const float4* __restrict__ F,
+                                              const CellW& cw, float x, float y, float z, float& ax,
+                                              float& ay, float& az, float& ph) {
+    if (g.quad) gx_accel_cell_t<true>(g, F, cw, x, y, z, ax, ay, az, ph);
+    else gx_accel_cell_t<false>(g, F, cw, x, y, z, ax, ay, az, ph);
 }
 
 // ---------------------------------------------------------------------------

@@ -90,7 +90,7 @@ __global__ void __launch_bounds__(ROW_TILE) k_row_reduce(int nrow, uint32_t* __r
 
 // row totals -> row starts, deposit work items, active ring range; one
 // block per tile of ROW_TILE rows, the carry-in from the tile sums
-__global__ void __launch_bounds__(ROW_TILE) k_row_scan(int nrow, int ngz, int nr,
+__global__ void __launch_bounds__(ROW_TILE) k_row_scan(int nrow, int ngz, int nr, int quad,
                                                        const uint32_t* __restrict__ rowcnt,
                                                        const int32_t* __restrict__ tile,
                                                        int32_t* __restrict__ rowstart,
@@ -163,7 +163,8 @@ __global__ void __launch_bounds__(ROW_TILE) k_row_scan(int nrow, int ngz, int nr
         }
         // 1-based ring range as massgn tracks it (jrad = j + 1, krad = j + 2)
         if (rmax >= 0) {
-            jrk[0] = rmin / ngz + 1;
+            // (quadratic: jrad = ju, the ring below the central one, massgn.f:180)
+            jrk[0] = rmin / ngz + (quad ? 0 : 1);
             jrk[1] = min(rmax / ngz + 2, nr);
         } else {
             jrk[0] = nr;
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(256) k_deposit(DevGeo g, const int32_t* __rest
                                                  int32_t* __restrict__ errword) {
     extern __shared__ __align__(16) int32_t bins[];  // [NW][na]
     const int na = g.na;
-    constexpr int NQ = NW / 2;
+    constexpr int NQ = (NW == 27) ? 9 : NW / 2;
     const int nit = *nitems;
     for (int item = blockIdx.x; item < nit; item += gridDim.x) {
         const int row = items[3 * item], s0 = items[3 * item + 1], s1 = items[3 * item + 2];
@@ -221,24 +222,36 @@ __global__ void __launch_bounds__(256) k_deposit(DevGeo g, const int32_t* __rest
             cw.key = keys[p];
             cw.du = fr[p];
             cw.dt = fr[cap + p];
-            cw.dz = (NW == 8) ? fr[2 * cap + p] : 0.f;
+            cw.dz = (NW >= 8) ? fr[2 * cap + p] : 0.f;
             if (cw.key < 0 || cw.key / na != row) {
                 atomicExch(errword, 1);
                 continue;
             }
             const int jt = cw.key - row * na;
-            float w[8];
-            gx_weights(g, cw, w);
+            float w[NW == 27 ? 27 : 8];
+            if constexpr (NW == 27) gx_weights27(cw, w);
+            else gx_weights(g, cw, w);
 #pragma unroll
             for (int k = 0; k < NW; k++) atomicAdd(&bins[k * na + jt], __float2int_rn(w[k] * FIXQ));
         }
         __syncthreads();
-        // output row q gets the lo weight at j and the hi weight from j - 1
         int32_t* dst = stage + (size_t)item * NQ * na;
-        for (int i = threadIdx.x; i < NQ * na; i += blockDim.x) {
-            const int q = i / na, j = i - q * na;
-            const int jm = (j == 0) ? na - 1 : j - 1;
-            dst[i] = bins[(2 * q) * na + j] + bins[(2 * q + 1) * na + jm];
+        if constexpr (NW == 27) {
+            // output row q = 3 (u offset + 1) + (z offset + 1) gets the theta
+            // weight i of the particles whose central spoke is j + 1 - i
+            for (int i = threadIdx.x; i < NQ * na; i += blockDim.x) {
+                const int q = i / na, j = i - q * na;
+                const int jp = (j == na - 1) ? 0 : j + 1, jm = (j == 0) ? na - 1 : j - 1;
+                dst[i] = bins[(3 * q) * na + jp] + bins[(3 * q + 1) * na + j] +
+                         bins[(3 * q + 2) * na + jm];
+            }
+        } else {
+            // output row q gets the lo weight at j and the hi weight from j - 1
+            for (int i = threadIdx.x; i < NQ * na; i += blockDim.x) {
+                const int q = i / na, j = i - q * na;
+                const int jm = (j == 0) ? na - 1 : j - 1;
+                dst[i] = bins[(2 * q) * na + j] + bins[(2 * q + 1) * na + jm];
+            }
         }
         __syncthreads();
     }
@@ -249,15 +262,18 @@ __global__ void k_mass_combine(DevGeo g, const int32_t* __restrict__ stage,
                                const int32_t* __restrict__ rowitem, float* __restrict__ mass,
                                float pm) {
     const int na = g.na, nrow = g.nrow;
-    const int NQ = (g.ndim == 3) ? 4 : 2;
+    const int NQ = g.quad ? 9 : (g.ndim == 3) ? 4 : 2;
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= (int64_t)nrow * na) return;
     const int R = (int)(i / na), j = (int)(i - (int64_t)R * na);
-    const int off[4] = {0, 1, g.ngz, g.ngz + 1};
+    // row offset of output row q from its base row: linear (same, plane
+    // above, ring above, both); quadratic (u - 1 .. u + 1) x (z - 1 .. z + 1)
+    const int offl[4] = {0, 1, g.ngz, g.ngz + 1};
     long long v = 0;
     for (int q = 0; q < NQ; q++) {
-        const int B = R - off[q];
-        if (B < 0) continue;
+        const int off = g.quad ? (q / 3 - 1) * g.ngz + (q % 3 - 1) : offl[q];
+        const int B = R - off;
+        if (B < 0 || B >= nrow) continue;
         for (int it = rowitem[B]; it < rowitem[B + 1]; it++) v += stage[((size_t)it * NQ + q) * na + j];
     }
     mass[i] = (float)((double)v * (1.0 / (double)FIXQ)) * pm;
@@ -293,7 +309,7 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
     k_row_reduce<<<ntile, ROW_TILE, 0, c->stream>>>(g.nrow, c->rowcnt, c->rowfill, c->rowbase, c->rowtot,
                                                      c->rowtile);
     GX_LAUNCHED(c);
-    k_row_scan<<<ntile, ROW_TILE, 0, c->stream>>>(g.nrow, g.ngz, g.nr, c->rowtot, c->rowtile, c->rowstart,
+    k_row_scan<<<ntile, ROW_TILE, 0, c->stream>>>(g.nrow, g.ngz, g.nr, g.quad, c->rowtot, c->rowtile, c->rowstart,
                                                    c->rowitem, c->items, c->nitems_d, c->jrk_d);
     GX_LAUNCHED(c);
     if (n > 0) {
@@ -304,10 +320,19 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
     }
     rc = gx_phase_mark(c, PH_DEPOSIT);
     if (rc) return rc;
-    const int nw = (g.ndim == 3) ? 8 : 4;
+    const int nw = g.quad ? 27 : (g.ndim == 3) ? 8 : 4;
     const size_t sm = sizeof(int32_t) * (size_t)nw * g.na;
     const int grid = std::min(c->maxitems, 148 * 16);
-    if (nw == 8)
+    if (nw == 27) {
+        static bool attr = false;  // 27 x 512 spokes of bins exceed the default 48 KB
+        if (!attr) {
+            GX_CUDA(c, cudaFuncSetAttribute(k_deposit<27>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)(sizeof(int32_t) * 27 * 512)));
+            attr = true;
+        }
+        k_deposit<27><<<grid, 256, sm, c->stream>>>(g, c->items, c->nitems_d, keys, fr, c->cap,
+                                                    perm_out, c->stage, c->errword);
+    } else if (nw == 8)
         k_deposit<8><<<grid, 256, sm, c->stream>>>(g, c->items, c->nitems_d, keys, fr, c->cap,
                                                    perm_out, c->stage, c->errword);
     else

@@ -12,10 +12,16 @@ __device__ __forceinline__ void accel_parts(const DevGeo& g, const float4* __res
     pgrid = phalo = 0.f;
     CellW cw = gx_cell(g, x, y, z, true);
     if (cw.key < 0) return;
-    float w[8];
-    int ic[8];
-    gx_weights(g, cw, w);
-    const int nc = gx_corners(g, cw.key, ic);
+    float w[27];
+    int ic[27];
+    int nc = 27;
+    if (g.quad) {
+        gx_weights27(cw, w);
+        gx_corners27(g, cw.key, ic);
+    } else {
+        gx_weights(g, cw, w);
+        nc = gx_corners(g, cw.key, ic);
+    }
     for (int k = 0; k < nc; k++) {
         if (ic[k] < 0) continue;
         const float4 f = F[ic[k]];

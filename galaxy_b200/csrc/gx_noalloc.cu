@@ -81,6 +81,8 @@ extern "C" int gx_massgn_noalloc(const GxConfig* cfg, const float* d_coords, int
         return na_fail(GX_ERR_ARG, "gx_massgn_noalloc: null argument");
     if (cfg->precision != GX_PREC_MIXED)
         return na_fail(GX_ERR_ARG, "gx_massgn_noalloc: mixed-precision cells only");
+    if (cfg->flags & GX_FLAG_QUADRATIC)
+        return na_fail(GX_ERR_ARG, "gx_massgn_noalloc: the linear scheme only");
     GxCtx tmp;
     tmp.cfg = *cfg;
     std::string err;

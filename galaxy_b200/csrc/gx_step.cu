@@ -33,6 +33,7 @@ __device__ __forceinline__ void gx_accel(const DevGeo& g, const float4* __restri
 // current position is the one the previous pass (or masset) stored; the
 // pass stores the cell of the new position for the deposit and the next
 // step, and counts the new rows for the deposit's counting sort.
+template <bool Q>
 __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict__ Pin,
                                               float* __restrict__ Pout, int64_t cap, int64_t n,
                                               const int32_t* __restrict__ perm,
@@ -73,7 +74,7 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
             cw.dz = d3 ? fr_in[2 * cap + p] : 0.f;
         }
         float ax, ay, az, ph;
-        gx_accel_cell(g, F, cw, x, y, z, ax, ay, az, ph);
+        gx_accel_cell_t<Q>(g, F, cw, x, y, z, ax, ay, az, ph);
         vx += ax;
         vy += ay;
         if (d3) vz += az;
@@ -167,7 +168,8 @@ int gx_mixed_step(GxCtx* c, int nsteps, int phys) {
         rc = gx_phase_mark(c, PH_PUSH);
         if (rc) return rc;
         if (n > 0) {
-            k_push<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
+            auto kp = g.quad ? k_push<true> : k_push<false>;
+            kp<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
                 g, c->pbuf[c->cur], c->pbuf[nxt], c->cap, n, c->perm, c->origin, c->origin_tmp,
                 c->field, c->pkey[c->cur], c->pfr[c->cur], c->pkey[nxt], c->pfr[nxt], c->rowcnt,
                 (phys && last) ? c->ppot : nullptr);
@@ -208,13 +210,17 @@ __global__ void k_weight_aos(DevGeo g, const float* __restrict__ aos, int64_t n,
                              int32_t* __restrict__ ncl, float* __restrict__ wt) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const int nw = 2 * g.ndim;
+    const int nw = 2 * g.ndim, nwt = g.quad ? 27 : 8;
     const float* q = aos + i * nw;
     CellW c = gx_cell(g, q[0], q[1], (g.ndim == 3) ? q[2] : 0.f, old != 0);
-    float w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (c.key >= 0) gx_weights(g, c, w);
+    float w[27];
+    for (int k = 0; k < 27; k++) w[k] = 0.f;
+    if (c.key >= 0) {
+        if (g.quad) gx_weights27(c, w);
+        else gx_weights(g, c, w);
+    }
     ncl[i] = c.key;
-    for (int k = 0; k < 8; k++) wt[i * 8 + k] = w[k];
+    for (int k = 0; k < nwt; k++) wt[i * nwt + k] = w[k];
 }
 
 extern "C" int gx_weight(GxCtx* c, const float* coords, int64_t n, int old, int32_t* ncl, float* wt) {
@@ -226,13 +232,14 @@ extern "C" int gx_weight(GxCtx* c, const float* coords, int64_t n, int old, int3
     float *daos = nullptr, *dwt = nullptr;
     int32_t* dncl = nullptr;
     GX_CUDA(c, cudaMallocAsync((void**)&daos, sizeof(float) * nw * n, c->stream));
-    GX_CUDA(c, cudaMallocAsync((void**)&dwt, sizeof(float) * 8 * n, c->stream));
+    const int nwt = c->g.quad ? 27 : 8;
+    GX_CUDA(c, cudaMallocAsync((void**)&dwt, sizeof(float) * nwt * n, c->stream));
     GX_CUDA(c, cudaMallocAsync((void**)&dncl, sizeof(int32_t) * n, c->stream));
     GX_CUDA(c, cudaMemcpyAsync(daos, coords, sizeof(float) * nw * n, cudaMemcpyHostToDevice, c->stream));
     k_weight_aos<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, daos, n, old, dncl, dwt);
     GX_LAUNCHED(c);
     GX_CUDA(c, cudaMemcpyAsync(ncl, dncl, sizeof(int32_t) * n, cudaMemcpyDeviceToHost, c->stream));
-    GX_CUDA(c, cudaMemcpyAsync(wt, dwt, sizeof(float) * 8 * n, cudaMemcpyDeviceToHost, c->stream));
+    GX_CUDA(c, cudaMemcpyAsync(wt, dwt, sizeof(float) * nwt * n, cudaMemcpyDeviceToHost, c->stream));
     GX_CUDA(c, cudaFreeAsync(daos, c->stream));
     GX_CUDA(c, cudaFreeAsync(dwt, c->stream));
     GX_CUDA(c, cudaFreeAsync(dncl, c->stream));

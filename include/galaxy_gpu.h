@@ -57,6 +57,10 @@ extern "C" {
 
 /* flags */
 #define GX_FLAG_COMPENSATED 1   /* compensated (two-float) position update  */
+#define GX_FLAG_QUADRATIC   2   /* p3d 'inte 3': 27-point quadratic interpolation
+                                   (weight.f:251-314, massgn.f:173-202,
+                                   grdacc.f:267-299) instead of the 8-point one */
+#define GX_MAX_WEIGHTS     27   /* weights per particle of gx_weight          */
 
 /* grid arrays for gx_get_grid / gx_set_mass */
 #define GX_GRID_MASS        0   /* mass (after the pmass scaling)            */
@@ -180,8 +184,10 @@ int gx_loadup(GxCtx* ctx, const float* coords, int64_t n);
 
 /* weight: cell numbers (ncl - 1, or -1 off the grid / in the hole) and the
  * 4 (2D) or 8 (3D) interpolation weights, 8 floats per particle, of n AoS
- * particle records.  old != 0 selects the interpolation form (no sector
- * folding).  SRC/lib15/weight.f:61-101 (p2d), 196-250 (p3d). */
+ * particle records; with GX_FLAG_QUADRATIC the central node's number and
+ * 27 weights, 27 floats per particle.  old != 0 selects the interpolation
+ * form (no sector folding).  SRC/lib15/weight.f:61-101 (p2d), 196-250 (p3d
+ * linear), 251-314 (p3d quadratic). */
 int gx_weight(GxCtx* ctx, const float* coords, int64_t n, int old, int32_t* ncl, float* wt);
 
 /* dumpp (coordinates only): copy the particle records back out, in the

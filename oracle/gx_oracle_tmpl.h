@@ -14,6 +14,7 @@
 /* geometry in the working precision (SRC/lib15/setgrd.f:52-200) */
 typedef struct {
     int ndim, nr, na, ngz, nkz, ng, mmax, nsect, mesh, tsoft, rmap, halo;
+    int quad; /* 27-point quadratic interpolation (p3d jmass = 3) */
     R alpha, ua, uoffs, rinh, rgrid, zm, thmax, dzg, softl, softl2;
     R halo_v2, halo_rc;
     unsigned char lg[260];
@@ -35,6 +36,7 @@ static int F(og_init)(const GxConfig* c, F(og) * g) {
     g->tsoft = c->tsoft;
     g->rmap = c->rmap;
     g->halo = c->halo;
+    g->quad = (c->ndim == 3) && (c->flags & GX_FLAG_QUADRATIC);
     memcpy(g->lg, geo.lg, sizeof g->lg);
 #if MIRROR
     g->alpha = geo.alpha;
@@ -287,12 +289,46 @@ int F(ox_green)(const GxConfig* c, R* G, R* D) {
 }
 
 /* ------------------------------------------------------------------ */
+/* quadratic (27-point) weights of p3d, jmass = 3 (weight.f:280-311): the
+ * central cell is the nearest node, (ju, jz, jt) = int(u + .5, z + .5,
+ * t + .5), ju clamped to [1, nr - 2], jz to [0, ngz - 2], jt = na wrapping
+ * to 0 in the key; per axis dd = coord + .5 - index and the factors
+ * (1 - 2dd + dd^2, 1 + 2dd - 2dd^2, dd^2); weight l (theta fastest, then z,
+ * then u) = .125 f_theta f_z f_u.                                        */
+static int F(weight27)(const F(og) * gp, R u, R t, R z, int32_t* keyp, R* w) {
+    R zz = (z + gp->zm) / gp->dzg;
+    R uh = u + (R)0.5, th = t + (R)0.5, zh = zz + (R)0.5;
+    int ju = (int)uh;
+    if (ju > gp->nr - 2) ju = gp->nr - 2;
+    if (ju < 1) ju = 1;
+    int jt = (int)th;
+    int jz = (int)zh;
+    if (jz < 0) jz = 0;
+    if (jz > gp->ngz - 2) jz = gp->ngz - 2;
+    int ncl = (ju * gp->ngz + jz) * gp->na + jt;
+    if (jt == gp->na) ncl -= gp->na;
+    *keyp = ncl;
+    R dp[3][3];
+    for (int i = 0; i < 3; i++) {
+        R dd = (i == 0) ? th - (R)jt : (i == 1) ? zh - (R)jz : uh - (R)ju;
+        dp[i][0] = (R)1 - (R)2 * dd + dd * dd;
+        dp[i][1] = (R)1 + (R)2 * dd - (R)2 * (dd * dd);
+        dp[i][2] = dd * dd;
+    }
+    int l = 0;
+    for (int k = 0; k < 3; k++)
+        for (int j = 0; j < 3; j++)
+            for (int i = 0; i < 3; i++) w[l++] = (R)0.125 * dp[0][i] * dp[1][j] * dp[2][k];
+    return 1;
+}
+
+/* ------------------------------------------------------------------ */
 /* weight (SRC/lib15/weight.f:61-101 p2d, 196-250 p3d linear) together
  * with the off-grid test of offgrd.f:51-77.  key = ncl - 1 or -1.      */
 static int F(weight1)(const F(og) * gp, int old, const R* q, int32_t* keyp, R* w) {
     const int nd = gp->ndim;
     R x = q[0], y = q[1], z = (nd == 3) ? q[2] : (R)0;
-    for (int k = 0; k < 8; k++) w[k] = 0;
+    for (int k = 0; k < (gp->quad ? 27 : 8); k++) w[k] = 0;
     *keyp = -1;
     R rr = SQRT(x * x + y * y);
     if (rr > gp->rgrid) return 0;
@@ -311,6 +347,7 @@ static int F(weight1)(const F(og) * gp, int old, const R* q, int32_t* keyp, R* w
     }
     if (!old && gp->nsect > 1) t = FMOD(t, gp->thmax);
     if (rr < gp->rinh) return 0;
+    if (gp->quad) return F(weight27)(gp, u, t, z, keyp, w);
     int ju = (int)u;
     if (ju > gp->nr - 2) ju = gp->nr - 2;
     int jt = (int)t;
@@ -349,7 +386,8 @@ int F(ox_weight)(const GxConfig* c, int old, int64_t n, const R* pos, int32_t* k
     const int stride = 2 * g.ndim;
 #pragma omp parallel for schedule(static) num_threads(ox_threads) if (ox_threads > 1)
     for (int64_t p = 0; p < n; p++)
-        on[p] = (uint8_t)F(weight1)(&g, old, pos + p * stride, key + p, wt + p * 8);
+        on[p] = (uint8_t)F(weight1)(&g, old, pos + p * stride, key + p,
+                                     wt + p * (g.quad ? 27 : 8));
     return 0;
 }
 
@@ -358,6 +396,22 @@ int F(ox_weight)(const GxConfig* c, int old, int64_t n, const R* pos, int32_t* k
  * are returned as -1.                                                   */
 static int F(corners)(const F(og) * g, int32_t key, int32_t* ic) {
     const int na = g->na;
+    if (g->quad) {
+        /* massgn.f:180-193 / grdacc.f:271-283: the 3 x 3 x 3 nodes around
+         * the central one, theta wrapping, planes and rings by flat offsets */
+        const int c0 = key, tm = (key % na == 0) ? key - 1 + na : key - 1;
+        const int tp = ((key + 1) % na == 0) ? key + 1 - na : key + 1;
+        const int mid[3] = {tm, c0, tp};
+        const int pl = g->ngz * na;
+        int l = 0;
+        for (int k = -1; k <= 1; k++)
+            for (int j = -1; j <= 1; j++)
+                for (int i = 0; i < 3; i++) {
+                    int v = mid[i] + j * na + k * pl;
+                    ic[l++] = (v < 0 || v >= g->mesh) ? -1 : v;
+                }
+        return 27;
+    }
     int end = ((key + 1) % na) == 0;
     ic[0] = key;
     ic[1] = key + 1 - (end ? na : 0);
@@ -402,13 +456,21 @@ int F(ox_massgn)(const GxConfig* c, int64_t n, const int32_t* key, const R* wt,
         const int tid = OX_TID;
         R* dst = priv ? priv + (size_t)tid * g.mesh : mass;
         int64_t p0 = n * tid / nt, p1 = n * (tid + 1) / nt;
-        int32_t ic[8];
+        int32_t ic[27];
         for (int64_t p = p0; p < p1; p++) {
             if (!on[p]) continue;
             int j = key[p] / div;
-            if (j + 1 < jlo[tid]) jlo[tid] = j + 1;
+            /* quadratic: jrad = j (massgn.f:180) */
+            const int jl = g.quad ? j : j + 1;
+            if (jl < jlo[tid]) jlo[tid] = jl;
             if (j + 2 > khi[tid]) khi[tid] = j + 2;
             int nc = F(corners)(&g, key[p], ic);
+            if (g.quad) {
+                const R* w = wt + p * 27;
+                for (int k = 0; k < 27; k++)
+                    if (ic[k] >= 0) dst[ic[k]] += w[k];
+                continue;
+            }
             const R* w = wt + p * 8;
             const int* ord = (nc == 4) ? ord4 : ord8;
             for (int k = 0; k < nc; k++) {
@@ -439,7 +501,7 @@ int F(ox_masset)(const GxConfig* c, int64_t n, const R* pos, R* mass, int32_t* j
     F(og) g;
     if (F(og_init)(c, &g)) return GX_ERR_ARG;
     int32_t* key = (int32_t*)malloc(sizeof(int32_t) * (n ? n : 1));
-    R* wt = (R*)malloc(sizeof(R) * 8 * (n ? n : 1));
+    R* wt = (R*)malloc(sizeof(R) * 27 * (n ? n : 1));
     uint8_t* on = (uint8_t*)malloc(n ? n : 1);
     memset(mass, 0, sizeof(R) * g.mesh);
     jrk[0] = g.nr;
@@ -690,8 +752,8 @@ int F(ox_grdacc)(const GxConfig* c, int64_t n, const R* pos, const R* fields, in
         const R* q = pos + p * stride;
         R a[3] = {0, 0, 0}, ph = 0;
         int32_t key;
-        R w[8];
-        int32_t ic[8];
+        R w[27];
+        int32_t ic[27];
         int on = F(weight1)(&g, 1, q, &key, w);
         if (on) {
             int nc = F(corners)(&g, key, ic);

@@ -72,7 +72,7 @@ int ox_zone_setup(const GxConfig* c, OxZones* z, int64_t n, double* pos, int32_t
     for (int64_t p = 0; p < n; p++) {
         double* q = pos + p * st;
         int32_t key;
-        R w[8];
+        R w[27];
         if (!F(weight1)(&g, 1, q, &key, w)) {
             zone[p] = z->nzones + 1;
             continue;
@@ -156,7 +156,7 @@ static int F(zoncmb)(OxZones* z, int64_t mesh, R* zm, const R* zo, R pmass, int3
 static void F(zmassgn)(const GxConfig* c, OxZones* z, int mzone, int64_t n, const R* pos,
                        const int32_t* zone, const uint8_t* sel, int64_t mesh, R* zm) {
     int32_t* key = (int32_t*)malloc(sizeof(int32_t) * (n ? n : 1));
-    R* wt = (R*)malloc(sizeof(R) * 8 * (n ? n : 1));
+    R* wt = (R*)malloc(sizeof(R) * 27 * (n ? n : 1));
     uint8_t* on = (uint8_t*)malloc(n ? n : 1);
     uint8_t* onz = (uint8_t*)malloc(n ? n : 1);
     F(ox_weight)(c, 0, n, pos, key, wt, on);
@@ -211,7 +211,7 @@ int ox_zone_step(const GxConfig* c, OxZones* z, const double* G, int64_t n, doub
                 q[i] = q[i] + q[nd + i];
             }
             int32_t key;
-            R w[8];
+            R w[27];
             const int on = F(weight1)(&g, 1, q, &key, w);
             int iz = z0;
             if (z0 != off) {

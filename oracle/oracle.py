@@ -119,7 +119,7 @@ def weight(cfg, pos, old=False, prec=64):
     pos = np.ascontiguousarray(pos, dtype=dt)
     n = pos.shape[0]
     key = np.zeros(n, np.int32)
-    wt = np.zeros((n, 8), dt)
+    wt = np.zeros((n, 27 if (cfg.ndim == 3 and cfg.flags & 2) else 8), dt)
     on = np.zeros(n, np.uint8)
     _chk(getattr(lib(), "ox_weight_" + s)(C.byref(cfg), int(old), n, _p(pos), _p(key), _p(wt),
                                            _p(on)), "weight")
