@@ -240,6 +240,7 @@ def run_ours(args, w, rank, world, comm):
             gc.greenm()
             gc.loadup(rec)
             gc.masset()
+            gc.findf(False)
             gc.tmcent(True)
             gc.step(3)
             kc = 50

@@ -74,6 +74,7 @@ def lib():
         L.gx_adjoint.argtypes = [P, C.c_int, C.c_int, P, P, P, P]
         L.gx_set_zones.argtypes = [P, C.c_int32, P, P]
         L.gx_zone_info.argtypes = [P, P, P]
+        L.gx_danl.argtypes = [P, C.c_double, P]
         _lib = L
     return _lib
 
@@ -272,6 +273,16 @@ class Galaxy:
         d = GxDiag()
         self._chk(self._L.gx_icheck(self._h, C.byref(d)))
         return d
+
+    def danl(self, lscale, ts):
+        """Density harmonics of the grid rings (densty.f 'danl'):
+        complex array [nr][ng], m = 0 the ring's surface density sum over
+        spokes, m >= 1 the harmonic divided by it."""
+        g = self.geo
+        w = np.zeros(2 * g.ng * g.nr, np.float32)
+        self._chk(self._L.gx_danl(self._h, 1.0 / (lscale * ts * ts), _ptr(w)))
+        half = g.ng * g.nr
+        return (w[:half] + 1j * w[half:]).reshape(g.nr, g.ng)
 
     def last_step_ms(self):
         v = C.c_float()

@@ -191,3 +191,99 @@ extern "C" int gx_icheck(GxCtx* c, GxDiag* d) {
     d->n_on_grid = (int64_t)s[7];
     return GX_OK;
 }
+
+// ---------------------------------------------------------------------------
+// danl (densty.f:82-118, 190-250): the mass projected onto one plane, as a
+// surface density (ring i spans grofu(i - 1/2) .. grofu(i + 1/2), the first
+// from grofu(0)), Fourier-analysed ring by ring; per ring the m = 0 term
+// (the sum over spokes) and, for m = 1 .. ng - 1, the cosine and sine sums
+// over it (zero where the ring is empty or the m = 0 term is below 1e-6 of
+// them).  One block per ring, FP64 sums.
+template <typename T>
+__global__ void k_danl(DevGeo g, const T* __restrict__ mass, const float* __restrict__ cfac,
+                       float* __restrict__ w) {
+    extern __shared__ double sig[];  // [na]
+    __shared__ double red[2][32];
+    const int ir = blockIdx.x, na = g.na, ngz = (g.ndim == 3) ? g.ngz : 1, ng = g.ng;
+    const double c = (double)cfac[ir];
+    for (int j = threadIdx.x; j < na; j += blockDim.x) {
+        double s = 0.0;
+        for (int iz = 0; iz < ngz; iz++) s += (double)mass[((size_t)ir * ngz + iz) * na + j];
+        sig[j] = c * s;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    double c0 = 0.0;
+    for (int m = 0; m < ng; m++) {
+        double a = 0.0, b = 0.0;
+        for (int j = threadIdx.x; j < na; j += blockDim.x) {
+            const int mj = (int)(((int64_t)m * j) % na);
+            double sn, cs;
+            sincospi(2.0 * (double)mj / (double)na, &sn, &cs);
+            a += sig[j] * cs;
+            b += sig[j] * sn;
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+        }
+        if (lane == 0) {
+            red[0][warp] = a;
+            red[1][warp] = b;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            a = b = 0.0;
+            for (int k = 0; k < nwarp; k++) {
+                a += red[0][k];
+                b += red[1][k];
+            }
+            float re = 0.f, im = 0.f;
+            if (m == 0) {
+                c0 = a;
+                re = (float)a;
+            } else if (c0 > 0.0 && c0 > 1e-6 * fmax(fabs(a), fabs(b))) {
+                re = (float)(a / c0);
+                im = (float)(b / c0);
+            }
+            w[(size_t)ir * ng + m] = re;
+            w[(size_t)ng * g.nr + (size_t)ir * ng + m] = im;
+        }
+        __syncthreads();
+    }
+}
+
+extern "C" int gx_danl(GxCtx* c, double sigmaf, float* w) {
+    if (!c || !w || !(sigmaf > 0.0)) return GX_ERR_ARG;
+    if (!c->have_mass) return c->err = "no mass array (call gx_masset)", GX_ERR_STATE;
+    cudaSetDevice(c->dev);
+    const DevGeo& g = c->g;
+    // surface-density factor of every ring: sigmaf / area, area = alpha/2 (r2^2 - r1^2)
+    std::vector<float> cf(g.nr);
+    auto grofu = [&](float u) {
+        return (g.rmap == GX_RMAP_STDPOL) ? expf(g.ua * u) - 1.f : expf(g.ua * (u - g.uoffs));
+    };
+    float r1 = grofu(0.f);
+    for (int i = 0; i < g.nr; i++) {
+        const float r2 = grofu((float)(i + 1) - 0.5f);
+        const float area = 0.5f * g.alpha * (r2 * r2 - r1 * r1);
+        cf[i] = (float)(sigmaf / (double)area);
+        r1 = r2;
+    }
+    const size_t nw = (size_t)2 * g.ng * g.nr;
+    float *dc = nullptr, *dw = nullptr;
+    GX_CUDA(c, cudaMallocAsync((void**)&dc, sizeof(float) * g.nr, c->stream));
+    GX_CUDA(c, cudaMallocAsync((void**)&dw, sizeof(float) * nw, c->stream));
+    GX_CUDA(c, cudaMemcpyAsync(dc, cf.data(), sizeof(float) * g.nr, cudaMemcpyHostToDevice, c->stream));
+    const size_t sm = sizeof(double) * g.na;
+    if (c->fp64)
+        k_danl<double><<<g.nr, 128, sm, c->stream>>>(g, c->mass64, dc, dw);
+    else
+        k_danl<float><<<g.nr, 128, sm, c->stream>>>(g, c->mass, dc, dw);
+    GX_LAUNCHED(c);
+    GX_CUDA(c, cudaMemcpyAsync(w, dw, sizeof(float) * nw, cudaMemcpyDeviceToHost, c->stream));
+    GX_CUDA(c, cudaFreeAsync(dc, c->stream));
+    GX_CUDA(c, cudaFreeAsync(dw, c->stream));
+    GX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GX_OK;
+}

@@ -254,6 +254,16 @@ int gx_tmcent(GxCtx* ctx, int start);
  * SRC/lib15/icheck.f:61-92. */
 int gx_icheck(GxCtx* ctx, GxDiag* diag);
 
+/* danl: sectoral harmonics of the surface density on the grid rings, as
+ * densty.f:82-118, 190-250 writes them to the results file: the current
+ * mass projected onto one plane, divided by each ring's area (ring i spans
+ * grofu(i - 1/2) .. grofu(i + 1/2)) and scaled by sigmaf = 1 / (lscale ts^2);
+ * then per ring the m = 0 term (the sum over spokes) and, for
+ * m = 1 .. ng - 1, the cosine and sine sums divided by it.  w holds
+ * 2 ng nr floats: real parts [nr][ng] (m = 0: the sum), then imaginary
+ * parts [nr][ng] (m = 0: 0). */
+int gx_danl(GxCtx* ctx, double sigmaf, float* w);
+
 /* Device time of the last gx_step (ms, CUDA events on the context stream). */
 int gx_last_step_ms(const GxCtx* ctx, float* ms);
 

@@ -222,3 +222,53 @@ int ox_icheck(const GxConfig* c, int64_t n, const double* pos, const double* acc
     d->n_on_grid = n;
     return 0;
 }
+
+/* danl (SRC/lib15/densty.f:82-118, 190-250): surface density of the mass
+ * projected onto one plane (ring areas from FP32 grofu as the reference
+ * forms them), per ring the FFTPACK forward sums for m = 0 .. ng - 1
+ * (a_m = sum x cos, the sine sum sum x sin = -b_m), m >= 1 divided by the
+ * m = 0 term unless the ring is empty or that term is below 1e-6 of them.
+ * w: real parts [nr][ng] then imaginary parts [nr][ng].                   */
+int ox_danl(const GxConfig* c, const double* mass, double sigmaf, double* w) {
+    GxGeometry geo;
+    char err[256];
+    if (ox_geometry(c, &geo, err, sizeof err)) return GX_ERR_ARG;
+    const int nr = geo.nr, na = geo.na, ng = geo.ng, ngz = (c->ndim == 3) ? geo.ngz : 1;
+#define GROFU(u) ((c->rmap == GX_RMAP_STDPOL) ? expf(geo.ua * (u)) - 1.f \
+                                              : expf(geo.ua * ((u) - geo.uoffs)))
+    float r1 = GROFU(0.f);
+    double* sig = (double*)malloc(sizeof(double) * na);
+    for (int i = 0; i < nr; i++) {
+        const float r2 = GROFU((float)(i + 1) - 0.5f);
+        const float area = 0.5f * geo.alpha * (r2 * r2 - r1 * r1);
+        const double cf = (double)(float)(sigmaf / (double)area);
+        r1 = r2;
+        for (int j = 0; j < na; j++) {
+            double s = 0;
+            for (int iz = 0; iz < ngz; iz++) s += mass[((int64_t)i * ngz + iz) * na + j];
+            sig[j] = cf * s;
+        }
+        double c0 = 0;
+        for (int m = 0; m < ng; m++) {
+            double a = 0, b = 0;
+            for (int j = 0; j < na; j++) {
+                const double ph = 2.0 * OX_PI * (double)((int64_t)m * j % na) / (double)na;
+                a += sig[j] * cos(ph);
+                b += sig[j] * sin(ph);
+            }
+            double re = 0, im = 0;
+            if (m == 0) {
+                c0 = a;
+                re = a;
+            } else if (c0 > 0 && c0 > 1e-6 * fmax(fabs(a), fabs(b))) {
+                re = a / c0;
+                im = b / c0;
+            }
+            w[(int64_t)i * ng + m] = re;
+            w[(int64_t)ng * nr + (int64_t)i * ng + m] = im;
+        }
+    }
+#undef GROFU
+    free(sig);
+    return 0;
+}

@@ -99,6 +99,10 @@ int ox_zone_masset(const GxConfig* cfg, OxZones* z, int64_t n, const double* pos
 int ox_zone_step(const GxConfig* cfg, OxZones* z, const double* G, int64_t n, double* pos,
                  int32_t* zone, double* zm, double* zo, int32_t* jrk, int nsteps);
 
+/* danl density harmonics of the grid rings in FP64 (densty.f); w is
+ * 2 ng nr: real parts [nr][ng] then imaginary parts */
+int ox_danl(const GxConfig* cfg, const double* mass, double sigmaf, double* w);
+
 /* icheck-style integrals in FP64 from FP64 particle records and potentials */
 int ox_icheck(const GxConfig* cfg, int64_t n, const double* pos,
               const double* acc, const double* pot, double pmass_phys,

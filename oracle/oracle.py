@@ -334,3 +334,15 @@ class ZoneRun:
         _chk(lib().ox_zone_unscale(C.byref(self.cfg), C.byref(self.z), len(q), _p(q),
                                    _p(self.zone)), "zone_unscale")
         return q
+
+
+def danl(cfg, mass, lscale, ts):
+    """density harmonics [nr][ng] complex of a mass array (densty.f 'danl')"""
+    L = lib()
+    L.ox_danl.argtypes = [C.POINTER(GxConfig), C.c_void_p, C.c_double, C.c_void_p]
+    g = geometry(cfg)
+    m = np.ascontiguousarray(mass, np.float64)
+    w = np.zeros(2 * g.ng * g.nr)
+    _chk(L.ox_danl(C.byref(cfg), _p(m), 1.0 / (lscale * ts * ts), _p(w)), "danl")
+    half = g.ng * g.nr
+    return (w[:half] + 1j * w[half:]).reshape(g.nr, g.ng)
