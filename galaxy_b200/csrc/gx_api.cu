@@ -235,7 +235,7 @@ void gx_destroy(GxCtx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     gx_comm_destroy(c);
     void* ptrs[] = {c->green32, c->green64, c->pbuf[0], c->pbuf[1], c->perm, c->origin,
-                    c->origin_tmp, c->pkey[0], c->pkey[1], c->pfr[0], c->pfr[1], c->p64, c->key64, c->w64, c->acc64, c->ppot,
+                    c->origin_tmp, c->pkey[0], c->pkey[1], c->pfr, c->p64, c->key64, c->w64, c->acc64, c->ppot,
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
                     c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->perm_next, c->rowstart,
                     c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->rowtile, c->stage, c->jrk_d,
@@ -356,7 +356,7 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     if (n <= c->cap && c->cap > 0) return GX_OK;
     // grow: free old
     void* old[] = {c->pbuf[0], c->pbuf[1], c->perm, c->origin, c->origin_tmp, c->pkey[0], c->pkey[1],
-                   c->pfr[0], c->pfr[1], c->p64,
+                   c->pfr, c->p64,
                    c->key64, c->w64, c->acc64, c->ppot, c->pacc, c->perm_next, c->items, c->stage,
                    c->pzone[0], c->pzone[1]};
     for (void* p : old)
@@ -364,7 +364,7 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     c->pbuf[0] = c->pbuf[1] = nullptr;
     c->perm = c->origin = c->origin_tmp = nullptr;
     c->pkey[0] = c->pkey[1] = nullptr;
-    c->pfr[0] = c->pfr[1] = nullptr;
+    c->pfr = nullptr;
     c->pzone[0] = c->pzone[1] = nullptr;
     c->p64 = nullptr;
     c->key64 = nullptr;
@@ -394,8 +394,7 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     DALLOC(c, c->origin_tmp, cap);
     DALLOC(c, c->pkey[0], cap);
     DALLOC(c, c->pkey[1], cap);
-    DALLOC(c, c->pfr[0], 3 * cap);
-    DALLOC(c, c->pfr[1], 3 * cap);
+    DALLOC(c, c->pfr, 3 * cap);
     DALLOC(c, c->perm_next, cap);
     // deposit work items: every row once plus one per DEP_CH particles
     c->maxitems = c->g.nrow + 1 + (int)((cap + DEP_CH - 1) / DEP_CH);

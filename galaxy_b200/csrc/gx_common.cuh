@@ -81,8 +81,9 @@ struct GxCtx {
     int32_t* origin = nullptr;             // original load index of pbuf[cur][i]
     int32_t* origin_tmp = nullptr;
     int32_t* pkey[2] = {nullptr, nullptr}; // cell key (ncl - 1, -1 off the grid) of the particles of pbuf[i]
-    float* pfr[2] = {nullptr, nullptr};    // their cell fractions du, dt, dz: SoA [3][cap]
-    bool have_keys = false;                // pkey/pfr[cur] match pbuf[cur]
+    float* pfr = nullptr;                  // cell fractions du, dt, dz of pkey[cur], SoA [3][cap],
+                                           // written by the pass that keyed them for its deposit
+    bool have_keys = false;                // pkey[cur] matches pbuf[cur]
     double* p64 = nullptr;                 // SoA [2*ndim][cap] (FP64 path)
     int32_t* key64 = nullptr;
     double* w64 = nullptr;                 // [8][cap]
@@ -524,7 +525,8 @@ int gx_fp64_masset(GxCtx* c);
 int gx_fp64_findf(GxCtx* c, int lpot, bool polcat);
 int gx_fp64_getacc(GxCtx* c, float* acc, float* pot);
 int gx_fp64_step(GxCtx* c, int nsteps, int phys);
-// rows counted by the caller's pass -> permutation, deposit, mass.  With
+// rows counted by the caller's pass -> permutation, deposit (from the
+// keys and fractions the pass stored), mass.  With
 // zone set, only particles whose zone code is zsel are deposited (the
 // counting pass filtered the same way); the mass goes to mass_out
 // (default c->mass), scaled by pm (default pmass).

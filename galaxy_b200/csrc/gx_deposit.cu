@@ -27,60 +27,78 @@
 
 #define FIXQ 1048576.0f  // 2^20
 
-// block-wide sums / extremes of one value per thread (ROW_TILE threads)
-__device__ __forceinline__ void tile_reduce(int& a, int& b, int& lo, int& hi, int* sh) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// per row: total over the counter copies, each copy's offset in the row;
+// clears the counters for the next pass.  Per tile of ROW_TILE rows: the
+// particles, the deposit work items and the occupied row range.  A block
+// of 4 ROW_TILE threads takes one tile: thread (g, r) reads copies
+// 8g .. 8g + 7 of row r (coalesced over r), so that every thread issues
+// eight independent loads.
+#define RR_GROUPS 4
+static_assert(NCOPY % RR_GROUPS == 0, "copies split evenly over the groups");
+__global__ void __launch_bounds__(ROW_TILE * RR_GROUPS) k_row_reduce(
+    int nrow, uint32_t* __restrict__ rowcnt, uint32_t* __restrict__ rowfill,
+    uint32_t* __restrict__ rowbase, uint32_t* __restrict__ rowtot, int32_t* __restrict__ tile) {
+    constexpr int CPG = NCOPY / RR_GROUPS;  // copies per group
+    __shared__ uint32_t gsum[RR_GROUPS][ROW_TILE];
+    __shared__ int sh[4 * (ROW_TILE / 32)];
+    const int rl = threadIdx.x % ROW_TILE, grp = threadIdx.x / ROW_TILE;
+    const int r = blockIdx.x * ROW_TILE + rl;
+    const size_t st = (size_t)nrow + 1;
+    uint32_t v[CPG], run = 0;
+    if (r <= nrow) {
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, o);
-        b += __shfl_xor_sync(0xffffffffu, b, o);
-        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
-        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        for (int k = 0; k < CPG; k++) v[k] = rowcnt[(grp * CPG + k) * st + r];
+#pragma unroll
+        for (int k = 0; k < CPG; k++) run += v[k];
     }
-    if (lane == 0) {
-        sh[4 * warp] = a;
-        sh[4 * warp + 1] = b;
-        sh[4 * warp + 2] = lo;
-        sh[4 * warp + 3] = hi;
+    gsum[grp][rl] = run;
+    __syncthreads();
+    uint32_t base = 0, tot = 0;
+#pragma unroll
+    for (int q = 0; q < RR_GROUPS; q++) {
+        const uint32_t x = gsum[q][rl];
+        base += (q < grp) ? x : 0u;
+        tot += x;
+    }
+    if (r <= nrow) {
+#pragma unroll
+        for (int k = 0; k < CPG; k++) {
+            const size_t a = (grp * CPG + k) * st + r;
+            rowbase[a] = base;
+            base += v[k];
+            rowcnt[a] = 0;
+            rowfill[a] = 0;
+        }
+        if (grp == 0) rowtot[r] = tot;
+    }
+    if (grp == 0) {
+        // tile statistics over the first ROW_TILE threads (warps 0 .. 7)
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        int a = (r <= nrow) ? (int)tot : 0, b = (r < nrow) ? (int)((tot + DEP_CH - 1) / DEP_CH) : 0;
+        int lo = (r < nrow && tot > 0) ? r : 0x7fffffff, hi = (r < nrow && tot > 0) ? r : -1;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(0xffffffffu, a, o);
+            b += __shfl_xor_sync(0xffffffffu, b, o);
+            lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) {
+            sh[4 * warp] = a;
+            sh[4 * warp + 1] = b;
+            sh[4 * warp + 2] = lo;
+            sh[4 * warp + 3] = hi;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        for (int w = 1; w < nw; w++) {
+        int a = 0, b = 0, lo = 0x7fffffff, hi = -1;
+        for (int w = 0; w < ROW_TILE / 32; w++) {
             a += sh[4 * w];
             b += sh[4 * w + 1];
             lo = min(lo, sh[4 * w + 2]);
             hi = max(hi, sh[4 * w + 3]);
         }
-    }
-}
-
-// per row: total over the counter copies, each copy's offset in the row;
-// clears the counters for the next pass.  Per tile of ROW_TILE rows: the
-// particles, the deposit work items and the occupied row range.
-__global__ void __launch_bounds__(ROW_TILE) k_row_reduce(int nrow, uint32_t* __restrict__ rowcnt,
-                                                         uint32_t* __restrict__ rowfill,
-                                                         uint32_t* __restrict__ rowbase,
-                                                         uint32_t* __restrict__ rowtot,
-                                                         int32_t* __restrict__ tile) {
-    __shared__ int sh[4 * (ROW_TILE / 32)];
-    const int r = blockIdx.x * ROW_TILE + threadIdx.x;
-    const size_t st = (size_t)nrow + 1;
-    uint32_t run = 0;
-    if (r <= nrow) {
-#pragma unroll 8
-        for (int c = 0; c < NCOPY; c++) {
-            const uint32_t v = rowcnt[c * st + r];
-            rowbase[c * st + r] = run;
-            run += v;
-            rowcnt[c * st + r] = 0;
-            rowfill[c * st + r] = 0;
-        }
-        rowtot[r] = run;
-    }
-    int a = (int)run, b = (r < nrow) ? (int)((run + DEP_CH - 1) / DEP_CH) : 0;
-    int lo = (r < nrow && run > 0) ? r : 0x7fffffff, hi = (r < nrow && run > 0) ? r : -1;
-    tile_reduce(a, b, lo, hi, sh);
-    if (threadIdx.x == 0) {
         tile[4 * blockIdx.x] = a;
         tile[4 * blockIdx.x + 1] = b;
         tile[4 * blockIdx.x + 2] = lo;
@@ -152,23 +170,33 @@ __global__ void __launch_bounds__(ROW_TILE) k_row_scan(int nrow, int ngz, int nr
         }
     }
     if (r == nrow) {
-        // the off-grid row closes the arrays: totals and the active ring range
+        // the off-grid row closes the arrays
         rowstart[nrow + 1] = ea + cnt;
         *nitems = eb;
+    }
+    if (b == nrow / ROW_TILE && warp == 0) {
+        // the active ring range over all tiles, one warp
         const int ntile = nrow / ROW_TILE + 1;
         int rmin = 0x7fffffff, rmax = -1;
-        for (int t = 0; t < ntile; t++) {
+        for (int t = lane; t < ntile; t += 32) {
             rmin = min(rmin, tile[4 * t + 2]);
             rmax = max(rmax, tile[4 * t + 3]);
         }
-        // 1-based ring range as massgn tracks it (jrad = j + 1, krad = j + 2)
-        if (rmax >= 0) {
-            // (quadratic: jrad = ju, the ring below the central one, massgn.f:180)
-            jrk[0] = rmin / ngz + (quad ? 0 : 1);
-            jrk[1] = min(rmax / ngz + 2, nr);
-        } else {
-            jrk[0] = nr;
-            jrk[1] = 0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+            rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        }
+        // 1-based ring range as massgn tracks it (jrad = j + 1, krad = j + 2;
+        // quadratic: jrad = ju, the ring below the central one, massgn.f:180)
+        if (lane == 0) {
+            if (rmax >= 0) {
+                jrk[0] = rmin / ngz + (quad ? 0 : 1);
+                jrk[1] = min(rmax / ngz + 2, nr);
+            } else {
+                jrk[0] = nr;
+                jrk[1] = 0;
+            }
         }
     }
     (void)nw;
@@ -257,24 +285,54 @@ __global__ void __launch_bounds__(256) k_deposit(DevGeo g, const int32_t* __rest
     }
 }
 
-// mass[R][j] = pmass 2^-20 (sum over the base rows R, R-1, R-ngz, R-ngz-1)
-__global__ void k_mass_combine(DevGeo g, const int32_t* __restrict__ stage,
-                               const int32_t* __restrict__ rowitem, float* __restrict__ mass,
-                               float pm) {
+// mass[R][j] = pmass 2^-20 (sum over the base rows that feed row R: R,
+// R-1, R-ngz, R-ngz-1 for the linear scheme, R + 1 .. R - 1 - ngz for the
+// quadratic one).  The item ranges of all base rows are loaded first and
+// the first item of each in one batch, so that a thread waits on two
+// dependent loads rather than one chain per base row.
+template <int NQ>
+__global__ void __launch_bounds__(256) k_mass_combine(DevGeo g, const int32_t* __restrict__ stage,
+                                                      const int32_t* __restrict__ rowitem,
+                                                      float* __restrict__ mass, float pm) {
     const int na = g.na, nrow = g.nrow;
-    const int NQ = g.quad ? 9 : (g.ndim == 3) ? 4 : 2;
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= (int64_t)nrow * na) return;
-    const int R = (int)(i / na), j = (int)(i - (int64_t)R * na);
-    // row offset of output row q from its base row: linear (same, plane
-    // above, ring above, both); quadratic (u - 1 .. u + 1) x (z - 1 .. z + 1)
-    const int offl[4] = {0, 1, g.ngz, g.ngz + 1};
-    long long v = 0;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;  // mesh < 2^24
+    if (i >= nrow * na) return;
+    int j;
+    const int R = gx_div_na(g, i, j);
+    int b0[NQ], b1[NQ];
+#pragma unroll
     for (int q = 0; q < NQ; q++) {
-        const int off = g.quad ? (q / 3 - 1) * g.ngz + (q % 3 - 1) : offl[q];
+        // row offset of output row q from its base row: linear (same, plane
+        // above, ring above, both); quadratic (u - 1 .. u + 1) x (z - 1 .. z + 1)
+        const int off = (NQ == 9) ? (q / 3 - 1) * g.ngz + (q % 3 - 1)
+                                  : ((q & 1) + ((q >> 1) ? g.ngz : 0));
         const int B = R - off;
-        if (B < 0 || B >= nrow) continue;
-        for (int it = rowitem[B]; it < rowitem[B + 1]; it++) v += stage[((size_t)it * NQ + q) * na + j];
+        const bool ok = B >= 0 && B < nrow;
+        b0[q] = ok ? __ldg(rowitem + B) : 0;
+        b1[q] = ok ? __ldg(rowitem + B + 1) : 0;
+    }
+    int first[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+        first[q] = (b0[q] < b1[q]) ? __ldg(stage + ((size_t)b0[q] * NQ + q) * na + j) : 0;
+    long long v = 0;
+#pragma unroll
+    for (int q = 0; q < NQ; q++) v += first[q];
+    // rows with more than DEP_CH particles have several items: sixteen
+    // loads in flight per thread (the densest rows of an evolved disc hold
+    // 100+ items)
+    for (int q = 0; q < NQ; q++) {
+        const int32_t* sp = stage + (size_t)q * na + j;
+        const size_t stride = (size_t)NQ * na;
+        int it = b0[q] + 1;
+        for (; it + 16 <= b1[q]; it += 16) {
+            int32_t x[16];
+#pragma unroll
+            for (int u = 0; u < 16; u++) x[u] = __ldg(sp + (size_t)(it + u) * stride);
+#pragma unroll
+            for (int u = 0; u < 16; u++) v += x[u];
+        }
+        for (; it < b1[q]; it++) v += __ldg(sp + (size_t)it * stride);
     }
     mass[i] = (float)((double)v * (1.0 / (double)FIXQ)) * pm;
 }
@@ -306,8 +364,8 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
     int rc = gx_phase_mark(c, PH_SORT);
     if (rc) return rc;
     const int ntile = (g.nrow + 1 + ROW_TILE - 1) / ROW_TILE;
-    k_row_reduce<<<ntile, ROW_TILE, 0, c->stream>>>(g.nrow, c->rowcnt, c->rowfill, c->rowbase, c->rowtot,
-                                                     c->rowtile);
+    k_row_reduce<<<ntile, ROW_TILE * RR_GROUPS, 0, c->stream>>>(g.nrow, c->rowcnt, c->rowfill, c->rowbase,
+                                                                 c->rowtot, c->rowtile);
     GX_LAUNCHED(c);
     k_row_scan<<<ntile, ROW_TILE, 0, c->stream>>>(g.nrow, g.ngz, g.nr, g.quad, c->rowtot, c->rowtile, c->rowstart,
                                                    c->rowitem, c->items, c->nitems_d, c->jrk_d);
@@ -342,7 +400,8 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
     rc = gx_phase_mark(c, PH_COMBINE);
     if (rc) return rc;
     const int64_t tot = (int64_t)g.nrow * g.na;
-    k_mass_combine<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(
+    auto kc = g.quad ? k_mass_combine<9> : (g.ndim == 3) ? k_mass_combine<4> : k_mass_combine<2>;
+    kc<<<(unsigned)((tot + 255) / 256), 256, 0, c->stream>>>(
         g, c->stage, c->rowitem, mass_out ? mass_out : c->mass, pm < 0.f ? g.pmass : pm);
     GX_LAUNCHED(c);
     return GX_OK;
@@ -353,10 +412,10 @@ int gx_mixed_masset(GxCtx* c) {
     const int64_t n = c->n;
     if (n > 0) {
         k_row_keys<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
-            g, c->pbuf[c->cur], c->cap, n, c->pkey[c->cur], c->pfr[c->cur], c->rowcnt);
+            g, c->pbuf[c->cur], c->cap, n, c->pkey[c->cur], c->pfr, c->rowcnt);
         GX_LAUNCHED(c);
     }
-    int rc = gx_deposit_rows(c, c->pkey[c->cur], c->pfr[c->cur], c->perm);
+    int rc = gx_deposit_rows(c, c->pkey[c->cur], c->pfr, c->perm);
     if (rc) return rc;
     c->have_keys = true;
     return gx_phase_end(c);

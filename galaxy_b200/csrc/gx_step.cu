@@ -6,11 +6,12 @@
 //                  gather of the float4 field at the 4/8 corners
 //                  (grdacc.f:40-84, 189-218), rigid halo (getacc.f:103-122,
 //                  frhalo.f:55-56), v += a, x += v (stpgrp.f:26-32), off-grid
-//                  test (offgrd.f:51-77), the new cell key and fractions
-//                  (stored for the deposit and the next step: the cell of
-//                  each position is computed once).  The pass also counts
-//                  the new rows for the deposit's counting sort
-//                  (gx_deposit.cu).
+//                  test (offgrd.f:51-77), the key and fractions of the new
+//                  cell for the deposit of the same step (whose rows the
+//                  pass also counts, gx_deposit.cu).  The interpolation
+//                  cell of the current position is recomputed from it
+//                  rather than stored from the previous step: the pass is
+//                  bound by memory traffic, not by that arithmetic.
 #include <algorithm>
 
 #include "gx_common.cuh"
@@ -29,10 +30,9 @@ __device__ __forceinline__ void gx_accel(const DevGeo& g, const float4* __restri
     gx_accel_cell(g, F, cw, x, y, z, ax, ay, az, ph);
 }
 
-// the fused particle pass of one step.  The interpolation cell of the
-// current position is the one the previous pass (or masset) stored; the
-// pass stores the cell of the new position for the deposit and the next
-// step, and counts the new rows for the deposit's counting sort.
+// the fused particle pass of one step: the interpolation cell of the
+// current position, the move, the key and fractions of the new cell,
+// counted by row for the deposit's counting sort.
 template <bool Q>
 __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict__ Pin,
                                               float* __restrict__ Pout, int64_t cap, int64_t n,
@@ -40,8 +40,6 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
                                               const int32_t* __restrict__ orig_in,
                                               int32_t* __restrict__ orig_out,
                                               const float4* __restrict__ F,
-                                              const int32_t* __restrict__ key_in,
-                                              const float* __restrict__ fr_in,
                                               int32_t* __restrict__ key_out,
                                               float* __restrict__ fr_out,
                                               uint32_t* __restrict__ rowcnt,
@@ -63,16 +61,7 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
             vy = Pin[3 * cap + p];
         }
         const int32_t o = orig_in[p];
-        CellW cw;
-        if (g.nsect > 1) {
-            // the stored cell is folded into the first sector; interpolation is not
-            cw = gx_cell(g, x, y, z, true);
-        } else {
-            cw.key = key_in[p];
-            cw.du = fr_in[p];
-            cw.dt = fr_in[cap + p];
-            cw.dz = d3 ? fr_in[2 * cap + p] : 0.f;
-        }
+        const CellW cw = gx_cell(g, x, y, z, true);
         float ax, ay, az, ph;
         gx_accel_cell_t<Q>(g, F, cw, x, y, z, ax, ay, az, ph);
         vx += ax;
@@ -136,30 +125,10 @@ __global__ void k_getacc(DevGeo g, const float* __restrict__ P, int64_t cap, int
     if (pot) pot[o] = ph;
 }
 
-// cell keys and fractions of the stored particles (when the mass array came
-// from gx_set_mass rather than a deposit of these particles)
-__global__ void k_cell_keys(DevGeo g, const float* __restrict__ P, int64_t cap, int64_t n,
-                            int32_t* __restrict__ keys, float* __restrict__ fr) {
-    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float z = (g.ndim == 3) ? P[2 * cap + i] : 0.f;
-    const CellW cw = gx_cell(g, P[i], P[cap + i], z, false);
-    keys[i] = cw.key;
-    fr[i] = cw.du;
-    fr[cap + i] = cw.dt;
-    if (g.ndim == 3) fr[2 * cap + i] = cw.dz;
-}
-
 // ---------------------------------------------------------------------------
 int gx_mixed_step(GxCtx* c, int nsteps, int phys) {
     const DevGeo& g = c->g;
     const int64_t n = c->n;
-    if (!c->have_keys && n > 0) {
-        k_cell_keys<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(g, c->pbuf[c->cur], c->cap, n,
-                                                                       c->pkey[c->cur], c->pfr[c->cur]);
-        GX_LAUNCHED(c);
-        c->have_keys = true;
-    }
     for (int s = 0; s < nsteps; s++) {
         const bool last = (s == nsteps - 1);
         int rc = gx_mixed_findf(c, phys && last, true);
@@ -171,7 +140,7 @@ int gx_mixed_step(GxCtx* c, int nsteps, int phys) {
             auto kp = g.quad ? k_push<true> : k_push<false>;
             kp<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
                 g, c->pbuf[c->cur], c->pbuf[nxt], c->cap, n, c->perm, c->origin, c->origin_tmp,
-                c->field, c->pkey[c->cur], c->pfr[c->cur], c->pkey[nxt], c->pfr[nxt], c->rowcnt,
+                c->field, c->pkey[nxt], c->pfr, c->rowcnt,
                 (phys && last) ? c->ppot : nullptr);
             GX_LAUNCHED(c);
         }
@@ -179,7 +148,7 @@ int gx_mixed_step(GxCtx* c, int nsteps, int phys) {
         c->cur = nxt;
         // the pass wrote particles in processing order; the new permutation
         // orders them by their new rows
-        rc = gx_deposit_rows(c, c->pkey[c->cur], c->pfr[c->cur], c->perm_next);
+        rc = gx_deposit_rows(c, c->pkey[c->cur], c->pfr, c->perm_next);
         if (rc) return rc;
         std::swap(c->perm, c->perm_next);
     }

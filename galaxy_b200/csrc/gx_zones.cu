@@ -130,8 +130,7 @@ __global__ void k_zone_rows(DevGeo g, const int32_t* __restrict__ keys,
 __global__ void __launch_bounds__(256) k_push_zone(
     DevGeo g, ZoneTab zt, int mzone, const float* __restrict__ Pin, float* __restrict__ Pout,
     int64_t cap, int64_t n, const int32_t* __restrict__ perm, const int32_t* __restrict__ orig_in,
-    int32_t* __restrict__ orig_out, const float4* __restrict__ F,
-    const int32_t* __restrict__ key_in, const float* __restrict__ fr_in,
+    int32_t* __restrict__ orig_out, const float4* __restrict__ F, const int32_t* __restrict__ key_in,
     int32_t* __restrict__ key_out, float* __restrict__ fr_out, const int32_t* __restrict__ zone_in,
     int32_t* __restrict__ zone_out, float* __restrict__ pot) {
     const int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -143,25 +142,16 @@ __global__ void __launch_bounds__(256) k_push_zone(
     const float z = (nd == 3) ? q[2] : 0.f;
     const int z0 = zone_in[p];
     orig_out[s] = orig_in[p];
-    CellW cw;
-    if (g.nsect > 1) {
-        cw = gx_cell(g, q[0], q[1], z, true);
-    } else {
-        cw.key = key_in[p];
-        cw.du = fr_in[p];
-        cw.dt = fr_in[cap + p];
-        cw.dz = (nd == 3) ? fr_in[2 * cap + p] : 0.f;
-    }
     const bool moves = z0 <= mzone || (z0 == off && mzone == nz);
     float a[3] = {0.f, 0.f, 0.f}, ph = 0.f;
-    if (z0 != off && (moves || pot)) gx_accel_cell(g, F, cw, q[0], q[1], z, a[0], a[1], a[2], ph);
+    if (z0 != off && (moves || pot)) {
+        const CellW cw = gx_cell(g, q[0], q[1], z, true);
+        gx_accel_cell(g, F, cw, q[0], q[1], z, a[0], a[1], a[2], ph);
+    }
     if (pot) pot[s] = ph;
     if (!moves) {
         for (int k = 0; k < nw; k++) Pout[k * cap + s] = q[k];
         key_out[s] = key_in[p];
-        fr_out[s] = fr_in[p];
-        fr_out[cap + s] = fr_in[cap + p];
-        if (nd == 3) fr_out[2 * cap + s] = fr_in[2 * cap + p];
         zone_out[s] = z0;
         return;
     }
@@ -196,6 +186,7 @@ __global__ void __launch_bounds__(256) k_push_zone(
         }
     }
     for (int k = 0; k < nw; k++) Pout[k * cap + s] = q[k];
+    // fractions for this step's deposit, which takes only particles that moved
     key_out[s] = cn.key;
     fr_out[s] = cn.du;
     fr_out[cap + s] = cn.dt;
@@ -266,7 +257,7 @@ static int zone_deposit(GxCtx* c, int mzone, int32_t* perm_out) {
                                                                            c->rowcnt);
             GX_LAUNCHED(c);
         }
-        int rc = gx_deposit_rows(c, keys, c->pfr[c->cur], perm_out, zone, k + 1,
+        int rc = gx_deposit_rows(c, keys, c->pfr, perm_out, zone, k + 1,
                                  k == 0 ? c->mass : c->znew[k], 1.f);
         if (rc) return rc;
         GX_CUDA(c, cudaMemcpyAsync(c->zjrk_d + 2 * k, c->jrk_d, 2 * sizeof(int32_t),
@@ -331,7 +322,7 @@ int gx_zone_masset(GxCtx* c) {
     const int64_t n = c->n;
     if (n > 0) {
         k_zone_keys<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
-            c->g, c->pbuf[c->cur], c->cap, n, c->pkey[c->cur], c->pfr[c->cur]);
+            c->g, c->pbuf[c->cur], c->cap, n, c->pkey[c->cur], c->pfr);
         GX_LAUNCHED(c);
     }
     zone_masscl(c, c->nzones, false);
@@ -359,8 +350,8 @@ int gx_zone_step(GxCtx* c, int nsteps, int phys) {
         if (n > 0) {
             k_push_zone<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
                 c->g, c->zt, mzone, c->pbuf[c->cur], c->pbuf[nxt], c->cap, n, c->perm, c->origin,
-                c->origin_tmp, c->field, c->pkey[c->cur], c->pfr[c->cur], c->pkey[nxt], c->pfr[nxt],
-                c->pzone[c->cur], c->pzone[nxt], (phys && last) ? c->ppot : nullptr);
+                c->origin_tmp, c->field, c->pkey[c->cur], c->pkey[nxt], c->pfr, c->pzone[c->cur],
+                c->pzone[nxt], (phys && last) ? c->ppot : nullptr);
             GX_LAUNCHED(c);
         }
         std::swap(c->origin, c->origin_tmp);
