@@ -113,6 +113,9 @@ void fill_devgeo(GxCtx* c) {
     d.inv_dzg = (d.ndim == 3) ? 1.0f / c->cfg.dzg : 0.f;
     d.t_scale = (float)((double)G.na / (2.0 * GX_PI));
     d.inv_na = 1.0f / (float)G.na;
+    d.fna = (float)G.na;
+    d.eps_t = 4.0e-6f * (float)(G.na + 1);
+    d.eps_z = 4.0e-6f * ((float)G.ngz + 1.f);
     d.comp = (c->cfg.flags & GX_FLAG_COMPENSATED) ? 1 : 0;
     d.quad = (c->cfg.ndim == 3 && (c->cfg.flags & GX_FLAG_QUADRATIC)) ? 1 : 0;
     d.halo_v2 = c->cfg.halo_v2;

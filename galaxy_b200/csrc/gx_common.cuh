@@ -30,6 +30,8 @@ struct DevGeo {
     float alpha, ua, inv_ua, uoffs, rinh, rgrid, zm, thmax, dzg, inv_dzg;
     float t_scale;  // na / (2 pi) in FP32
     float inv_na;   // 1 / na (fast division of cell keys, gx_div_na)
+    float fna;      // na, as a float
+    float eps_t, eps_z;  // guard bands of the spoke and plane coordinates (gx_cell)
     int comp;       // compensated positions: planes 2 ndim .. 3 ndim - 1 hold the low parts
     int quad;       // 27-point quadratic interpolation (p3d jmass = 3)
     float halo_v2, halo_rc2;
@@ -191,7 +193,23 @@ int gx_phase_end(GxCtx* c);
 struct CellW {
     int key;      // ncl - 1, or -1 when off the grid / in the hole
     float du, dt, dz;  // fractions in the cell; quadratic: coord + 1/2 - index
+    int row, jt;  // ring-plane row and spoke of key (set by gx_cell)
 };
+
+// floor of a float in [0, 2^23) and the exact fraction v - floor(v), on the
+// FMA and integer pipes: v + 2^23 rounded toward zero holds floor(v) in its
+// low mantissa bits (negative v count as 0: the fraction is then v itself,
+// as v - (int)v gives for the reference's truncation of -0 < v < 0)
+__device__ __forceinline__ int gx_trunc(float v, float& frac) {
+    const float t = __fadd_rz(fmaxf(v, 0.f), 8388608.0f);
+    frac = v - (t - 8388608.0f);
+    return __float_as_int(t) - 0x4B000000;
+}
+
+// (float)i for 0 <= i < 2^23, exact, without a conversion instruction
+__device__ __forceinline__ float gx_i2f(int i) {
+    return __int_as_float(0x4B000000 | i) - 8388608.0f;
+}
 
 __device__ __forceinline__ float gx_u_exact(const DevGeo& g, float rr) {
     if (g.rmap == GX_RMAP_STDPOL) {
@@ -211,7 +229,8 @@ __device__ __forceinline__ float gx_t_exact(const DevGeo& g, float x, float y) {
 }
 
 __device__ __forceinline__ bool gx_near_int(float v, float eps) {
-    float f = v - floorf(v);
+    float f;
+    gx_trunc(v, f);
     return (f < eps) || (f > 1.f - eps);
 }
 
@@ -221,21 +240,20 @@ __device__ __forceinline__ bool gx_near_int(float v, float eps) {
 // coord + 1/2 - index (outside [0, 1) where an index was clamped)
 __device__ __forceinline__ CellW gx_cell27(const DevGeo& g, float u, float t, float z, CellW c) {
     const float uh = __fadd_rn(u, 0.5f), th = __fadd_rn(t, 0.5f);
-    int ju = (int)uh;
+    float f;
+    int ju = gx_trunc(uh, f);
     ju = min(max(ju, 1), g.nr - 2);
-    const int jt = (int)th;
+    const int jt = gx_trunc(th, c.dt);
     float zz = (z + g.zm) * g.inv_dzg;
-    {
-        float eps = 4.0e-6f * ((float)g.ngz + 1.f);
-        if (gx_near_int(zz + 0.5f, eps)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
-    }
+    if (gx_near_int(zz + 0.5f, g.eps_z)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
     const float zh = __fadd_rn(zz, 0.5f);
-    int jz = (int)zh;
+    int jz = gx_trunc(zh, f);
     jz = min(max(jz, 0), g.ngz - 2);
-    c.du = uh - (float)ju;
-    c.dt = th - (float)jt;
-    c.dz = zh - (float)jz;
-    c.key = (ju * g.ngz + jz) * g.na + ((jt == g.na) ? 0 : jt);
+    c.du = uh - gx_i2f(ju);
+    c.dz = zh - gx_i2f(jz);
+    c.row = ju * g.ngz + jz;
+    c.jt = (jt == g.na) ? 0 : jt;
+    c.key = c.row * g.na + c.jt;
     return c;
 }
 
@@ -244,6 +262,7 @@ __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, floa
     CellW c;
     c.key = -1;
     c.du = c.dt = c.dz = 0.f;
+    c.row = c.jt = 0;
     float rr = __fsqrt_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)));
     if (rr > g.rgrid) return c;
     if (g.ndim == 3 && fabsf(z) > g.zm) return c;
@@ -263,32 +282,39 @@ __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, floa
     float t;
     if (g.ndim == 2 || rr > 0.f) {
         t = atan2f(y, x) * g.t_scale;
-        if (t < 0.f) t += (float)g.na;
-        float eps = 4.0e-6f * (float)(g.na + 1);
-        if (gx_near_int(t + sh, eps) || t < eps || t > (float)g.na - eps) t = gx_t_exact(g, x, y);
+        if (t < 0.f) t += g.fna;
+        const float eps = g.eps_t;
+        if (gx_near_int(t + sh, eps) || t < eps || t > g.fna - eps) t = gx_t_exact(g, x, y);
     } else {
         t = 0.f;
     }
     if (!old && g.nsect > 1) t = fmodf(t, g.thmax);
     if (g.quad) return gx_cell27(g, u, t, z, c);
-    int ju = (int)u;
-    if (ju > g.nr - 2) ju = g.nr - 2;
-    int jt = (int)t;
-    c.du = u - (float)ju;
-    c.dt = t - (float)jt;
+    int ju = gx_trunc(u, c.du);
+    if (ju > g.nr - 2) {
+        ju = g.nr - 2;
+        c.du = u - gx_i2f(ju);
+    }
+    const int jt = gx_trunc(t, c.dt);
     if (g.ndim == 2) {
-        c.key = ju * g.na + jt;
+        c.row = ju;
     } else {
         float zz = (z + g.zm) * g.inv_dzg;
-        {
-            float eps = 4.0e-6f * ((float)g.ngz + 1.f);
-            if (gx_near_int(zz, eps)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
+        if (gx_near_int(zz, g.eps_z)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
+        int jz = gx_trunc(zz, c.dz);
+        if (jz > g.ngz - 2) {
+            jz = g.ngz - 2;
+            c.dz = zz - gx_i2f(jz);
         }
-        int jz = (int)zz;
-        if (jz < 0) jz = 0;
-        if (jz > g.ngz - 2) jz = g.ngz - 2;
-        c.dz = zz - (float)jz;
-        c.key = (ju * g.ngz + jz) * g.na + jt;
+        c.row = ju * g.ngz + jz;
+    }
+    c.key = c.row * g.na + jt;
+    // a spoke coordinate that rounded up to na keys the next row's spoke 0,
+    // as the reference's flat cell number does; row and jt follow the key
+    c.jt = jt;
+    if (jt >= g.na) {
+        c.jt = jt - g.na;
+        c.row += 1;
     }
     return c;
 }
@@ -370,11 +396,9 @@ __device__ __forceinline__ void gx_weights27(const CellW& c, float* w) {
 // the 27 nodes of a quadratic cell in weight order (massgn.f:180-193,
 // grdacc.f:271-283): theta wraps, planes and rings are flat offsets of
 // na and ngz na; nodes outside the mesh are -1
-__device__ __forceinline__ void gx_corners27(const DevGeo& g, int key, int* ic) {
+__device__ __forceinline__ void gx_corners27(const DevGeo& g, int row, int r, int* ic) {
     const int na = g.na, pl = g.ngz * na;
-    int r;
-    const int row = gx_div_na(g, key, r);
-    const int base = row * na;
+    const int base = row * na, key = base + r;
     const int mid[3] = {base + ((r == 0) ? na - 1 : r - 1), key, base + ((r == na - 1) ? 0 : r + 1)};
 #pragma unroll
     for (int k = 0; k < 3; k++)
@@ -387,10 +411,8 @@ __device__ __forceinline__ void gx_corners27(const DevGeo& g, int key, int* ic) 
             }
 }
 
-__device__ __forceinline__ int gx_corners(const DevGeo& g, int key, int* ic) {
+__device__ __forceinline__ int gx_corners_rt(const DevGeo& g, int key, int jt, int* ic) {
     const int na = g.na;
-    int jt;
-    gx_div_na(g, key, jt);
     const int end = (jt == na - 1);
     ic[0] = key;
     ic[1] = key + 1 - (end ? na : 0);
@@ -411,6 +433,13 @@ __device__ __forceinline__ int gx_corners(const DevGeo& g, int key, int* ic) {
     for (int k = 0; k < 8; k++)
         if (ic[k] >= g.mesh) ic[k] = -1;
     return 8;
+}
+
+// the same from a key alone
+__device__ __forceinline__ int gx_corners(const DevGeo& g, int key, int* ic) {
+    int jt;
+    gx_div_na(g, key, jt);
+    return gx_corners_rt(g, key, jt, ic);
 }
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
@@ -462,7 +491,7 @@ __device__ __forceinline__ void gx_accel_cell_t(const DevGeo& g, const float4* _
         float w[27];
         int ic[27];
         gx_weights27(cw, w);
-        gx_corners27(g, cw.key, ic);
+        gx_corners27(g, cw.row, cw.jt, ic);
 #pragma unroll
         for (int k = 0; k < 27; k++) {
             if (ic[k] < 0) continue;
@@ -476,7 +505,7 @@ __device__ __forceinline__ void gx_accel_cell_t(const DevGeo& g, const float4* _
         float w[8];
         int ic[8];
         gx_weights(g, cw, w);
-        const int nc = gx_corners(g, cw.key, ic);
+        const int nc = gx_corners_rt(g, cw.key, cw.jt, ic);
         for (int k = 0; k < nc; k++) {
             if (ic[k] < 0) continue;
             const float4 f = __ldg(F + ic[k]);

@@ -17,7 +17,7 @@ __device__ __forceinline__ void accel_parts(const DevGeo& g, const float4* __res
     int nc = 27;
     if (g.quad) {
         gx_weights27(cw, w);
-        gx_corners27(g, cw.key, ic);
+        gx_corners27(g, cw.row, cw.jt, ic);
     } else {
         gx_weights(g, cw, w);
         nc = gx_corners(g, cw.key, ic);

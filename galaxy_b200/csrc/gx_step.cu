@@ -19,8 +19,7 @@
 // ---------------------------------------------------------------------------
 // row key of a cell (nrow for particles off the grid)
 __device__ __forceinline__ uint32_t row_of(const DevGeo& g, const CellW& c) {
-    int r;
-    return (c.key >= 0) ? (uint32_t)gx_div_na(g, c.key, r) : (uint32_t)g.nrow;
+    return (c.key >= 0) ? (uint32_t)c.row : (uint32_t)g.nrow;
 }
 
 __device__ __forceinline__ void gx_accel(const DevGeo& g, const float4* __restrict__ F, float x,
