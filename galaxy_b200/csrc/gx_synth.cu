@@ -21,12 +21,13 @@ struct ActList {
 };
 
 struct SynTab {
-    const float* WAe;  // [ru4(Z0)][KE]  wA(2i, z)
-    const float* WBe;  // [ru4(Z0)][KE]  wB(2i, z)
-    const float* WAo;  // [ru4(Z0)][KO]  wA(2i+1, z)
-    const float* WBo;  // [ru4(Z0)][KO]  wB(2i+1, z)
+    const float* WAe;  // [KE][ru4(Z0)]  wA(2i, z), the planes of one wavenumber contiguous
+    const float* WBe;  // [KE][ru4(Z0)]  wB(2i, z)
+    const float* WAo;  // [KO][ru4(Z0)]  wA(2i+1, z)
+    const float* WBo;  // [KO][ru4(Z0)]  wB(2i+1, z)
     const float* TC;   // [nact][njp]    cosine row weights (scaled)
     const float* TS;   // [nact][njp]    sine row weights (scaled)
+    const float* CS;   // [2][njp]       cos, sin of the spoke angles 2 pi j / na (polcat)
     int Z0, KE, KO, njp;
 };
 
@@ -52,19 +53,25 @@ __device__ __forceinline__ float wB(int k, int z, int ngz) {
 }
 
 __global__ void k_syntab(DevGeo g, ActList act, int nact, float scale, float* WAe, float* WBe,
-                         float* WAo, float* WBo, float* TC, float* TS, int Z0, int KE, int KO,
-                         int njp) {
+                         float* WAo, float* WBo, float* TC, float* TS, float* CS, int Z0, int KE,
+                         int KO, int njp) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nz = ru4s(Z0);
     if (tid < nz * KE) {
-        int z = tid / KE, i = tid - z * KE;
+        int i = tid / nz, z = tid - i * nz;
         WAe[tid] = (z < Z0) ? wA(2 * i, z, g.ngz) : 0.f;
         WBe[tid] = (z < Z0) ? wB(2 * i, z, g.ngz) : 0.f;
     }
     if (tid < nz * KO) {
-        int z = tid / KO, i = tid - z * KO;
+        int i = tid / nz, z = tid - i * nz;
         WAo[tid] = (z < Z0) ? wA(2 * i + 1, z, g.ngz) : 0.f;
         WBo[tid] = (z < Z0) ? wB(2 * i + 1, z, g.ngz) : 0.f;
+    }
+    if (tid < njp) {
+        float sn = 0.f, cs = 1.f;
+        if (tid <= g.na / 2) sincospif(2.0f * (float)tid / (float)g.na, &sn, &cs);
+        CS[tid] = cs;
+        CS[njp + tid] = sn;
     }
     if (tid < nact * njp) {
         int a = tid / njp, j = tid - a * njp;
@@ -118,13 +125,13 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
     float* Be = Ae + KE * ncp;
     float* Ao = Be + KE * ncp;          // [KO][ncp]
     float* Bo = Ao + KO * ncp;
-    for (int i = threadIdx.x; i < nz4 * KE; i += blockDim.x) {
-        sWAe[i] = tb.WAe[i];
-        sWBe[i] = tb.WBe[i];
-    }
-    for (int i = threadIdx.x; i < nz4 * KO; i += blockDim.x) {
-        sWAo[i] = tb.WAo[i];
-        sWBo[i] = tb.WBo[i];
+    // the four twiddle tables are one contiguous block of 2 nz4 (KE + KO)
+    // floats in global memory, in the order of the shared copies
+    {
+        const float4* src = reinterpret_cast<const float4*>(tb.WAe);
+        float4* dst = reinterpret_cast<float4*>(sWAe);
+        const int n4 = (2 * nz4 * (KE + KO)) >> 2;
+        for (int i = threadIdx.x; i < n4; i += blockDim.x) dst[i] = __ldg(src + i);
     }
     // spectrum of this ring: rows k, columns (a-row, b-row) of each harmonic
     for (int i = threadIdx.x; i < nkz * nact; i += blockDim.x) {
@@ -173,10 +180,11 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
 #pragma unroll 4
         for (int i = 0; i < kr; i++) {
             const float4 v = *reinterpret_cast<const float4*>(Sp + i * ncp + c0);
+            const float4 w4 = *reinterpret_cast<const float4*>(Wp + i * nz4 + z0);
+            const float w[4] = {w4.x, w4.y, w4.z, w4.w};
 #pragma unroll
             for (int r = 0; r < 4; r++) {
-                const float w = Wp[(z0 + r) * KR + i];
-                acc[r][0] += w * v.x; acc[r][1] += w * v.y; acc[r][2] += w * v.z; acc[r][3] += w * v.w;
+                acc[r][0] += w[r] * v.x; acc[r][1] += w[r] * v.y; acc[r][2] += w[r] * v.z; acc[r][3] += w[r] * v.w;
             }
         }
         float lo[4][4], hi[4][4];
@@ -215,7 +223,7 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
     }
 }
 
-#define SYN_ZB 8
+#define SYN_ZB 16
 // azimuthal synthesis + polcat, one CTA per (ring, SYN_ZB planes)
 __global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int tmask,
                                               const float* __restrict__ R, SynTab tb,
@@ -226,10 +234,14 @@ __global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int 
     const int nz = min(SYN_ZB, ngz - zb);
     float* TC = sm;                      // [nact][njp]
     float* TS = TC + nact * njp;
-    float* Rs = TS + nact * njp;         // [4][SYN_ZB][ncp]
-    for (int i = threadIdx.x; i < nact * njp; i += blockDim.x) {
-        TC[i] = tb.TC[i];
-        TS[i] = tb.TS[i];
+    float* CS = TS + nact * njp;         // [2][njp]
+    float* Rs = CS + 2 * njp;            // [4][SYN_ZB][ncp]
+    {
+        // TC, TS and CS are one contiguous block of 2 (nact + 1) njp floats
+        const float4* src = reinterpret_cast<const float4*>(tb.TC);
+        float4* dst = reinterpret_cast<float4*>(TC);
+        const int n4 = (2 * (nact + 1) * njp) >> 2;
+        for (int i = threadIdx.x; i < n4; i += blockDim.x) dst[i] = __ldg(src + i);
     }
     for (int i = threadIdx.x; i < 4 * SYN_ZB * ncp; i += blockDim.x) {
         const int t = i / (SYN_ZB * ncp), rem = i - t * SYN_ZB * ncp;
@@ -253,8 +265,8 @@ __global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int 
             const float4 ts = *reinterpret_cast<const float4*>(TS + a * njp + j0);
 #pragma unroll
             for (int t = 0; t < 4; t++) {
-                const float rc = Rs[(t * SYN_ZB + z) * ncp + 2 * a];
-                const float rs = Rs[(t * SYN_ZB + z) * ncp + 2 * a + 1];
+                const float2 r = *reinterpret_cast<const float2*>(Rs + (t * SYN_ZB + z) * ncp + 2 * a);
+                const float rc = r.x, rs = r.y;
                 C[t][0] += rc * tc.x; C[t][1] += rc * tc.y; C[t][2] += rc * tc.z; C[t][3] += rc * tc.w;
                 S[t][0] += rs * ts.x; S[t][1] += rs * ts.y; S[t][2] += rs * ts.z; S[t][3] += rs * ts.w;
             }
@@ -264,8 +276,7 @@ __global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int 
         for (int q = 0; q < 4; q++) {
             const int j = j0 + q;
             if (j > half) continue;
-            float sn, cs;
-            sincospif(2.0f * (float)j / (float)na, &sn, &cs);
+            const float cs = CS[j], sn = CS[njp + j];
             {
                 const float fr = C[0][q] + S[0][q], ft = C[1][q] + S[1][q];
                 const float fz = C[2][q] + S[2][q], ph = C[3][q] + S[3][q];
@@ -304,22 +315,22 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar) {
     const size_t nWe = (size_t)nz4 * KE, nWo = (size_t)nz4 * KO, nT = (size_t)nact * njp;
     if (!c->syntab) {
         if (nact > 64) return c->err = "more than 64 active harmonics", GX_ERR_RANGE;
-        const size_t tot = 2 * nWe + 2 * nWo + 2 * nT;
+        const size_t tot = 2 * nWe + 2 * nWo + 2 * nT + 2 * (size_t)njp;
         GX_CUDA(c, cudaMalloc((void**)&c->syntab, sizeof(float) * tot));
         ActList act;
         for (int a = 0; a < 64; a++) act.m[a] = a < nact ? c->spec.m[a] : 0;
         const float scale = (g.ndim == 3) ? 1.0f / (float)(2 * g.ngz * g.na) : 1.0f / (float)g.na;
         float* b = c->syntab;
-        const size_t mx = std::max(std::max(nWe, nWo), nT);
+        const size_t mx = std::max(std::max(nWe, nWo), std::max(nT, (size_t)njp));
         k_syntab<<<(unsigned)((mx + 255) / 256), 256, 0, c->stream>>>(
             g, act, nact, scale, b, b + nWe, b + 2 * nWe, b + 2 * nWe + nWo, b + 2 * nWe + 2 * nWo,
-            b + 2 * nWe + 2 * nWo + nT, Z0, KE, KO, njp);
+            b + 2 * nWe + 2 * nWo + nT, b + 2 * nWe + 2 * nWo + 2 * nT, Z0, KE, KO, njp);
         GX_LAUNCHED(c);
     }
     if (!c->synR) GX_CUDA(c, cudaMalloc((void**)&c->synR, sizeof(float) * 4 * g.nr * g.ngz * ncp));
     const float* b = c->syntab;
     SynTab tb{b, b + nWe, b + 2 * nWe, b + 2 * nWe + nWo, b + 2 * nWe + 2 * nWo,
-              b + 2 * nWe + 2 * nWo + nT, Z0, KE, KO, njp};
+              b + 2 * nWe + 2 * nWo + nT, b + 2 * nWe + 2 * nWo + 2 * nT, Z0, KE, KO, njp};
     {
         const size_t sm = sizeof(float) * (2 * nWe + 2 * nWo + (size_t)(KE + KO) * 2 * ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_synz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -328,7 +339,7 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar) {
         GX_LAUNCHED(c);
     }
     {
-        const size_t sm = sizeof(float) * (2 * nT + (size_t)4 * SYN_ZB * ncp);
+        const size_t sm = sizeof(float) * (2 * nT + 2 * (size_t)njp + (size_t)4 * SYN_ZB * ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_synaz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         dim3 grid(g.nr, (g.ngz + SYN_ZB - 1) / SYN_ZB);
         k_synaz<<<grid, 256, sm, c->stream>>>(g, nact, ncp, tmask, c->synR, tb, c->field, polar);
