@@ -163,12 +163,41 @@ __global__ void __launch_bounds__(288) k_fwd_az(DevGeo g, int ncp, const int32_t
     const int ldx = na + 1;
     float* X = sm;                 // [FWD_RB][na + 1]
     float* T = X + FWD_RB * ldx;   // [na][ncp]
-    for (int i = threadIdx.x; i < FWD_RB * na; i += blockDim.x) {
-        const int r = i / na, j = i - r * na;
-        X[r * ldx + j] = (r < nrows) ? mass[(size_t)(row0 + r) * na + j] : 0.f;
+    // several loads in flight per thread: the prologue is latency-bound
+    for (int b = threadIdx.x; b < FWD_RB * na; b += 4 * blockDim.x) {
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = b + u * blockDim.x, r = i / na;
+            v[u] = (i < FWD_RB * na && r < nrows) ? __ldg(mass + (size_t)row0 * na + i) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = b + u * blockDim.x;
+            if (i < FWD_RB * na) {
+                const int r = i / na, j = i - r * na;
+                X[r * ldx + j] = v[u];
+            }
+        }
     }
-    for (int i = threadIdx.x; i < na * ncp / 4; i += blockDim.x)
-        reinterpret_cast<float4*>(T)[i] = reinterpret_cast<const float4*>(Taz)[i];
+    {
+        const int n4 = na * ncp / 4;
+        const float4* src = reinterpret_cast<const float4*>(Taz);
+        float4* dst = reinterpret_cast<float4*>(T);
+        for (int b = threadIdx.x; b < n4; b += 8 * blockDim.x) {
+            float4 v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int i = b + u * blockDim.x;
+                if (i < n4) v[u] = __ldg(src + i);
+            }
+#pragma unroll
+            for (int u = 0; u < 8; u++) {
+                const int i = b + u * blockDim.x;
+                if (i < n4) dst[i] = v[u];
+            }
+        }
+    }
     __syncthreads();
     sgemm44_sk<4>(FWD_RB, ncp, na, X, ldx, T, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
 #pragma unroll

@@ -93,8 +93,17 @@ __global__ void k_syntab(DevGeo g, ActList act, int nact, float scale, float* WA
     }
 }
 
-// vertical synthesis, one CTA per (ring, field type); R[t][ir][z][ncp]
-#define SYNZ_THREADS 576
+// vertical synthesis, one CTA per (ring, field type); R[t][ir][z][ncp].
+// With P = EA + OB and Q = OA + EB (E/O: even/odd wavenumbers, A/B: the
+// two parts of the spectrum), plane z is P + Q and plane ngz - z is P - Q.
+// Each thread owns a 4 x 4 (plane, column) tile of P and Q; per wavenumber
+// pair it reads one float4 of each twiddle table (the planes of a
+// wavenumber are contiguous) and one float4 of each spectrum part, for 64
+// FMAs.  The four twiddle tables start on different shared-memory banks.
+#define SYNZ_THREADS 256
+__device__ __forceinline__ int synz_pad(int start, int want) {
+    return ((want - start) % 32 + 32) % 32;  // floats to add so that start lands on bank want
+}
 __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int ncp, int tmask,
                                              const float4* __restrict__ O, SynTab tb,
                                              float* __restrict__ R) {
@@ -117,33 +126,68 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
         return;
     }
     const int Z0 = tb.Z0, KE = tb.KE, KO = tb.KO, nz4 = ru4s(Z0);
+    const int tE = KE * nz4, tO = KO * nz4;
     float* sWAe = sm;
-    float* sWBe = sWAe + nz4 * KE;
-    float* sWAo = sWBe + nz4 * KE;
-    float* sWBo = sWAo + nz4 * KO;
-    float* Ae = sWBo + nz4 * KO;        // [KE][ncp]
+    float* sWBe = sWAe + tE;
+    sWBe += synz_pad((int)(sWBe - sm), 8);
+    float* sWAo = sWBe + tE;
+    sWAo += synz_pad((int)(sWAo - sm), 16);
+    float* sWBo = sWAo + tO;
+    sWBo += synz_pad((int)(sWBo - sm), 24);
+    float* Ae = sWBo + tO;              // [KE][ncp]
     float* Be = Ae + KE * ncp;
     float* Ao = Be + KE * ncp;          // [KO][ncp]
     float* Bo = Ao + KO * ncp;
-    // the four twiddle tables are one contiguous block of 2 nz4 (KE + KO)
-    // floats in global memory, in the order of the shared copies
+    // eight loads in flight per thread: the prologue is bound by the latency
+    // of L2 (twiddles) and of scattered HBM reads (spectrum)
     {
+        // the tables lie one after another in global memory: WAe, WBe, WAo, WBo
         const float4* src = reinterpret_cast<const float4*>(tb.WAe);
-        float4* dst = reinterpret_cast<float4*>(sWAe);
-        const int n4 = (2 * nz4 * (KE + KO)) >> 2;
-        for (int i = threadIdx.x; i < n4; i += blockDim.x) dst[i] = __ldg(src + i);
+        float* dsts[4] = {sWAe, sWBe, sWAo, sWBo};
+        const int n4[4] = {tE >> 2, tE >> 2, tO >> 2, tO >> 2};
+        for (int q = 0; q < 4; q++) {
+            float4* d = reinterpret_cast<float4*>(dsts[q]);
+            for (int b = threadIdx.x; b < n4[q]; b += 8 * blockDim.x) {
+                float4 v[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int i = b + u * blockDim.x;
+                    if (i < n4[q]) v[u] = __ldg(src + i);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int i = b + u * blockDim.x;
+                    if (i < n4[q]) d[i] = v[u];
+                }
+            }
+            src += n4[q];
+        }
     }
     // spectrum of this ring: rows k, columns (a-row, b-row) of each harmonic
-    for (int i = threadIdx.x; i < nkz * nact; i += blockDim.x) {
-        const int k = i / nact, a = i - k * nact;
-        const float4 o = Ot[((size_t)a * nkz + k) * nr + ir];
-        const int h = k >> 1;
-        float* A = (k & 1) ? Ao : Ae;
-        float* B = (k & 1) ? Bo : Be;
-        A[h * ncp + 2 * a] = o.x;
-        B[h * ncp + 2 * a] = o.y;
-        A[h * ncp + 2 * a + 1] = o.z;
-        B[h * ncp + 2 * a + 1] = o.w;
+    for (int b = threadIdx.x; b < nkz * nact; b += 8 * blockDim.x) {
+        float4 o[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int i = b + u * blockDim.x;
+            if (i < nkz * nact) {
+                const int k = i / nact, a = i - k * nact;
+                o[u] = __ldg(Ot + ((size_t)a * nkz + k) * nr + ir);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int i = b + u * blockDim.x;
+            if (i < nkz * nact) {
+                const int k = i / nact, a = i - k * nact;
+                const int h = k >> 1;
+                float* A = (k & 1) ? Ao : Ae;
+                float* B = (k & 1) ? Bo : Be;
+                A[h * ncp + 2 * a] = o[u].x;
+                B[h * ncp + 2 * a] = o[u].y;
+                A[h * ncp + 2 * a + 1] = o[u].z;
+                B[h * ncp + 2 * a + 1] = o[u].w;
+            }
+        }
     }
     for (int i = threadIdx.x; i < (KE + KO) * (ncp - 2 * nact); i += blockDim.x) {
         const int w = ncp - 2 * nact;
@@ -157,68 +201,50 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
         }
     }
     __syncthreads();
-    // 4x4 tiles of (z, column); the four sums of a tile (even/odd kz x A/B
-    // part) go to four adjacent lanes, recombined by shuffles:
-    // lo = EA + OA + EB + OB, hi = EA - OA - EB + OB
-    const int tilesN = ncp >> 2, tilesM = nz4 >> 2, nt = tilesM * tilesN;
-    const int per = blockDim.x / 4, role = threadIdx.x & 3;
-    const float* Sp = (role == 0) ? Ae : (role == 1) ? Be : (role == 2) ? Ao : Bo;
-    const float* Wp = (role == 0) ? sWAe : (role == 1) ? sWBe : (role == 2) ? sWAo : sWBo;
-    const int KR = (role < 2) ? KE : KO;
-    const float hs = (role == 0 || role == 3) ? 1.f : -1.f;
-    for (int t0 = 0; t0 < nt; t0 += per) {
-        const int tile = t0 + threadIdx.x / 4;
-        const bool act = tile < nt;
-        const int tm = act ? tile / tilesN : 0, tn = act ? tile - tm * tilesN : 0;
+    const int tilesN = ncp >> 2, nt = (nz4 >> 2) * tilesN;
+    for (int tile = threadIdx.x; tile < nt; tile += blockDim.x) {
+        const int tm = tile / tilesN, tn = tile - tm * tilesN;
         const int z0 = tm * 4, c0 = tn * 4;
-        float acc[4][4];
+        float P[4][4], Q[4][4];
 #pragma unroll
         for (int r = 0; r < 4; r++)
 #pragma unroll
-            for (int q = 0; q < 4; q++) acc[r][q] = 0.f;
-        const int kr = act ? KR : 0;
-#pragma unroll 4
-        for (int i = 0; i < kr; i++) {
-            const float4 v = *reinterpret_cast<const float4*>(Sp + i * ncp + c0);
-            const float4 w4 = *reinterpret_cast<const float4*>(Wp + i * nz4 + z0);
-            const float w[4] = {w4.x, w4.y, w4.z, w4.w};
+            for (int q = 0; q < 4; q++) P[r][q] = Q[r][q] = 0.f;
+#pragma unroll 2
+        for (int i = 0; i < KE; i++) {
+            const float4 we = *reinterpret_cast<const float4*>(sWAe + i * nz4 + z0);
+            const float4 ve = *reinterpret_cast<const float4*>(Ae + i * ncp + c0);
+            const float4 wb = *reinterpret_cast<const float4*>(sWBe + i * nz4 + z0);
+            const float4 vb = *reinterpret_cast<const float4*>(Be + i * ncp + c0);
+            const float w1[4] = {we.x, we.y, we.z, we.w}, w2[4] = {wb.x, wb.y, wb.z, wb.w};
 #pragma unroll
             for (int r = 0; r < 4; r++) {
-                acc[r][0] += w[r] * v.x; acc[r][1] += w[r] * v.y; acc[r][2] += w[r] * v.z; acc[r][3] += w[r] * v.w;
+                P[r][0] += w1[r] * ve.x; P[r][1] += w1[r] * ve.y; P[r][2] += w1[r] * ve.z; P[r][3] += w1[r] * ve.w;
+                Q[r][0] += w2[r] * vb.x; Q[r][1] += w2[r] * vb.y; Q[r][2] += w2[r] * vb.z; Q[r][3] += w2[r] * vb.w;
+            }
+            if (i < KO) {
+                const float4 wo = *reinterpret_cast<const float4*>(sWAo + i * nz4 + z0);
+                const float4 vo = *reinterpret_cast<const float4*>(Ao + i * ncp + c0);
+                const float4 wq = *reinterpret_cast<const float4*>(sWBo + i * nz4 + z0);
+                const float4 vq = *reinterpret_cast<const float4*>(Bo + i * ncp + c0);
+                const float w3[4] = {wo.x, wo.y, wo.z, wo.w}, w4[4] = {wq.x, wq.y, wq.z, wq.w};
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    Q[r][0] += w3[r] * vo.x; Q[r][1] += w3[r] * vo.y; Q[r][2] += w3[r] * vo.z; Q[r][3] += w3[r] * vo.w;
+                    P[r][0] += w4[r] * vq.x; P[r][1] += w4[r] * vq.y; P[r][2] += w4[r] * vq.z; P[r][3] += w4[r] * vq.w;
+                }
             }
         }
-        float lo[4][4], hi[4][4];
-#pragma unroll
-        for (int r = 0; r < 4; r++)
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                lo[r][q] = acc[r][q];
-                hi[r][q] = hs * acc[r][q];
-            }
-#pragma unroll
-        for (int o = 1; o < 4; o <<= 1)
-#pragma unroll
-            for (int r = 0; r < 4; r++)
-#pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    lo[r][q] += __shfl_xor_sync(0xffffffffu, lo[r][q], o);
-                    hi[r][q] += __shfl_xor_sync(0xffffffffu, hi[r][q], o);
-                }
-        if (!act || role > 1) continue;
-        // role 0 writes the planes z, role 1 the mirrored planes ngz - z
 #pragma unroll
         for (int r = 0; r < 4; r++) {
             const int z = z0 + r;
             if (z >= Z0) continue;
-            if (role == 0) {
-                *reinterpret_cast<float4*>(Rt + (size_t)z * ncp + c0) =
-                    make_float4(lo[r][0], lo[r][1], lo[r][2], lo[r][3]);
-            } else {
-                const int zm = ngz - z;
-                if (z >= 1 && zm != z && zm < ngz)
-                    *reinterpret_cast<float4*>(Rt + (size_t)zm * ncp + c0) =
-                        make_float4(hi[r][0], hi[r][1], hi[r][2], hi[r][3]);
-            }
+            *reinterpret_cast<float4*>(Rt + (size_t)z * ncp + c0) =
+                make_float4(P[r][0] + Q[r][0], P[r][1] + Q[r][1], P[r][2] + Q[r][2], P[r][3] + Q[r][3]);
+            const int zm = ngz - z;
+            if (z >= 1 && zm != z && zm < ngz)
+                *reinterpret_cast<float4*>(Rt + (size_t)zm * ncp + c0) =
+                    make_float4(P[r][0] - Q[r][0], P[r][1] - Q[r][1], P[r][2] - Q[r][2], P[r][3] - Q[r][3]);
         }
     }
 }
@@ -241,7 +267,19 @@ __global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int 
         const float4* src = reinterpret_cast<const float4*>(tb.TC);
         float4* dst = reinterpret_cast<float4*>(TC);
         const int n4 = (2 * (nact + 1) * njp) >> 2;
-        for (int i = threadIdx.x; i < n4; i += blockDim.x) dst[i] = __ldg(src + i);
+        for (int b = threadIdx.x; b < n4; b += 4 * blockDim.x) {
+            float4 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = b + u * blockDim.x;
+                if (i < n4) v[u] = __ldg(src + i);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = b + u * blockDim.x;
+                if (i < n4) dst[i] = v[u];
+            }
+        }
     }
     for (int i = threadIdx.x; i < 4 * SYN_ZB * ncp; i += blockDim.x) {
         const int t = i / (SYN_ZB * ncp), rem = i - t * SYN_ZB * ncp;
@@ -332,7 +370,8 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar) {
     SynTab tb{b, b + nWe, b + 2 * nWe, b + 2 * nWe + nWo, b + 2 * nWe + 2 * nWo,
               b + 2 * nWe + 2 * nWo + nT, b + 2 * nWe + 2 * nWo + 2 * nT, Z0, KE, KO, njp};
     {
-        const size_t sm = sizeof(float) * (2 * nWe + 2 * nWo + (size_t)(KE + KO) * 2 * ncp);
+        // the tables, three bank pads of at most 31 floats, the spectrum
+        const size_t sm = sizeof(float) * (2 * nWe + 2 * nWo + 3 * 32 + (size_t)(KE + KO) * 2 * ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_synz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         dim3 grid(g.nr, 4);
         k_synz<<<grid, SYNZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, tb, c->synR);
