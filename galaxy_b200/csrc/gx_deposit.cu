@@ -202,28 +202,52 @@ __global__ void __launch_bounds__(ROW_TILE) k_row_scan(int nrow, int ngz, int nr
     (void)nw;
 }
 
-// slot of every particle in the row-ordered permutation: perm[slot] = t
-__global__ void k_place(const int32_t* __restrict__ keys, int64_t n, int nrow, int na,
-                        const int32_t* __restrict__ rowstart, const uint32_t* __restrict__ rowbase,
-                        uint32_t* __restrict__ rowfill, int32_t* __restrict__ perm,
-                        const int32_t* __restrict__ zone, int zsel) {
-    // same block -> counter-copy map as the pass that counted the rows
-    const size_t co = (size_t)(blockIdx.x & (NCOPY - 1)) * (nrow + 1);
-    rowfill += co;
-    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const bool act = t < n;
-    uint32_t row = 0xffffffffu;
-    if (act) {
-        const int32_t key = keys[t];
-        row = (key >= 0 && (!zone || zone[t] == zsel)) ? (uint32_t)(key / na) : (uint32_t)nrow;
+// slot of every particle in the row-ordered permutation: perm[slot] = t.
+// A thread places PLACE_U particles, one from each of PLACE_U consecutive
+// 256-particle blocks of the counting pass (whose block index chose the
+// counter copy), with their loads and atomics issued together.
+#define PLACE_U 4
+__global__ void __launch_bounds__(256) k_place(DevGeo g, const int32_t* __restrict__ keys, int64_t n,
+                                               const int32_t* __restrict__ rowstart,
+                                               const uint32_t* __restrict__ rowbase,
+                                               uint32_t* __restrict__ rowfill,
+                                               int32_t* __restrict__ perm,
+                                               const int32_t* __restrict__ zone, int zsel) {
+    const int nrow = g.nrow;
+    const unsigned lane = threadIdx.x & 31;
+    int64_t t[PLACE_U];
+    uint32_t row[PLACE_U], peers[PLACE_U], base[PLACE_U];
+    size_t co[PLACE_U];
+#pragma unroll
+    for (int u = 0; u < PLACE_U; u++) {
+        const int64_t blk = (int64_t)blockIdx.x * PLACE_U + u;
+        t[u] = blk * 256 + threadIdx.x;
+        co[u] = (size_t)(blk & (NCOPY - 1)) * (nrow + 1);
+        row[u] = 0xffffffffu;
+        if (t[u] < n) {
+            const int32_t key = __ldg(keys + t[u]);
+            int r;
+            row[u] = (key >= 0 && (!zone || __ldg(zone + t[u]) == zsel)) ? (uint32_t)gx_div_na(g, key, r)
+                                                                         : (uint32_t)nrow;
+        }
     }
-    const uint32_t am = __ballot_sync(0xffffffffu, act);
-    const uint32_t peers = __match_any_sync(0xffffffffu, row) & am;
-    const int leader = __ffs(peers) - 1;
-    uint32_t base = 0;
-    if (act && (int)(threadIdx.x & 31) == leader) base = atomicAdd(&rowfill[row], (uint32_t)__popc(peers));
-    base = __shfl_sync(0xffffffffu, base, leader < 0 ? 0 : leader);
-    if (act) perm[rowstart[row] + rowbase[co + row] + base + __popc(peers & lanemask_lt())] = (int32_t)t;
+#pragma unroll
+    for (int u = 0; u < PLACE_U; u++) {
+        const bool act = t[u] < n;
+        const uint32_t am = __ballot_sync(0xffffffffu, act);
+        peers[u] = __match_any_sync(0xffffffffu, row[u]) & am;
+        const int leader = __ffs(peers[u]) - 1;
+        base[u] = 0;
+        if (act && (int)lane == leader) base[u] = atomicAdd(rowfill + co[u] + row[u], (uint32_t)__popc(peers[u]));
+    }
+#pragma unroll
+    for (int u = 0; u < PLACE_U; u++) {
+        const int leader = __ffs(peers[u]) - 1;
+        const uint32_t b = __shfl_sync(0xffffffffu, base[u], leader < 0 ? 0 : leader);
+        if (t[u] < n)
+            perm[__ldg(rowstart + row[u]) + __ldg(rowbase + co[u] + row[u]) + b +
+                 __popc(peers[u] & lanemask_lt())] = (int32_t)t[u];
+    }
 }
 
 // owner-computes deposit of one work item per CTA iteration, from the cell
@@ -244,21 +268,33 @@ __global__ void __launch_bounds__(256) k_deposit(DevGeo g, const int32_t* __rest
         const int row = items[3 * item], s0 = items[3 * item + 1], s1 = items[3 * item + 2];
         for (int i = threadIdx.x; i < NW * na; i += blockDim.x) bins[i] = 0;
         __syncthreads();
-        for (int s = s0 + threadIdx.x; s < s1; s += blockDim.x) {
-            const int p = perm[s];
-            CellW cw;
-            cw.key = keys[p];
-            cw.du = fr[p];
-            cw.dt = fr[cap + p];
-            cw.dz = (NW >= 8) ? fr[2 * cap + p] : 0.f;
-            if (cw.key < 0 || cw.key / na != row) {
+        // an item holds at most DEP_CH = 4 x 256 particles: each thread loads
+        // its four together, then adds them
+        static_assert(DEP_CH <= 4 * 256, "four particles per thread");
+        CellW cw[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int s = s0 + threadIdx.x + u * 256;
+            cw[u].key = -2;
+            if (s < s1) {
+                const int p = __ldg(perm + s);
+                cw[u].key = __ldg(keys + p);
+                cw[u].du = __ldg(fr + p);
+                cw[u].dt = __ldg(fr + cap + p);
+                cw[u].dz = (NW >= 8) ? __ldg(fr + 2 * cap + p) : 0.f;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            if (cw[u].key == -2) continue;
+            int jt;
+            if (cw[u].key < 0 || gx_div_na(g, cw[u].key, jt) != row) {
                 atomicExch(errword, 1);
                 continue;
             }
-            const int jt = cw.key - row * na;
             float w[NW == 27 ? 27 : 8];
-            if constexpr (NW == 27) gx_weights27(cw, w);
-            else gx_weights(g, cw, w);
+            if constexpr (NW == 27) gx_weights27(cw[u], w);
+            else gx_weights(g, cw[u], w);
 #pragma unroll
             for (int k = 0; k < NW; k++) atomicAdd(&bins[k * na + jt], __float2int_rn(w[k] * FIXQ));
         }
@@ -371,9 +407,9 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
                                                    c->rowitem, c->items, c->nitems_d, c->jrk_d);
     GX_LAUNCHED(c);
     if (n > 0) {
-        k_place<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(keys, n, g.nrow, g.na, c->rowstart,
-                                                                  c->rowbase, c->rowfill, perm_out,
-                                                                  zone, zsel);
+        const int64_t nblk = (n + 255) / 256;
+        k_place<<<(unsigned)((nblk + PLACE_U - 1) / PLACE_U), 256, 0, c->stream>>>(
+            g, keys, n, c->rowstart, c->rowbase, c->rowfill, perm_out, zone, zsel);
         GX_LAUNCHED(c);
     }
     rc = gx_phase_mark(c, PH_DEPOSIT);
