@@ -96,11 +96,12 @@ __global__ void k_syntab(DevGeo g, ActList act, int nact, float scale, float* WA
 // vertical synthesis, one CTA per (ring, field type); R[t][ir][z][ncp].
 // With P = EA + OB and Q = OA + EB (E/O: even/odd wavenumbers, A/B: the
 // two parts of the spectrum), plane z is P + Q and plane ngz - z is P - Q.
-// Each thread owns a 4 x 4 (plane, column) tile of P and Q; per wavenumber
-// pair it reads one float4 of each twiddle table (the planes of a
-// wavenumber are contiguous) and one float4 of each spectrum part, for 64
-// FMAs.  The four twiddle tables start on different shared-memory banks.
-#define SYNZ_THREADS 256
+// Two threads own a 4 x 4 (plane, column) tile of P and Q, each summing
+// every other wavenumber pair, combined by a shuffle; per pair a thread
+// reads one float4 of each twiddle table (the planes of a wavenumber are
+// contiguous) and one float4 of each spectrum part, for 64 FMAs.  The four
+// twiddle tables start on different shared-memory banks.
+#define SYNZ_THREADS 288
 __device__ __forceinline__ int synz_pad(int start, int want) {
     return ((want - start) % 32 + 32) % 32;  // floats to add so that start lands on bank want
 }
@@ -202,16 +203,20 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
     }
     __syncthreads();
     const int tilesN = ncp >> 2, nt = (nz4 >> 2) * tilesN;
-    for (int tile = threadIdx.x; tile < nt; tile += blockDim.x) {
-        const int tm = tile / tilesN, tn = tile - tm * tilesN;
+    const int ks = threadIdx.x & 1;
+    for (int t0 = 0; t0 < nt; t0 += blockDim.x >> 1) {
+        const int tile = t0 + (threadIdx.x >> 1);
+        const bool act = tile < nt;
+        const int tm = act ? tile / tilesN : 0, tn = act ? tile - tm * tilesN : 0;
         const int z0 = tm * 4, c0 = tn * 4;
         float P[4][4], Q[4][4];
 #pragma unroll
         for (int r = 0; r < 4; r++)
 #pragma unroll
             for (int q = 0; q < 4; q++) P[r][q] = Q[r][q] = 0.f;
+        const int kend = act ? KE : 0;
 #pragma unroll 2
-        for (int i = 0; i < KE; i++) {
+        for (int i = ks; i < kend; i += 2) {
             const float4 we = *reinterpret_cast<const float4*>(sWAe + i * nz4 + z0);
             const float4 ve = *reinterpret_cast<const float4*>(Ae + i * ncp + c0);
             const float4 wb = *reinterpret_cast<const float4*>(sWBe + i * nz4 + z0);
@@ -235,6 +240,14 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
                 }
             }
         }
+#pragma unroll
+        for (int r = 0; r < 4; r++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                P[r][q] += __shfl_xor_sync(0xffffffffu, P[r][q], 1);
+                Q[r][q] += __shfl_xor_sync(0xffffffffu, Q[r][q], 1);
+            }
+        if (!act || ks) continue;
 #pragma unroll
         for (int r = 0; r < 4; r++) {
             const int z = z0 + r;
