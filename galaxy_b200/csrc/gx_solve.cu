@@ -243,11 +243,38 @@ __global__ void __launch_bounds__(288) k_fwd_z(DevGeo g, int nact, int ncp,
     }
     float* B = sm;                      // [ngz][ncp]
     float* Tk = B + ngz * ncp;          // [FWD_KR][ngz]
-    const float* src = C1 + (size_t)ir * ngz * ncp;
-    for (int i = threadIdx.x; i < ngz * ncp / 4; i += blockDim.x)
-        reinterpret_cast<float4*>(B)[i] = reinterpret_cast<const float4*>(src)[i];
-    for (int i = threadIdx.x; i < FWD_KR * ngz; i += blockDim.x)
-        Tk[i] = (i < nrow_out * ngz) ? Tz[(size_t)kr0 * ngz + i] : 0.f;
+    // several loads in flight per thread: the prologue is latency-bound
+    {
+        const float4* src = reinterpret_cast<const float4*>(C1 + (size_t)ir * ngz * ncp);
+        float4* dst = reinterpret_cast<float4*>(B);
+        const int n4 = ngz * ncp / 4;
+        for (int b = threadIdx.x; b < n4; b += 4 * blockDim.x) {
+            float4 v[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = b + u * blockDim.x;
+                if (i < n4) v[u] = __ldg(src + i);
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int i = b + u * blockDim.x;
+                if (i < n4) dst[i] = v[u];
+            }
+        }
+    }
+    for (int b = threadIdx.x; b < FWD_KR * ngz; b += 4 * blockDim.x) {
+        float v[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = b + u * blockDim.x;
+            v[u] = (i < nrow_out * ngz) ? __ldg(Tz + (size_t)kr0 * ngz + i) : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int i = b + u * blockDim.x;
+            if (i < FWD_KR * ngz) Tk[i] = v[u];
+        }
+    }
     __syncthreads();
     sgemm44_sk<4>(nrow_out, ncp, ngz, Tk, ngz, B, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
         // rows r0 = 2k, 2k+1, 2k+2, 2k+3 (relative to kr0); cols c0 = 2a .. 2a+3

@@ -294,12 +294,22 @@ __global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int 
             }
         }
     }
-    for (int i = threadIdx.x; i < 4 * SYN_ZB * ncp; i += blockDim.x) {
-        const int t = i / (SYN_ZB * ncp), rem = i - t * SYN_ZB * ncp;
-        const int z = rem / ncp, c = rem - z * ncp;
-        float v = 0.f;
-        if (((tmask >> t) & 1) && z < nz) v = R[(((size_t)t * nr + ir) * ngz + zb + z) * ncp + c];
-        Rs[i] = v;
+    for (int b = threadIdx.x; b < 4 * SYN_ZB * ncp; b += 8 * blockDim.x) {
+        float v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int i = b + u * blockDim.x;
+            const int t = i / (SYN_ZB * ncp), rem = i - t * SYN_ZB * ncp;
+            const int z = rem / ncp, c = rem - z * ncp;
+            v[u] = 0.f;
+            if (i < 4 * SYN_ZB * ncp && ((tmask >> t) & 1) && z < nz)
+                v[u] = __ldg(R + (((size_t)t * nr + ir) * ngz + zb + z) * ncp + c);
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int i = b + u * blockDim.x;
+            if (i < 4 * SYN_ZB * ncp) Rs[i] = v[u];
+        }
     }
     __syncthreads();
     const int nq = njp >> 2, half = na / 2;
