@@ -173,9 +173,12 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB) k_conv_bulk(ConvArgs A) 
         }
         for (int t = 0; t < 4; t++) {
             if (!((A.tmask >> t) & 1)) continue;
-            float4* out = A.O + (((size_t)t * A.nact + a) * nkz + k) * nr;
+            // ring-major output [t][ir][kz][a]: the synthesis reads a ring's
+            // spectrum as one contiguous block
+            const size_t ost = (size_t)nkz * A.nact;
+            float4* out = A.O + ((size_t)t * nr * nkz + k) * A.nact + a;
             if (!type_valid(g, t, m, k)) {
-                for (int i = threadIdx.x; i < nr; i += NCW * 32) out[i] = make_float4(0, 0, 0, 0);
+                for (int i = threadIdx.x; i < nr; i += NCW * 32) out[i * ost] = make_float4(0, 0, 0, 0);
                 continue;
             }
             float4 acc[NJ][4];
@@ -238,7 +241,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB) k_conv_bulk(ConvArgs A) 
                     const float4 p = part[w * nr + i];
                     v.x += p.x; v.y += p.y; v.z += p.z; v.w += p.w;
                 }
-                out[i] = v;
+                out[i * ost] = v;
             }
             consumer_sync<NCW>();
         }

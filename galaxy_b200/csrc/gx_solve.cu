@@ -357,9 +357,11 @@ __global__ void __launch_bounds__(256) k_conv(DevGeo g, int nact, int tmask,
         bool valid = true;
         if (t == 1) valid = (m >= 1) && (m <= min(ng, mmax - 1) - 1);
         if (t == 2) valid = (g.ndim == 3) && (k >= 1) && (k <= ngz - 1);
-        float4* out = O + (((size_t)t * nact + a) * nkz + k) * nr;
+        // ring-major output [t][ir][kz][a] (read as one block per ring by the synthesis)
+        const size_t ost = (size_t)nkz * nact;
+        float4* out = O + ((size_t)t * nr * nkz + k) * nact + a;
         if (!valid) {
-            for (int i = threadIdx.x; i < nr; i += blockDim.x) out[i] = make_float4(0, 0, 0, 0);
+            for (int i = threadIdx.x; i < nr; i += blockDim.x) out[i * ost] = make_float4(0, 0, 0, 0);
             continue;
         }
         const float* Gt = G + ((((size_t)t * ng + m) * nkz + k) * nr) * (size_t)nr;
@@ -408,7 +410,7 @@ __global__ void __launch_bounds__(256) k_conv(DevGeo g, int nact, int tmask,
                 float4 p = part[w * nr + i];
                 s.x += p.x; s.y += p.y; s.z += p.z; s.w += p.w;
             }
-            out[i] = s;
+            out[i * ost] = s;
         }
         __syncthreads();
     }

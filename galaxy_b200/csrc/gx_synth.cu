@@ -113,13 +113,14 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
     if (!((tmask >> t) & 1)) return;
     const int nr = g.nr, nkz = g.nkz, ngz = g.ngz;
     float* Rt = R + (((size_t)t * nr + ir) * ngz) * ncp;
-    const float4* Ot = O + (size_t)t * nact * nkz * nr;
+    // this ring's spectrum, one contiguous block [kz][a] (ring-major [t][ir][kz][a])
+    const float4* Ot = O + (((size_t)t * nr + ir) * nkz) * nact;
     if (g.ndim == 2) {
         for (int c = threadIdx.x; c < ncp; c += blockDim.x) {
             const int a = c >> 1;
             float v = 0.f;
             if (a < nact) {
-                float4 o = Ot[(size_t)a * nr + ir];
+                float4 o = Ot[a];
                 v = (c & 1) ? o.z : o.x;
             }
             Rt[c] = v;
@@ -170,10 +171,7 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
 #pragma unroll
         for (int u = 0; u < 8; u++) {
             const int i = b + u * blockDim.x;
-            if (i < nkz * nact) {
-                const int k = i / nact, a = i - k * nact;
-                o[u] = __ldg(Ot + ((size_t)a * nkz + k) * nr + ir);
-            }
+            if (i < nkz * nact) o[u] = __ldg(Ot + i);
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {
