@@ -238,6 +238,7 @@ __device__ __forceinline__ bool gx_near_int(float v, float eps) {
 // nearest node (ju, jz, jt) = int(coord + 1/2), ju in [1, nr - 2], jz in
 // [0, ngz - 2], jt = na wrapping to spoke 0 in the key; the fractions are
 // coord + 1/2 - index (outside [0, 1) where an index was clamped)
+template <bool EXACT = true>
 __device__ __forceinline__ CellW gx_cell27(const DevGeo& g, float u, float t, float z, CellW c) {
     const float uh = __fadd_rn(u, 0.5f), th = __fadd_rn(t, 0.5f);
     float f;
@@ -245,7 +246,7 @@ __device__ __forceinline__ CellW gx_cell27(const DevGeo& g, float u, float t, fl
     ju = min(max(ju, 1), g.nr - 2);
     const int jt = gx_trunc(th, c.dt);
     float zz = (z + g.zm) * g.inv_dzg;
-    if (gx_near_int(zz + 0.5f, g.eps_z)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
+    if (EXACT && gx_near_int(zz + 0.5f, g.eps_z)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
     const float zh = __fadd_rn(zz, 0.5f);
     int jz = gx_trunc(zh, f);
     jz = min(max(jz, 0), g.ngz - 2);
@@ -258,7 +259,12 @@ __device__ __forceinline__ CellW gx_cell27(const DevGeo& g, float u, float t, fl
 }
 
 // Cell of a particle; old != 0 for interpolation (no sector folding).
-__device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, float z, bool old) {
+// EXACT = false drops the guard bands: the cell may then differ from the
+// reference's for a coordinate within a few ulp of a cell boundary, where
+// the interpolated field is continuous (the particle pass's interpolation
+// cell); keys that are deposited or reported use the exact form.
+template <bool EXACT>
+__device__ __forceinline__ CellW gx_cell_t(const DevGeo& g, float x, float y, float z, bool old) {
     CellW c;
     c.key = -1;
     c.du = c.dt = c.dz = 0.f;
@@ -273,7 +279,7 @@ __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, floa
     else u = __logf(rr) * g.inv_ua + g.uoffs;
     // the quadratic scheme truncates coord + 1/2: its boundaries sit at half-integers
     const float sh = g.quad ? 0.5f : 0.f;
-    {
+    if (EXACT) {
         // __logf: 2^-21.41 absolute error on [0.5, 2], 3 ulp elsewhere
         float eps = 5.0e-7f * g.inv_ua + 2.0e-6f * (fabsf(u) + fabsf(g.uoffs) + 1.0f);
         if (gx_near_int(u + sh, eps) || u < eps) u = gx_u_exact(g, rr);
@@ -284,12 +290,12 @@ __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, floa
         t = atan2f(y, x) * g.t_scale;
         if (t < 0.f) t += g.fna;
         const float eps = g.eps_t;
-        if (gx_near_int(t + sh, eps) || t < eps || t > g.fna - eps) t = gx_t_exact(g, x, y);
+        if (EXACT && (gx_near_int(t + sh, eps) || t < eps || t > g.fna - eps)) t = gx_t_exact(g, x, y);
     } else {
         t = 0.f;
     }
     if (!old && g.nsect > 1) t = fmodf(t, g.thmax);
-    if (g.quad) return gx_cell27(g, u, t, z, c);
+    if (g.quad) return gx_cell27<EXACT>(g, u, t, z, c);
     int ju = gx_trunc(u, c.du);
     if (ju > g.nr - 2) {
         ju = g.nr - 2;
@@ -300,7 +306,7 @@ __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, floa
         c.row = ju;
     } else {
         float zz = (z + g.zm) * g.inv_dzg;
-        if (gx_near_int(zz, g.eps_z)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
+        if (EXACT && gx_near_int(zz, g.eps_z)) zz = __fdiv_rn(__fadd_rn(z, g.zm), g.dzg);
         int jz = gx_trunc(zz, c.dz);
         if (jz > g.ngz - 2) {
             jz = g.ngz - 2;
@@ -317,6 +323,10 @@ __device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, floa
         c.row += 1;
     }
     return c;
+}
+
+__device__ __forceinline__ CellW gx_cell(const DevGeo& g, float x, float y, float z, bool old) {
+    return gx_cell_t<true>(g, x, y, z, old);
 }
 
 // x + v with the rounding error of the sum carried in a low part (the

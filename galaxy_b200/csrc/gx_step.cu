@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
             vy = Pin[3 * cap + p];
         }
         const int32_t o = orig_in[p];
-        const CellW cw = gx_cell(g, x, y, z, true);
+        const CellW cw = gx_cell_t<false>(g, x, y, z, true);
         float ax, ay, az, ph;
         gx_accel_cell_t<Q>(g, F, cw, x, y, z, ax, ay, az, ph);
         vx += ax;
