@@ -289,20 +289,25 @@ def run_e2e(args, w, rec, pm, cfg_dev):
     gal.masset()
     gal.step(1)
     n = rec.shape[0]
-    t0 = time.perf_counter()
-    gal.loadup_ptr(src, n)
-    gal.masset()
-    gal.step(args.steps)
-    gal.unload_ptr(dst)
-    t1 = time.perf_counter()
+    # best of two runs: the wall clock includes host-side copies whose speed
+    # varies with what else the host is doing
+    best = None
+    for _ in range(2):
+        t0 = time.perf_counter()
+        gal.loadup_ptr(src, n)
+        gal.masset()
+        gal.step(args.steps)
+        gal.unload_ptr(dst)
+        t1 = time.perf_counter()
+        best = (t1 - t0) if best is None else min(best, t1 - t0)
     ok = bool(np.isfinite(pin_out.array).all())
     gal.close()
     pin_in.free()
     pin_out.free()
     nbytes = n * rec.shape[1] * 4
-    return {"value": n * args.steps / (t1 - t0), "unit": UNIT,
+    return {"value": n * args.steps / best, "unit": UNIT,
             "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
-            "pinned": pinned, "finite": ok, "what": "gx_loadup + gx_masset + gx_step(K) + gx_unload, wall clock"}
+            "pinned": pinned, "finite": ok, "what": "gx_loadup + gx_masset + gx_step(K) + gx_unload, wall clock, best of 2"}
 
 
 def run_sfp(n=20_000_000, reps=5):
