@@ -19,7 +19,7 @@ from ._abi import (GxConfig, GxDiag, GxGeometry, make_config, GX_OK, GX_PREC_FP6
                    GX_SOFT_SPLINE, GX_GRID_MASS, GX_GRID_FR, GX_GRID_FT, GX_GRID_FZ,
                    GX_GRID_POT, GX_GRID_FX, GX_GRID_FY, GX_GREEN_FR, GX_GREEN_FT,
                    GX_GREEN_FZ, GX_GREEN_POT, GX_FLAG_COMPENSATED,
-                   GX_FLAG_QUADRATIC)
+                   GX_FLAG_QUADRATIC, GX_FLAG_WHOLE_GRID)
 
 __all__ = ["Galaxy", "GxError", "GxConfig", "GxDiag", "GxGeometry", "make_config", "lib",
            "LIB_PATH"]
@@ -74,6 +74,7 @@ def lib():
         L.gx_adjoint.argtypes = [P, C.c_int, C.c_int, P, P, P, P]
         L.gx_set_zones.argtypes = [P, C.c_int32, P, P]
         L.gx_zone_info.argtypes = [P, P, P]
+        L.gx_zone_rings.argtypes = [P, P]
         L.gx_danl.argtypes = [P, C.c_double, P]
         _lib = L
     return _lib
@@ -265,6 +266,13 @@ class Galaxy:
         istep = np.zeros(1, np.int32)
         self._chk(self._L.gx_zone_info(self._h, _ptr(zone), _ptr(istep)))
         return zone, int(istep[0])
+
+    def zone_rings(self):
+        """((jrs, krs) source rings, (jrf, krf) field rings) of the next
+        step's solve, 1-based inclusive"""
+        r = np.zeros(4, np.int32)
+        self._chk(self._L.gx_zone_rings(self._h, _ptr(r)))
+        return (int(r[0]), int(r[1])), (int(r[2]), int(r[3]))
 
     def tmcent(self, start=True):
         self._chk(self._L.gx_tmcent(self._h, int(start)))

@@ -23,6 +23,7 @@ GX_PREC_FP64 = 1
 GX_PREC_MIXED_TC05 = 2
 GX_FLAG_COMPENSATED = 1
 GX_FLAG_QUADRATIC = 2
+GX_FLAG_WHOLE_GRID = 4
 
 GX_GRID_MASS = 0
 GX_GRID_FR = 1

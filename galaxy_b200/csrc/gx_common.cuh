@@ -145,7 +145,8 @@ struct GxCtx {
     float* zbuf = nullptr;                   // [2][nzones][mesh] mass arrays of zones 2..nzones
     float* znew[GX_MAX_ZONES] = {};          // newest array of each zone (index >= 1)
     float* zold[GX_MAX_ZONES] = {};          // the one before it
-    int32_t* zjrk_d = nullptr;               // [GX_MAX_ZONES][2] ring range of each zone's mass
+    int32_t* zjrk_d = nullptr;               // [GX_MAX_ZONES][2] ring range of each zone's mass,
+                                             // then [2] the field rings of the next partial solve
     int istep = 0;                           // step counter of the zone schedule
     int lstep[GX_MAX_ZONES][2] = {};         // step numbers of zold, znew
     bool zones_ready = false;                // zone arrays deposited (gx_masset)
@@ -555,7 +556,8 @@ int setgrd(const GxConfig* c, GxGeometry* g, std::string& err);
 void fill_devgeo(GxCtx* c);
 int gx_green_build_dev(GxCtx* c);
 int gx_mixed_masset(GxCtx* c);
-int gx_mixed_findf(GxCtx* c, int lpot, bool polcat);
+// frk: device [2] 1-based field ring range of a partial-grid solve, or null
+int gx_mixed_findf(GxCtx* c, int lpot, bool polcat, const int32_t* frk = nullptr);
 int gx_mixed_getacc(GxCtx* c, float* acc, float* pot);
 int gx_mixed_step(GxCtx* c, int nsteps, int phys);
 int gx_mixed_sort_deposit(GxCtx* c);
@@ -577,6 +579,6 @@ int gx_zone_unload(GxCtx* c, float* staging);
 int gx_zone_masset(GxCtx* c);
 int gx_zone_step(GxCtx* c, int nsteps, int phys);
 int gx_comm_reduce_range(GxCtx* c);
-int gx_synthesis(GxCtx* c, int tmask, float* polar);
+int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk = nullptr);
 int gx_comm_reduce_spectrum(GxCtx* c);
 void gx_comm_destroy(GxCtx* c);

@@ -427,7 +427,7 @@ static int set_act(GxCtx* c) {
 }
 
 // findf for the mixed path: mass -> field (and optional polar copy)
-int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
+int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* frk) {
     const DevGeo& g = c->g;
     const int nact = c->spec.nact;
     if (nact == 0) return c->err = "no active harmonics", GX_ERR_ARG;
@@ -495,7 +495,7 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field) {
     }
     rc = gx_phase_mark(c, PH_SYN);
     if (rc) return rc;
-    rc = gx_synthesis(c, tmask, polar);
+    rc = gx_synthesis(c, tmask, polar, frk);
     if (rc) return rc;
     rc = gx_phase_end(c);
     if (rc) return rc;

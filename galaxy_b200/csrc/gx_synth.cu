@@ -107,10 +107,11 @@ __device__ __forceinline__ int synz_pad(int start, int want) {
 }
 __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int ncp, int tmask,
                                              const float4* __restrict__ O, SynTab tb,
-                                             float* __restrict__ R) {
+                                             float* __restrict__ R, const int32_t* __restrict__ frk) {
     extern __shared__ __align__(16) float sm[];
     const int ir = blockIdx.x, t = blockIdx.y;
     if (!((tmask >> t) & 1)) return;
+    if (frk && (ir + 1 < frk[0] || ir + 1 > frk[1])) return;  // partial grid (p3fsyn jrf..krf)
     const int nr = g.nr, nkz = g.nkz, ngz = g.ngz;
     float* Rt = R + (((size_t)t * nr + ir) * ngz) * ncp;
     // this ring's spectrum, one contiguous block [kz][a] (ring-major [t][ir][kz][a])
@@ -264,9 +265,11 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
 // azimuthal synthesis + polcat, one CTA per (ring, SYN_ZB planes)
 __global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int tmask,
                                               const float* __restrict__ R, SynTab tb,
-                                              float4* __restrict__ F, float* __restrict__ polar) {
+                                              float4* __restrict__ F, float* __restrict__ polar,
+                                              const int32_t* __restrict__ frk) {
     extern __shared__ __align__(16) float sm[];
     const int ir = blockIdx.x, zb = blockIdx.y * SYN_ZB;
+    if (frk && (ir + 1 < frk[0] || ir + 1 > frk[1])) return;  // rings no moving particle reads
     const int nr = g.nr, ngz = g.ngz, na = g.na, njp = tb.njp;
     const int nz = min(SYN_ZB, ngz - zb);
     float* TC = sm;                      // [nact][njp]
@@ -364,7 +367,7 @@ __global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int 
 }
 
 // ---------------------------------------------------------------------------
-int gx_synthesis(GxCtx* c, int tmask, float* polar) {
+int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk) {
     const DevGeo& g = c->g;
     const int nact = c->spec.nact;
     const int ncp = ru4s(2 * nact);
@@ -395,14 +398,14 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar) {
         const size_t sm = sizeof(float) * (2 * nWe + 2 * nWo + 3 * 32 + (size_t)(KE + KO) * 2 * ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_synz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         dim3 grid(g.nr, 4);
-        k_synz<<<grid, SYNZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, tb, c->synR);
+        k_synz<<<grid, SYNZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, tb, c->synR, frk);
         GX_LAUNCHED(c);
     }
     {
         const size_t sm = sizeof(float) * (2 * nT + 2 * (size_t)njp + (size_t)4 * SYN_ZB * ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_synaz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         dim3 grid(g.nr, (g.ngz + SYN_ZB - 1) / SYN_ZB);
-        k_synaz<<<grid, 256, sm, c->stream>>>(g, nact, ncp, tmask, c->synR, tb, c->field, polar);
+        k_synaz<<<grid, 256, sm, c->stream>>>(g, nact, ncp, tmask, c->synR, tb, c->field, polar, frk);
         GX_LAUNCHED(c);
     }
     return GX_OK;

@@ -202,9 +202,10 @@ struct ZoneSrc {
 };
 
 // zoncmb + scaled: mass = (mass + sum fr_k src_k) pmass, in the reference's
-// order; block 0 also forms the source ring range over the zones
+// order; block 0 also forms the source ring range over the zones and the
+// field rings of a partial-grid solve in which zones 1..mz move
 __global__ void k_zone_combine(int64_t mesh, float* __restrict__ mass, ZoneSrc src, float pm,
-                               int nz, int nr, int32_t* __restrict__ zjrk,
+                               int nz, int nr, int mz, int32_t* __restrict__ zjrk,
                                int32_t* __restrict__ jrk) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i < mesh) {
@@ -221,6 +222,14 @@ __global__ void k_zone_combine(int64_t mesh, float* __restrict__ mass, ZoneSrc s
         }
         jrk[0] = jrs;
         jrk[1] = krs;
+        // p3fndf.f:66-80, p2fndf.f:41-55: from jrad(1) to krad(mz), the
+        // outer edge moved out while it lies inside jrad(1)
+        int jrf = zjrk[0] < nr ? zjrk[0] : 1;
+        int kz = mz - 1, krf = zjrk[2 * kz + 1];
+        while (krf < jrf && kz + 1 < nz) krf = zjrk[2 * (++kz) + 1];
+        int32_t* frk = zjrk + 2 * GX_MAX_ZONES;
+        frk[0] = krf < jrf ? 1 : jrf;
+        frk[1] = krf < jrf ? nr : min(krf, nr);
     }
 }
 
@@ -287,7 +296,8 @@ static int zone_combine(GxCtx* c) {
     }
     const int64_t mesh = c->g.mesh;
     k_zone_combine<<<(unsigned)((mesh + 255) / 256), 256, 0, c->stream>>>(
-        mesh, c->mass, src, c->g.pmass, c->nzones, c->g.nr, c->zjrk_d, c->jrk_d);
+        mesh, c->mass, src, c->g.pmass, c->nzones, c->g.nr, zone_mzone(c, c->istep), c->zjrk_d,
+        c->jrk_d);
     GX_LAUNCHED(c);
     return GX_OK;
 }
@@ -341,7 +351,11 @@ int gx_zone_step(GxCtx* c, int nsteps, int phys) {
     for (int s = 0; s < nsteps; s++) {
         const bool last = (s == nsteps - 1);
         const int mzone = zone_mzone(c, c->istep);
-        int rc = gx_mixed_findf(c, phys && last, true);
+        // findf.f:41-54: the field over the rings of zones 1..mzone only, when
+        // the outer zones stay and no potential is wanted
+        const bool lpot = phys && last;
+        const bool partial = !lpot && mzone < c->nzones && !(c->cfg.flags & GX_FLAG_WHOLE_GRID);
+        int rc = gx_mixed_findf(c, lpot, true, partial ? c->zjrk_d + 2 * GX_MAX_ZONES : nullptr);
         if (rc) return rc;
         zone_masscl(c, mzone, true);
         const int nxt = c->cur ^ 1;
@@ -405,7 +419,7 @@ int gx_set_zones(GxCtx* c, int32_t nzones, const int32_t* nstep, const float* zb
     if (nzones == 1) return GX_OK;
     const size_t mesh = c->g.mesh;
     if (cudaMalloc((void**)&c->zbuf, sizeof(float) * 2 * (nzones - 1) * mesh) != cudaSuccess ||
-        cudaMalloc((void**)&c->zjrk_d, sizeof(int32_t) * 2 * GX_MAX_ZONES) != cudaSuccess) {
+        cudaMalloc((void**)&c->zjrk_d, sizeof(int32_t) * (2 * GX_MAX_ZONES + 2)) != cudaSuccess) {
         c->nzones = 1;
         return c->err = "cudaMalloc of the zone mass arrays failed", GX_ERR_NOMEM;
     }
@@ -414,6 +428,23 @@ int gx_set_zones(GxCtx* c, int32_t nzones, const int32_t* nstep, const float* zb
         c->zold[k] = c->zbuf + (size_t)(2 * (k - 1) + 1) * mesh;
     }
     GX_CUDA(c, cudaMemset(c->zbuf, 0, sizeof(float) * 2 * (nzones - 1) * mesh));
+    return GX_OK;
+}
+
+int gx_zone_rings(GxCtx* c, int32_t* rings) {
+    if (!c || !rings) return GX_ERR_ARG;
+    if (c->nzones < 2) return c->err = "no time-step zones (gx_set_zones)", GX_ERR_STATE;
+    if (!c->zones_ready) return c->err = "zone mass arrays not assigned (call gx_masset)", GX_ERR_STATE;
+    cudaSetDevice(c->dev);
+    GX_CUDA(c, cudaMemcpyAsync(rings, c->jrk_d, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, c->stream));
+    GX_CUDA(c, cudaMemcpyAsync(rings + 2, c->zjrk_d + 2 * GX_MAX_ZONES, 2 * sizeof(int32_t),
+                               cudaMemcpyDeviceToHost, c->stream));
+    GX_CUDA(c, cudaStreamSynchronize(c->stream));
+    const int mz = zone_mzone(c, c->istep);
+    if (mz == c->nzones || (c->cfg.flags & GX_FLAG_WHOLE_GRID)) {
+        rings[2] = 1;
+        rings[3] = c->g.nr;
+    }
     return GX_OK;
 }
 

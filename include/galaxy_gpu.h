@@ -60,6 +60,9 @@ extern "C" {
 #define GX_FLAG_QUADRATIC   2   /* p3d 'inte 3': 27-point quadratic interpolation
                                    (weight.f:251-314, massgn.f:173-202,
                                    grdacc.f:267-299) instead of the 8-point one */
+#define GX_FLAG_WHOLE_GRID  4   /* time-step zones: the field over the whole grid
+                                   on every step (the 'wholeg' option, findf.f:41)
+                                   instead of partial-grid solves */
 #define GX_MAX_WEIGHTS     27   /* weights per particle of gx_weight          */
 
 /* grid arrays for gx_get_grid / gx_set_mass */
@@ -237,10 +240,20 @@ int gx_step(GxCtx* ctx, int nsteps, int phys);
  * nstep^2 (getacc.f:141-150), particles crossing a boundary change step
  * (rezgrp.f, chstep.f) and particles leaving the grid move to the outer
  * zone's step (addoff.f); each zone keeps its own mass array and the solve
- * uses their linear interpolation in time (masscl.f:64-96, zoncmb.f:46-129),
- * over the whole grid.  Mixed path; no compensated positions, ensembles,
- * adjoint or guard zones.  nzones = 1 restores the single-zone step. */
+ * uses their linear interpolation in time (masscl.f:64-96, zoncmb.f:46-129).
+ * On steps where only zones 1..m < nzones move and no potential is wanted,
+ * the field is synthesised only over the rings from jrad(1) to krad(m)
+ * (findf.f:41-54, p3fndf.f:66-80): the forces on every moving particle are
+ * those of the whole-grid solve, the other rings keep their last field.
+ * GX_FLAG_WHOLE_GRID solves the whole grid on every step.  Mixed path; no
+ * compensated positions, ensembles, adjoint or guard zones.  nzones = 1
+ * restores the single-zone step. */
 int gx_set_zones(GxCtx* ctx, int32_t nzones, const int32_t* nstep, const float* zbr);
+
+/* The ring ranges (1-based, inclusive) of the next step's solve: rings[0..1]
+ * the source rings jrs..krs holding mass, rings[2..3] the field rings jrf..krf
+ * (1..nr on whole-grid steps) -- what findf.f:49-53 reports.  After gx_masset. */
+int gx_zone_rings(GxCtx* ctx, int32_t* rings);
 
 /* Zone of every particle in load order (1..nzones, nzones + 1 off the
  * grid) and the step counter; zone may be NULL. */

@@ -67,3 +67,13 @@ def test_grdset_rejects_bad_cards_without_gpu():
         Galaxy(make_config(3, 16, 128, ngz=15, dzg=0.5, ng=4, softl=0.4))
     with pytest.raises(GxError, match="Unrecognized softening rule"):
         Galaxy(make_config(2, 16, 32, ng=4, softl=0.5, tsoft=3))
+
+
+def test_python_constants_match_the_header():
+    """every GX_* integer constant the Python side defines has the header's value"""
+    from galaxy_b200 import _abi
+    hdr = dict(re.findall(r"^#define\s+(GX_\w+)\s+(-?\d+)\b", open(HDR).read(), re.M))
+    py = {k: v for k, v in vars(_abi).items() if k.startswith("GX_") and isinstance(v, int)}
+    assert len(py) >= 20
+    for k, v in py.items():
+        assert k in hdr and int(hdr[k]) == v, k

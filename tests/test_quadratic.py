@@ -206,3 +206,21 @@ def test_gpu_quadratic_with_time_step_zones_tracks_oracle():
     scale = np.abs(ref[:, :3]).max()
     d = np.abs(pos[:, :3] - ref[:, :3]).max(axis=1)
     assert np.mean(d > 2e-5 * scale) < 2e-3 and d.max() / scale < 1e-3
+
+
+@pytest.mark.gpu
+def test_gpu_quadratic_keys_with_sectors_and_an_empty_deposit():
+    """sector folding (nsect = 2) ahead of the nearest-node rule; no particles"""
+    cfg = cfgq()
+    cfg.nsect = 2
+    cfg.ng = 9
+    rec = np.concatenate([disk(20000)[0], boundary_points(cfg, 2000)])
+    for old in (False, True):
+        okey, owt, oon = ox.weight(cfg, rec, old=old, prec=32)
+        with Galaxy(cfg) as gal:
+            key, wt = gal.weight(rec, old=old)
+        assert np.array_equal(key, np.where(oon, okey, -1)), old
+    with Galaxy(cfgq()) as gal:
+        gal.loadup(np.zeros((0, 6), np.float32))
+        gal.masset()
+        assert not np.any(gal.grid(GX_GRID_MASS))

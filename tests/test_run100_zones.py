@@ -188,3 +188,82 @@ def test_gpu_tmcent_uses_each_zones_step(fx):
     t = np.asarray(nstep, np.float64)[np.minimum(zone, 2) - 1]
     want = -0.5 * acc.astype(np.float64) * t[:, None]
     assert np.abs((v1 - v0) - want).max() < 1e-6 * np.abs(v0).max()
+
+
+@pytest.mark.gpu
+def test_gpu_zone_api_checks_and_empty_runs(fx):
+    from galaxy_b200 import GxError, GX_PREC_FP64
+    cfg, nstep, zbr = run100(fx)
+    with Galaxy(cfg) as gal:
+        for bad_nstep, bad_zbr in (([2, 2], zbr),             # nstep[0] must be 1
+                                   ([1, 2, 4], [0.0, 40.0, 20.0]),  # boundaries descending
+                                   ([1, 2], [0.0, 1e4])):       # boundary outside the grid
+            with pytest.raises(GxError):
+                gal.set_zones(bad_nstep, bad_zbr)
+        gal.set_zones(nstep, zbr)
+        # no particles: masset, steps and the zone report still work
+        gal.greenm()
+        gal.loadup(np.zeros((0, 4), np.float32))
+        gal.masset()
+        gal.step(3)
+        zone, istep = gal.zone_info()
+        assert zone.size == 0 and istep == 3
+        assert not np.any(gal.grid(GX_GRID_MASS))
+        # zones are set before the particles
+        gal.loadup(base_records(fx["records0"][:100], fx["zone0"][:100].astype(np.int32), nstep))
+        with pytest.raises(GxError):
+            gal.set_zones(nstep, zbr)
+    # not on the plain FP64 path
+    cfg64, _, _ = run100(fx)
+    cfg64.precision = GX_PREC_FP64
+    with Galaxy(cfg64) as gal:
+        with pytest.raises(GxError):
+            gal.set_zones(nstep, zbr)
+
+
+@pytest.mark.gpu
+def test_gpu_partial_grid_solves_give_the_whole_grid_trajectories(fx):
+    """on the steps where only zone 1 moves the field is synthesised over
+    zone 1's rings only (findf.f:41-54); every moving particle reads the
+    same field values as in the whole-grid solve, so the run is the same
+    bit for bit"""
+    from galaxy_b200 import GX_FLAG_WHOLE_GRID
+    cfg, nstep, zbr = run100(fx)
+    rec = base_records(fx["records0"], fx["zone0"].astype(np.int32), nstep)
+    out = []
+    for flags in (0, GX_FLAG_WHOLE_GRID):
+        cfg.flags = flags
+        with Galaxy(cfg) as gal:
+            gal.greenm()
+            gal.set_zones(nstep, zbr)
+            gal.loadup(rec)
+            gal.masset()
+            gal.step(301)
+            out.append((gal.unload(), gal.zone_info()[0], gal.grid(GX_GRID_MASS)))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+
+
+@pytest.mark.gpu
+def test_gpu_partial_grid_range_covers_the_moving_zone(fx):
+    """the field rings of a partial solve run from jrad(1) to krad(1): the
+    rings of zone 1's cells and their outer neighbours (massgn.f:75-76)"""
+    gal, nstep = gpu_run(fx)
+    nr = int(fx["nr"])
+    with gal:
+        src, fld = gal.zone_rings()
+        assert fld == (1, nr)  # step 0: both zones move
+        gal.step(1)
+        src, fld = gal.zone_rings()
+        rec = gal.unload()
+        zone, istep = gal.zone_info()
+    assert istep == 1
+    key, _, on = ox.weight(gal.cfg, rec, old=False, prec=32)
+    na = int(fx["na"])
+    ring = key // na
+    z1 = (zone == 1) & on.astype(bool)
+    assert fld == (int(ring[z1].min()) + 1, int(ring[z1].max()) + 2)
+    assert fld[1] < nr - 10  # narrower than the grid
+    # the sources span every zone's mass
+    assert 1 <= src[0] <= fld[0] and fld[1] < src[1] <= nr

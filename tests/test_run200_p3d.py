@@ -83,3 +83,24 @@ def test_run200_zoned_steps_track_the_oracle(gold):
     assert np.mean(d > 2e-5 * scale) < 2e-3 and d.max() / scale < 1e-3, (d.max() / scale)
     dv = np.abs(pos[:, 3:] - ref[:, 3:]).max(axis=1)
     assert np.median(dv) < 1e-5 * np.abs(ref[:, 3:]).max()
+
+
+@pytest.mark.gpu
+def test_run200_partial_grid_solves_give_the_whole_grid_trajectories(gold):
+    """3D: zones 1..m < 3 move on most steps and the field is synthesised over
+    their rings only (p3fndf.f:66-80); the run is the whole-grid run bit for bit"""
+    from galaxy_b200 import GX_FLAG_WHOLE_GRID
+    p, rec, pm = load(gold)
+    cfg, nstep, zbr = run200(gold, pm)
+    out = []
+    for flags in (0, GX_FLAG_WHOLE_GRID):
+        cfg.flags = flags
+        with Galaxy(cfg) as gal:
+            gal.greenm()
+            gal.set_zones(nstep, zbr)
+            gal.loadup(rec)
+            gal.masset()
+            gal.step(2 * max(nstep) + 1)
+            out.append((gal.unload(), gal.zone_info()[0]))
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1], out[1][1])
