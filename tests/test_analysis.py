@@ -9,7 +9,7 @@ import os
 import numpy as np
 import pytest
 
-from galaxy_b200 import Galaxy, make_config, GX_GRID_MASS, GX_RMAP_STDPOL
+from galaxy_b200 import Galaxy, make_config, GX_GRID_MASS, GX_RMAP_LOG, GX_RMAP_STDPOL
 from oracle import oracle as ox
 
 GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "run100_dmp.npz")
@@ -65,3 +65,71 @@ def test_gpu_danl_matches_oracle_on_the_reference_run():
     assert np.abs(got[0][:, 1:] - ref0[:, 1:]).max() < 1e-5
     # by step 3000 the bar mode dominates the inner rings' m = 2 harmonic
     assert np.abs(got[3000][:20, 2]).max() > 30 * np.abs(got[0][:20, 2]).max()
+
+
+def _icheck_ref(cfg, rec, acc, pot, tz, pm, halo_pot=None):
+    """the oracle's icheck of the on-grid particles with time-centred base-step
+    velocities v + a t / 2 (cencds.f:26-48); pe = pm (pot_grid / 2 + pot_halo)"""
+    nd = cfg.ndim
+    key, _, on = ox.weight(cfg, rec, old=False, prec=32)
+    on = on.astype(bool)
+    r = rec.astype(np.float64).copy()
+    r[:, nd:] += 0.5 * acc.astype(np.float64) * tz[:, None]
+    pg = pot.astype(np.float64) - (0 if halo_pot is None else halo_pot)
+    d = ox.icheck(cfg, r[on], acc[on], pg[on], pm)
+    if halo_pot is not None:
+        d.pe += pm * halo_pot[on].sum()
+    return d, int(on.sum())
+
+
+def _close(a, b, tol):
+    for f in ("ke", "pe", "lz", "virial", "a2_re", "a2_im"):
+        x, y = getattr(a, f), getattr(b, f)
+        assert abs(x - y) <= tol * max(abs(y), 1e-300), (f, x, y)
+
+
+@pytest.mark.gpu
+def test_gpu_icheck_matches_oracle_integrals():
+    """icheck.f:61-92 on a 3D disc with a rigid halo: energies, Lz, virial,
+    A2 and the on-grid count against the oracle on the same accelerations"""
+    from galaxy_b200.disk import kt_disk
+    nr = 32
+    cfg = make_config(3, nr, 64, ngz=15, dzg=0.1, ng=9, rmap=GX_RMAP_LOG, rmap_a=float(np.log(100.0) / (nr - 1)),
+                      rmap_r0=0.05, softl=0.2, tsoft=1, pmass=1.0)
+    rec, pm = kt_disk(100000, seed=4, rmax=6.0, ndim=3, z0=0.1, dt=0.025)  # some off the grid
+    cfg.pmass = pm
+    with Galaxy(cfg) as gal:
+        gal.greenm()
+        gal.loadup(rec)
+        gal.masset()
+        gal.findf(True)
+        acc, pot = gal.getacc(want_pot=True)
+        d = gal.icheck()
+    ref, non = _icheck_ref(cfg, rec, acc, pot, np.ones(len(rec)), np.float32(pm))
+    assert d.n_on_grid == non and 0 < non < len(rec)
+    _close(d, ref, 1e-6)
+
+
+@pytest.mark.gpu
+def test_gpu_icheck_with_zones_on_the_reference_run():
+    """run100 at step 0: each zone's velocities time-centred with its own
+    step, the analytic disc's potential added in full"""
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    from test_run100_zones import gpu_run
+    fx = dict(np.load(GOLD))
+    gal, nstep = gpu_run(fx)
+    with gal:
+        gal.findf(True)
+        acc, pot = gal.getacc(want_pot=True)
+        d = gal.icheck()
+        rec = gal.unload()
+        zone, _ = gal.zone_info()
+        cfg = gal.cfg
+    # the softened Kuz'min-Toomre disc's potential, -K / sqrt(r^2 + Rs^2)
+    r2 = rec[:, 0].astype(np.float64) ** 2 + rec[:, 1].astype(np.float64) ** 2
+    hp = -np.float64(np.float32(cfg.halo_v2)) / np.sqrt(r2 + np.float64(np.float32(cfg.halo_rc)) ** 2)
+    tz = np.asarray(nstep, np.float64)[np.minimum(zone, 2) - 1]
+    ref, non = _icheck_ref(cfg, rec, acc, pot, tz, np.float32(cfg.pmass), halo_pot=hp)
+    assert d.n_on_grid == non
+    _close(d, ref, 2e-6)
