@@ -223,6 +223,15 @@ int gx_grdset(const GxConfig* cfg, GxCtx** out) {
         return GX_ERR_CUDA;
     }
     rc = alloc_grids(c);
+    if (rc == GX_OK) {
+        // the active harmonics, once per context (the kernels read them through DevGeo)
+        if (cudaMalloc((void**)&c->act_d, sizeof(int) * 260) != cudaSuccess ||
+            cudaMemcpy(c->act_d, c->spec.m, sizeof(int) * 260, cudaMemcpyHostToDevice) != cudaSuccess) {
+            c->err = "cudaMalloc of the harmonic list failed";
+            rc = GX_ERR_NOMEM;
+        }
+        c->g.act = c->act_d;
+    }
     if (rc) {
         g_last_err = c->err;
         gx_destroy(c);
@@ -242,7 +251,7 @@ void gx_destroy(GxCtx* c) {
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
                     c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->perm_next, c->rowstart,
                     c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->rowtile, c->stage, c->jrk_d,
-                    c->errword, c->dsum, c->pzone[0], c->pzone[1], c->zbuf, c->zjrk_d};
+                    c->errword, c->dsum, c->pzone[0], c->pzone[1], c->zbuf, c->zjrk_d, c->act_d};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i <= GX_NPHASE; i++)

@@ -36,6 +36,7 @@ struct DevGeo {
     int quad;       // 27-point quadratic interpolation (p3d jmass = 3)
     float halo_v2, halo_rc2;
     float pmass;
+    const int* act;  // [nact] m of each active harmonic (device, per context)
     // FP64 copies for the plain FP64 path
     double ua_d, uoffs_d, rinh_d, rgrid_d, zm_d, thmax_d, dzg_d, halo_v2_d, halo_rc2_d;
 };
@@ -95,6 +96,7 @@ struct GxCtx {
 
     // grids
     float* mass = nullptr;                 // [mesh] scaled mass (mixed)
+    int* act_d = nullptr;                  // [260] active harmonics (DevGeo::act)
     double* mass64 = nullptr;              // [mesh] (FP64 path)
     float4* field = nullptr;               // [mesh] (fx, fy, fz, pot) mixed
     float* polar = nullptr;                // [4][mesh] polar fields (fr, ft, fz, pot)
@@ -191,6 +193,14 @@ int gx_phase_end(GxCtx* c);
 // (correctly rounded log, FP64 atan2), so the integer cell indices agree
 // with the reference's wherever its own libm calls are correctly rounded.
 
+// ND = 2 or 3 fixes the dimension at compile time (the particle pass is
+// instantiated per dimension, so that its corner loop unrolls and its
+// eight gathers are issued together); ND = 0 reads it from the geometry
+template <int ND>
+__device__ __forceinline__ bool gx_is3(const DevGeo& g) {
+    return ND == 0 ? g.ndim == 3 : ND == 3;
+}
+
 struct CellW {
     int key;      // ncl - 1, or -1 when off the grid / in the hole
     float du, dt, dz;  // fractions in the cell; quadratic: coord + 1/2 - index
@@ -229,6 +239,35 @@ __device__ __forceinline__ float gx_t_exact(const DevGeo& g, float x, float y) {
     return tf;
 }
 
+// atan2 for the fast cell estimate: octant reduction to q = min/max in
+// [0, 1], atan(q) = q P(q^2) with an 8-term odd minimax polynomial (own
+// Remez-exchange fit on [0, 1], 3.7e-8 absolute), then atan(y/x) =
+// pi/2 - atan(x/y) above the diagonal and the quadrant from the signs.
+// Absolute error about 4e-7 over the plane in FP32 (the final rounding near
+// pi and the approximate reciprocal dominate), the same class as the
+// library atan2f; gx_cell's guard band (4e-6 (na + 1) spokes, 2.5e-5 rad)
+// covers it with a margin of 60.
+__device__ __forceinline__ float gx_atan2_fast(float y, float x) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    const float mx = fmaxf(ax, ay), mn = fminf(ax, ay);
+    float rc;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(rc) : "f"(fmaxf(mx, 1e-30f)));
+    const float q = mn * rc;
+    const float s = q * q;
+    float p = -4.054567311e-03f;
+    p = fmaf(p, s, 2.186295763e-02f);
+    p = fmaf(p, s, -5.591232702e-02f);
+    p = fmaf(p, s, 9.642197192e-02f);
+    p = fmaf(p, s, -1.390862912e-01f);
+    p = fmaf(p, s, 1.994656622e-01f);
+    p = fmaf(p, s, -3.332985938e-01f);
+    p = fmaf(p, s, 9.999993443e-01f);
+    p *= q;
+    float r = (ay > ax) ? 1.570796327f - p : p;
+    r = (x < 0.f) ? 3.141592654f - r : r;
+    return (y < 0.f) ? -r : r;
+}
+
 __device__ __forceinline__ bool gx_near_int(float v, float eps) {
     float f;
     gx_trunc(v, f);
@@ -264,15 +303,22 @@ __device__ __forceinline__ CellW gx_cell27(const DevGeo& g, float u, float t, fl
 // reference's for a coordinate within a few ulp of a cell boundary, where
 // the interpolated field is continuous (the particle pass's interpolation
 // cell); keys that are deposited or reported use the exact form.
-template <bool EXACT>
+template <bool EXACT, int ND = 0>
 __device__ __forceinline__ CellW gx_cell_t(const DevGeo& g, float x, float y, float z, bool old) {
     CellW c;
     c.key = -1;
     c.du = c.dt = c.dz = 0.f;
     c.row = c.jt = 0;
-    float rr = __fsqrt_rn(__fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y)));
+    const float r2 = __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
+    float rr;
+    if (EXACT) {
+        rr = __fsqrt_rn(r2);
+    } else {
+        // the interpolation cell needs no correctly rounded radius
+        asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(rr) : "f"(r2));
+    }
     if (rr > g.rgrid) return c;
-    if (g.ndim == 3 && fabsf(z) > g.zm) return c;
+    if (gx_is3<ND>(g) && fabsf(z) > g.zm) return c;
     if (rr < g.rinh) return c;
     // u (fast path + guard)
     float u;
@@ -287,8 +333,8 @@ __device__ __forceinline__ CellW gx_cell_t(const DevGeo& g, float x, float y, fl
     }
     // t
     float t;
-    if (g.ndim == 2 || rr > 0.f) {
-        t = atan2f(y, x) * g.t_scale;
+    if (!gx_is3<ND>(g) || rr > 0.f) {
+        t = gx_atan2_fast(y, x) * g.t_scale;
         if (t < 0.f) t += g.fna;
         const float eps = g.eps_t;
         if (EXACT && (gx_near_int(t + sh, eps) || t < eps || t > g.fna - eps)) t = gx_t_exact(g, x, y);
@@ -303,7 +349,7 @@ __device__ __forceinline__ CellW gx_cell_t(const DevGeo& g, float x, float y, fl
         c.du = u - gx_i2f(ju);
     }
     const int jt = gx_trunc(t, c.dt);
-    if (g.ndim == 2) {
+    if (!gx_is3<ND>(g)) {
         c.row = ju;
     } else {
         float zz = (z + g.zm) * g.inv_dzg;
@@ -344,8 +390,9 @@ __device__ __forceinline__ void gx_comp_add(float& hi, float& lo, float v) {
 }
 
 // 8 (3D) or 4 (2D) weights in the reference order (weight.f:92-99, 241-248)
+template <int ND = 0>
 __device__ __forceinline__ void gx_weights(const DevGeo& g, const CellW& c, float* w) {
-    if (g.ndim == 2) {
+    if (!gx_is3<ND>(g)) {
         float dd = c.du * c.dt;
         w[0] = 1.f - c.du - c.dt + dd;
         w[1] = c.dt - dd;
@@ -422,6 +469,7 @@ __device__ __forceinline__ void gx_corners27(const DevGeo& g, int row, int r, in
             }
 }
 
+template <int ND = 0>
 __device__ __forceinline__ int gx_corners_rt(const DevGeo& g, int key, int jt, int* ic) {
     const int na = g.na;
     const int end = (jt == na - 1);
@@ -429,7 +477,7 @@ __device__ __forceinline__ int gx_corners_rt(const DevGeo& g, int key, int jt, i
     ic[1] = key + 1 - (end ? na : 0);
     ic[2] = key + na;
     ic[3] = ic[1] + na;
-    if (g.ndim == 2) {
+    if (!gx_is3<ND>(g)) {
 #pragma unroll
         for (int k = 0; k < 4; k++)
             if (ic[k] >= g.mesh) ic[k] = -1;
@@ -489,7 +537,7 @@ __device__ __forceinline__ void gx_disc_force(const DevGeo& g, float x, float y,
 
 // interpolated acceleration and potential of a particle at (x, y, z) whose
 // interpolation cell is cw: grdacc + halfrc (or the fixed disc force)
-template <bool Q>
+template <bool Q, int ND = 0>
 __device__ __forceinline__ void gx_accel_cell_t(const DevGeo& g, const float4* __restrict__ F,
                                                 const CellW& cw, float x, float y, float z,
                                                 float& ax, float& ay, float& az, float& ph) {
@@ -511,6 +559,22 @@ __device__ __forceinline__ void gx_accel_cell_t(const DevGeo& g, const float4* _
             ay += f.y * w[k];
             az += f.z * w[k];
             ph += f.w * w[k];
+        }
+    } else if constexpr (ND != 0) {
+        constexpr int NC = (ND == 3) ? 8 : 4;
+        float w[8];
+        int ic[8];
+        gx_weights<ND>(g, cw, w);
+        gx_corners_rt<ND>(g, cw.key, cw.jt, ic);
+        float4 f[NC];
+#pragma unroll
+        for (int k = 0; k < NC; k++) f[k] = (ic[k] >= 0) ? __ldg(F + ic[k]) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+        for (int k = 0; k < NC; k++) {
+            ax += f[k].x * w[k];
+            ay += f[k].y * w[k];
+            az += f[k].z * w[k];
+            ph += f[k].w * w[k];
         }
     } else {
         float w[8];

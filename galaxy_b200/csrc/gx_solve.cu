@@ -20,7 +20,6 @@
 
 #include "gx_common.cuh"
 
-__constant__ int c_act_m[260];
 
 __host__ __device__ static inline int ru4(int x) { return (x + 3) & ~3; }
 
@@ -56,12 +55,12 @@ __device__ __forceinline__ void sgemm44(int M, int N, int K, const float* A, int
 }
 
 // forward azimuthal twiddles T[j][2a] = cos(2 pi m_a j / na), T[j][2a+1] = -sin(...)
-__device__ void build_taz(float* T, int na, int nact, int ncp) {
+__device__ void build_taz(float* T, const int* __restrict__ act, int na, int nact, int ncp) {
     for (int i = threadIdx.x; i < na * ncp; i += blockDim.x) {
         int j = i / ncp, c = i - j * ncp;
         float v = 0.f;
         if (c < 2 * nact) {
-            int m = c_act_m[c >> 1];
+            int m = act[c >> 1];
             int idx = (int)(((int64_t)m * j) % na);
             float s, co;
             sincospif(2.0f * (float)idx / (float)na, &s, &co);
@@ -124,7 +123,7 @@ __global__ void k_fwdtab(DevGeo g, int nact, int ncp, float* __restrict__ Taz, f
         const int j = i / ncp, c = i - j * ncp;
         float v = 0.f;
         if (c < 2 * nact) {
-            const int m = c_act_m[c >> 1];
+            const int m = g.act[c >> 1];
             const int idx = (int)(((int64_t)m * j) % na);
             float sn, co;
             sincospif(2.0f * (float)idx / (float)na, &sn, &co);
@@ -207,7 +206,7 @@ __global__ void __launch_bounds__(288) k_fwd_az(DevGeo g, int ncp, const int32_t
                 make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
         }
     });
-    if (c_act_m[0] == 0) {
+    if (g.act[0] == 0) {
         __syncthreads();  // column 0 of the GEMM is written before the FP64 sum replaces it
         // 8 lanes per row, FP64 partial sums over na / 8 points each
         const int r = threadIdx.x >> 3, q = threadIdx.x & 7;
@@ -310,7 +309,7 @@ __global__ void k_fwd2(DevGeo g, int nact, int ncp, const float* __restrict__ ma
         int ir = ir0 + r;
         X[r * ldx + j] = (ir <= jr1) ? mass[(size_t)ir * na + j] : 0.f;
     }
-    build_taz(T, na, nact, ncp);
+    build_taz(T, g.act, na, nact, ncp);
     __syncthreads();
     sgemm44(RB2, ncp, na, X, ldx, T, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
 #pragma unroll
@@ -318,7 +317,7 @@ __global__ void k_fwd2(DevGeo g, int nact, int ncp, const float* __restrict__ ma
             int ir = ir0 + r0 + i;
             if (ir > jr1) continue;
             double s0 = 0.0;
-            bool m0 = (c0 == 0) && (c_act_m[0] == 0);
+            bool m0 = (c0 == 0) && (g.act[0] == 0);
             if (m0)
                 for (int j = 0; j < na; j++) s0 += (double)X[(r0 + i) * ldx + j];
 #pragma unroll
@@ -345,7 +344,7 @@ __global__ void __launch_bounds__(256) k_conv(DevGeo g, int nact, int tmask,
     const int nr = g.nr, nkz = g.nkz, ng = g.ng, mmax = g.mmax, ngz = g.ngz;
     // source rings jrs..krs (p3conv.f:149-150)
     const int js = max(jrk[0], 1) - 1, ks = min(jrk[1], nr) - 1;
-    const int a = blockIdx.x, k = blockIdx.y, m = c_act_m[a];
+    const int a = blockIdx.x, k = blockIdx.y, m = g.act[a];
     float4* Sin = sh4;              // [nr]
     float4* part = sh4 + nr;        // [8][nr]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -420,20 +419,13 @@ bool gx_conv_bulk_ok(const DevGeo& g);
 int gx_conv_bulk(GxCtx* c, int nact, int tmask);
 
 // ---------------------------------------------------------------------------
-static int set_act(GxCtx* c) {
-    GX_CUDA(c, cudaMemcpyToSymbolAsync(c_act_m, c->spec.m, sizeof(int) * 260, 0,
-                                       cudaMemcpyHostToDevice, c->stream));
-    return GX_OK;
-}
-
 // findf for the mixed path: mass -> field (and optional polar copy)
 int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* frk) {
     const DevGeo& g = c->g;
     const int nact = c->spec.nact;
     if (nact == 0) return c->err = "no active harmonics", GX_ERR_ARG;
     const int ncp = ru4(2 * nact);
-    int rc = set_act(c);
-    if (rc) return rc;
+    int rc = GX_OK;
     float* polar = nullptr;
     if (!polcat_only_field) {
         if (!c->polar) GX_CUDA(c, cudaMalloc((void**)&c->polar, sizeof(float) * 4 * g.mesh));

@@ -32,7 +32,7 @@ __device__ __forceinline__ void gx_accel(const DevGeo& g, const float4* __restri
 // the fused particle pass of one step: the interpolation cell of the
 // current position, the move, the key and fractions of the new cell,
 // counted by row for the deposit's counting sort.
-template <bool Q>
+template <bool Q, int ND>
 __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict__ Pin,
                                               float* __restrict__ Pout, int64_t cap, int64_t n,
                                               const int32_t* __restrict__ perm,
@@ -48,7 +48,7 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
     uint32_t row = 0;
     if (act) {
         const int p = perm[s];
-        const bool d3 = g.ndim == 3;
+        constexpr bool d3 = ND == 3;
         float x = Pin[p], y = Pin[cap + p], z = 0.f, vx, vy, vz = 0.f;
         if (d3) {
             z = Pin[2 * cap + p];
@@ -60,9 +60,9 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
             vy = Pin[3 * cap + p];
         }
         const int32_t o = orig_in[p];
-        const CellW cw = gx_cell_t<false>(g, x, y, z, true);
+        const CellW cw = gx_cell_t<false, ND>(g, x, y, z, true);
         float ax, ay, az, ph;
-        gx_accel_cell_t<Q>(g, F, cw, x, y, z, ax, ay, az, ph);
+        gx_accel_cell_t<Q, ND>(g, F, cw, x, y, z, ax, ay, az, ph);
         vx += ax;
         vy += ay;
         if (d3) vz += az;
@@ -97,7 +97,7 @@ __global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict_
         }
         orig_out[s] = o;
         if (pot) pot[s] = ph;
-        const CellW cn = gx_cell(g, x, y, z, false);
+        const CellW cn = gx_cell_t<true, ND>(g, x, y, z, false);
         key_out[s] = cn.key;
         fr_out[s] = cn.du;
         fr_out[cap + s] = cn.dt;
@@ -136,7 +136,7 @@ int gx_mixed_step(GxCtx* c, int nsteps, int phys) {
         rc = gx_phase_mark(c, PH_PUSH);
         if (rc) return rc;
         if (n > 0) {
-            auto kp = g.quad ? k_push<true> : k_push<false>;
+            auto kp = g.quad ? k_push<true, 3> : (g.ndim == 3) ? k_push<false, 3> : k_push<false, 2>;
             kp<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(
                 g, c->pbuf[c->cur], c->pbuf[nxt], c->cap, n, c->perm, c->origin, c->origin_tmp,
                 c->field, c->pkey[nxt], c->pfr, c->rowcnt,
