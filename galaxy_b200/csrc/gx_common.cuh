@@ -14,7 +14,7 @@
 
 // ---------------------------------------------------------------------------
 // particles per deposit work item (bounds the fixed-point bin sums)
-#define DEP_CH 1024
+#define DEP_CH 2047  // particles per deposit item (int32 bins: see gx_deposit.cu)
 // striped copies of the row counters (copy = block index mod NCOPY); spreads
 // the integer atomics of row-sorted particles over NCOPY addresses per row
 #define NCOPY 32

@@ -18,9 +18,12 @@
 //
 // Every sum is an integer sum, so the mass array is bitwise reproducible
 // whatever order the atomics resolve in; no floating-point atomics are used.
-// The fixed-point quantum is 2^-20 of one particle's mass (9.5e-7); a bin
-// holds at most DEP_CH (1 + 1e-6) 2^20 < 2^31 (each particle feeds one bin
-// per (output row, weight)), so int32 never overflows.
+// The fixed-point quantum is 2^-20 of one particle's mass (9.5e-7).  Each
+// particle feeds one bin per (output row, weight) and one weight to a staged
+// cell, and every weight is below 1 + 1e-4 in magnitude (the linear weights
+// lie in [0, 1] up to rounding; the quadratic ones reach -0.5 and 0.95 at
+// the clamped rings), so a bin or staged cell holds less than
+// DEP_CH (1 + 1e-4) 2^20 < 2^31 with DEP_CH = 2047: int32 never overflows.
 #include <algorithm>
 
 #include "gx_common.cuh"
@@ -268,35 +271,37 @@ __global__ void __launch_bounds__(256) k_deposit(DevGeo g, const int32_t* __rest
         const int row = items[3 * item], s0 = items[3 * item + 1], s1 = items[3 * item + 2];
         for (int i = threadIdx.x; i < NW * na; i += blockDim.x) bins[i] = 0;
         __syncthreads();
-        // an item holds at most DEP_CH = 4 x 256 particles: each thread loads
-        // its four together, then adds them
-        static_assert(DEP_CH <= 4 * 256, "four particles per thread");
-        CellW cw[4];
+        // an item holds at most DEP_CH < 8 x 256 particles: each thread loads
+        // four together, adds them, then the next four
+        static_assert(DEP_CH <= 8 * 256, "eight particles per thread");
+        for (int s00 = s0; s00 < s1; s00 += 1024) {
+            CellW cw[4];
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int s = s0 + threadIdx.x + u * 256;
-            cw[u].key = -2;
-            if (s < s1) {
-                const int p = __ldg(perm + s);
-                cw[u].key = __ldg(keys + p);
-                cw[u].du = __ldg(fr + p);
-                cw[u].dt = __ldg(fr + cap + p);
-                cw[u].dz = (NW >= 8) ? __ldg(fr + 2 * cap + p) : 0.f;
+            for (int u = 0; u < 4; u++) {
+                const int s = s00 + threadIdx.x + u * 256;
+                cw[u].key = -2;
+                if (s < s1) {
+                    const int p = __ldg(perm + s);
+                    cw[u].key = __ldg(keys + p);
+                    cw[u].du = __ldg(fr + p);
+                    cw[u].dt = __ldg(fr + cap + p);
+                    cw[u].dz = (NW >= 8) ? __ldg(fr + 2 * cap + p) : 0.f;
+                }
             }
-        }
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            if (cw[u].key == -2) continue;
-            int jt;
-            if (cw[u].key < 0 || gx_div_na(g, cw[u].key, jt) != row) {
-                atomicExch(errword, 1);
-                continue;
+            for (int u = 0; u < 4; u++) {
+                if (cw[u].key == -2) continue;
+                int jt;
+                if (cw[u].key < 0 || gx_div_na(g, cw[u].key, jt) != row) {
+                    atomicExch(errword, 1);
+                    continue;
+                }
+                float w[NW == 27 ? 27 : 8];
+                if constexpr (NW == 27) gx_weights27(cw[u], w);
+                else gx_weights<(NW == 8) ? 3 : 2>(g, cw[u], w);
+#pragma unroll
+                for (int k = 0; k < NW; k++) atomicAdd(&bins[k * na + jt], __float2int_rn(w[k] * FIXQ));
             }
-            float w[NW == 27 ? 27 : 8];
-            if constexpr (NW == 27) gx_weights27(cw[u], w);
-            else gx_weights(g, cw[u], w);
-#pragma unroll
-            for (int k = 0; k < NW; k++) atomicAdd(&bins[k * na + jt], __float2int_rn(w[k] * FIXQ));
         }
         __syncthreads();
         int32_t* dst = stage + (size_t)item * NQ * na;
