@@ -32,8 +32,11 @@ __device__ __forceinline__ void gx_accel(const DevGeo& g, const float4* __restri
 // the fused particle pass of one step: the interpolation cell of the
 // current position, the move, the key and fractions of the new cell,
 // counted by row for the deposit's counting sort.
+// Eight CTAs per SM (32 registers; four for the 27-point pass, which would
+// spill): the pass waits on its gathers, and the extra resident warps hide
+// more of that latency than the capped registers cost.
 template <bool Q, int ND>
-__global__ void __launch_bounds__(256) k_push(DevGeo g, const float* __restrict__ Pin,
+__global__ void __launch_bounds__(256, Q ? 4 : 8) k_push(DevGeo g, const float* __restrict__ Pin,
                                               float* __restrict__ Pout, int64_t cap, int64_t n,
                                               const int32_t* __restrict__ perm,
                                               const int32_t* __restrict__ orig_in,
