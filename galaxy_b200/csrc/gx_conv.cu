@@ -197,34 +197,44 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB) k_conv_bulk(ConvArgs A) 
                     continue;
                 }
                 const float* st = stage + s * stage_floats;
-#pragma unroll 2
-                for (int r = warp; r < rows; r += NCW) {
-                    const float4 sv = Sb[r0 + r];
+                // this warp's rows of the tile (warp, warp + NCW, ...) into
+                // registers first, so that the stage goes back to the
+                // producer before the arithmetic: more of the table stays in
+                // flight while the sums run
+                static_assert(NJ == 1, "one group of 128 output rings per lane");
+                constexpr int RW = 128 / NCW;  // rows per warp at most (R <= 128)
+                float4 gr[RW];
 #pragma unroll
-                    for (int j = 0; j < NJ; j++) {
-                        const int ir0 = 4 * lane + 128 * j;
-                        if (ir0 >= nr) continue;
-                        const float4 g4 = *reinterpret_cast<const float4*>(st + (size_t)r * nr + ir0);
-                        const float gv[4] = {g4.x, g4.y, g4.z, g4.w};
-#pragma unroll
-                        for (int q = 0; q < 4; q++) {
-                            const float gq = gv[q];
-                            float4& o = acc[j][q];
-                            if (t == 0 || t == 3) {
-                                o.x += gq * sv.x; o.y += gq * sv.y;
-                                o.z += gq * sv.z; o.w += gq * sv.w;
-                            } else if (t == 1) {
-                                o.x += gq * sv.z; o.z -= gq * sv.x;
-                                o.y += gq * sv.w; o.w -= gq * sv.y;
-                            } else {
-                                o.x += gq * sv.y; o.y -= gq * sv.x;
-                                o.z += gq * sv.w; o.w -= gq * sv.z;
-                            }
-                        }
-                    }
+                for (int u = 0; u < RW; u++) {
+                    const int r = warp + NCW * u;
+                    gr[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (r < rows && 4 * lane < nr)
+                        gr[u] = *reinterpret_cast<const float4*>(st + (size_t)r * nr + 4 * lane);
                 }
                 __syncwarp();
                 if (lane == 0) mbar_arrive(&empty[s]);
+#pragma unroll
+                for (int u = 0; u < RW; u++) {
+                    const int r = warp + NCW * u;
+                    if (r >= rows) break;
+                    const float4 sv = Sb[r0 + r];
+                    const float gv[4] = {gr[u].x, gr[u].y, gr[u].z, gr[u].w};
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        const float gq = gv[q];
+                        float4& o = acc[0][q];
+                        if (t == 0 || t == 3) {
+                            o.x += gq * sv.x; o.y += gq * sv.y;
+                            o.z += gq * sv.z; o.w += gq * sv.w;
+                        } else if (t == 1) {
+                            o.x += gq * sv.z; o.z -= gq * sv.x;
+                            o.y += gq * sv.w; o.w -= gq * sv.y;
+                        } else {
+                            o.x += gq * sv.y; o.y -= gq * sv.x;
+                            o.z += gq * sv.w; o.w -= gq * sv.z;
+                        }
+                    }
+                }
             }
 #pragma unroll
             for (int j = 0; j < NJ; j++) {
