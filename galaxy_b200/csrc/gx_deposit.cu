@@ -421,7 +421,7 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
     if (rc) return rc;
     const int nw = g.quad ? 27 : (g.ndim == 3) ? 8 : 4;
     const size_t sm = sizeof(int32_t) * (size_t)nw * g.na;
-    const int grid = std::min(c->maxitems, 148 * 16);
+    const int grid = std::min(c->maxitems, 148 * 32);  // ~4 items per CTA at 10M particles
     if (nw == 27) {
         static bool attr = false;  // 27 x 512 spokes of bins exceed the default 48 KB
         if (!attr) {
