@@ -423,12 +423,10 @@ int gx_deposit_rows(GxCtx* c, const int32_t* keys, const float* fr, int32_t* per
     const size_t sm = sizeof(int32_t) * (size_t)nw * g.na;
     const int grid = std::min(c->maxitems, 148 * 32);  // ~4 items per CTA at 10M particles
     if (nw == 27) {
-        static bool attr = false;  // 27 x 512 spokes of bins exceed the default 48 KB
-        if (!attr) {
-            GX_CUDA(c, cudaFuncSetAttribute(k_deposit<27>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)(sizeof(int32_t) * 27 * 512)));
-            attr = true;
-        }
+        // 27 rows of bins of up to 512 spokes exceed the default 48 KB (the
+        // attribute belongs to the calling thread's current device)
+        GX_CUDA(c, cudaFuncSetAttribute(k_deposit<27>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)(sizeof(int32_t) * 27 * 512)));
         k_deposit<27><<<grid, 256, sm, c->stream>>>(g, c->items, c->nitems_d, keys, fr, c->cap,
                                                     perm_out, c->stage, c->errword);
     } else if (nw == 8)
