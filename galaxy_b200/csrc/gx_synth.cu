@@ -262,8 +262,11 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
 }
 
 #define SYN_ZB 16
+// 288 threads: the SYN_ZB x njp / 4 (plane, 4-spoke) items of a CTA (528 at
+// 256 spokes) take two passes instead of two and a sliver
+#define SYNAZ_THREADS 288
 // azimuthal synthesis + polcat, one CTA per (ring, SYN_ZB planes)
-__global__ void __launch_bounds__(256) k_synaz(DevGeo g, int nact, int ncp, int tmask,
+__global__ void __launch_bounds__(SYNAZ_THREADS) k_synaz(DevGeo g, int nact, int ncp, int tmask,
                                               const float* __restrict__ R, SynTab tb,
                                               float4* __restrict__ F, float* __restrict__ polar,
                                               const int32_t* __restrict__ frk) {
@@ -405,7 +408,7 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk) {
         const size_t sm = sizeof(float) * (2 * nT + 2 * (size_t)njp + (size_t)4 * SYN_ZB * ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_synaz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         dim3 grid(g.nr, (g.ngz + SYN_ZB - 1) / SYN_ZB);
-        k_synaz<<<grid, 256, sm, c->stream>>>(g, nact, ncp, tmask, c->synR, tb, c->field, polar, frk);
+        k_synaz<<<grid, SYNAZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->synR, tb, c->field, polar, frk);
         GX_LAUNCHED(c);
     }
     return GX_OK;
