@@ -224,3 +224,25 @@ def test_gpu_quadratic_keys_with_sectors_and_an_empty_deposit():
         gal.loadup(np.zeros((0, 6), np.float32))
         gal.masset()
         assert not np.any(gal.grid(GX_GRID_MASS))
+
+
+@pytest.mark.gpu
+def test_gpu_quadratic_at_the_largest_spoke_count():
+    """na = 512, the largest spoke count: 27 rows of 512 fixed-point bins
+    (55 KB of shared memory per deposit CTA) and the 27-point gather"""
+    nr = 24
+    cfg = make_config(3, nr, 512, ngz=15, dzg=0.1, ng=5, rmap=GX_RMAP_LOG,
+                      rmap_a=float(np.log(100.0) / (nr - 1)), rmap_r0=0.05, softl=0.2,
+                      tsoft=1, pmass=1.0, flags=GX_FLAG_QUADRATIC)
+    rec, pm = disk(60000, seed=5)
+    cfg.pmass = pm
+    ref, _ = ox.masset(cfg, rec.astype(np.float64), prec=64)
+    okey, _, oon = ox.weight(cfg, rec, old=False, prec=32)
+    with Galaxy(cfg) as gal:
+        key, _ = gal.weight(rec, old=False)
+        gal.loadup(rec)
+        gal.masset()
+        m = gal.grid(GX_GRID_MASS).astype(np.float64)
+    assert np.array_equal(key, np.where(oon, okey, -1))
+    assert abs(m.sum() - ref.sum()) / ref.sum() < 1e-6
+    assert np.abs(m - ref).max() / ref.max() < 2e-6
