@@ -229,7 +229,9 @@ def test_gpu_quadratic_keys_with_sectors_and_an_empty_deposit():
 @pytest.mark.gpu
 def test_gpu_quadratic_at_the_largest_spoke_count():
     """na = 512, the largest spoke count: 27 rows of 512 fixed-point bins
-    (55 KB of shared memory per deposit CTA) and the 27-point gather"""
+    (55 KB of shared memory per deposit CTA) and the 27-point gather.  The
+    FP32 spoke coordinate resolves 6e-5 spokes near 512 (its ulp), so the
+    masses are compared per cell in units of one particle's mass."""
     nr = 24
     cfg = make_config(3, nr, 512, ngz=15, dzg=0.1, ng=5, rmap=GX_RMAP_LOG,
                       rmap_a=float(np.log(100.0) / (nr - 1)), rmap_r0=0.05, softl=0.2,
@@ -245,4 +247,4 @@ def test_gpu_quadratic_at_the_largest_spoke_count():
         m = gal.grid(GX_GRID_MASS).astype(np.float64)
     assert np.array_equal(key, np.where(oon, okey, -1))
     assert abs(m.sum() - ref.sum()) / ref.sum() < 1e-6
-    assert np.abs(m - ref).max() / ref.max() < 2e-6
+    assert np.abs(m - ref).max() < 5e-4 * pm
