@@ -261,6 +261,222 @@ __global__ void __launch_bounds__(SYNZ_THREADS) k_synz(DevGeo g, int nact, int n
     }
 }
 
+// ---------------------------------------------------------------------------
+// The same vertical synthesis on the tensor cores, persistent: P and Q are
+// two small GEMMs per (ring, type), P = WAe^T Ae + WBo^T Bo and
+// Q = WBe^T Be + WAo^T Ao (M = planes, N = columns, K = wavenumbers of one
+// parity), computed with mma.sync m16n8k8 TF32 and three products per
+// operand split x = hi + lo (hi = x rounded to TF32): lo hi + hi lo + hi hi
+// with FP32 accumulation, so the result keeps FP32-class accuracy.  One CTA
+// per SM loads the four twiddle tables once, split into their TF32 hi and
+// lo parts ([i][64] each, the planes of row i stored at z ^ 8 (i & 3); 200 KB
+// of shared memory with the spectrum), and walks its (ring, type) items; the spectrum of
+// the next item is loaded into registers while the tensor cores work on the
+// current one, then written to the [i][72] spectrum buffer.  Both layouts
+// give bank-conflict-free fragment loads.  Warp w owns columns 8w .. 8w + 7.
+#define SZT_K 64    // wavenumbers of one parity at most (KE, KO <= 64)
+#define SZT_SS 72   // spectrum row stride: columns (ncp <= 72, 9 warps x 8)
+#define SZT_PF 8    // spectrum float4 prefetched per thread (nkz nact <= 8 x 288)
+__device__ __forceinline__ uint32_t syn_tf32(float v) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+    return r & 0xffffe000u;
+}
+__device__ __forceinline__ void syn_mma(float* d, const uint32_t* a, const uint32_t* b) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+__device__ __forceinline__ void syn_split(float v, uint32_t& hi, uint32_t& lo) {
+    hi = syn_tf32(v);
+    lo = syn_tf32(v - __uint_as_float(hi));
+}
+
+static bool gx_synz_tc_ok(const DevGeo& g, int nact, int ncp) {
+    int Z0, KE, KO, njp;
+    syn_dims(g, Z0, KE, KO, njp);
+    return g.ndim == 3 && Z0 <= 64 && KE <= SZT_K && KO <= SZT_K && ncp <= SZT_SS &&
+           g.nkz * nact <= SZT_PF * SYNZ_THREADS;
+}
+
+// item it of a CTA's walk: (type, ring) with the type's bit in tmask and the
+// ring inside the partial-grid range; false for items to skip
+__device__ __forceinline__ bool szt_item(const DevGeo& g, int it, int tmask, const int32_t* frk,
+                                         int& t, int& ir) {
+    t = it / g.nr;
+    ir = it - t * g.nr;
+    if (!((tmask >> t) & 1)) return false;
+    if (frk && (ir + 1 < frk[0] || ir + 1 > frk[1])) return false;
+    return true;
+}
+
+__global__ void __launch_bounds__(SYNZ_THREADS, 1) k_synz_tc(DevGeo g, int nact, int ncp, int tmask,
+                                                             const float4* __restrict__ O, SynTab tb,
+                                                             float* __restrict__ R,
+                                                             const int32_t* __restrict__ frk) {
+    extern __shared__ __align__(16) float sm[];
+    const int nr = g.nr, nkz = g.nkz, ngz = g.ngz;
+    const int Z0 = tb.Z0, KE = tb.KE, KO = tb.KO, nz4 = ru4s(Z0);
+    const int kte = (KE + 7) >> 3, kto = (KO + 7) >> 3;  // k-steps of 8 per parity
+    const int nitems = 4 * nr, nsp = nkz * nact;
+    uint32_t* sWh = reinterpret_cast<uint32_t*>(sm);  // [4][SZT_K][64]: WAe, WBe, WAo, WBo, TF32 hi
+    uint32_t* sWl = sWh + 4 * SZT_K * 64;              // the same, lo = W - hi in TF32
+    float* sS = sm + 8 * SZT_K * 64;                   // [4][SZT_K][SZT_SS]: Ae, Be, Ao, Bo
+    {
+        // twiddle tables once per CTA, split into TF32 hi and lo parts; rows
+        // past KE / KO (to the k-step) and planes past nz4 are zero
+        const float* srcs[4] = {tb.WAe, tb.WBe, tb.WAo, tb.WBo};
+        const int rows[4] = {KE, KE, KO, KO}, prow[4] = {8 * kte, 8 * kte, 8 * kto, 8 * kto};
+        for (int q = 0; q < 4; q++) {
+            const float4* src = reinterpret_cast<const float4*>(srcs[q]);
+            uint4* dh = reinterpret_cast<uint4*>(sWh + q * SZT_K * 64);
+            uint4* dl = reinterpret_cast<uint4*>(sWl + q * SZT_K * 64);
+            const int n4 = prow[q] * 16, w4 = nz4 >> 2;
+            for (int b = threadIdx.x; b < n4; b += 8 * blockDim.x) {
+                float4 v[8];
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int e = b + u * blockDim.x, i = e >> 4, z4 = e & 15;
+                    v[u] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (e < n4 && i < rows[q] && z4 < w4) v[u] = __ldg(src + i * w4 + z4);
+                }
+#pragma unroll
+                for (int u = 0; u < 8; u++) {
+                    const int e = b + u * blockDim.x, i = e >> 4, z4 = e & 15;
+                    if (e < n4) {
+                        uint4 h, l;
+                        syn_split(v[u].x, h.x, l.x);
+                        syn_split(v[u].y, h.y, l.y);
+                        syn_split(v[u].z, h.z, l.z);
+                        syn_split(v[u].w, h.w, l.w);
+                        dh[i * 16 + (z4 ^ (2 * (i & 3)))] = h;
+                        dl[i * 16 + (z4 ^ (2 * (i & 3)))] = l;
+                    }
+                }
+            }
+        }
+        // the spectrum buffer's padding (columns past 2 nact, rows past KE /
+        // KO to the k-step) is zero for every item: the items write only
+        // their data region
+        for (int i = threadIdx.x; i < 4 * SZT_K * SZT_SS; i += blockDim.x) {
+            const int q = i / (SZT_K * SZT_SS), rem = i - q * SZT_K * SZT_SS;
+            const int h = rem / SZT_SS, c = rem - h * SZT_SS;
+            const int rq = (q < 2) ? KE : KO, pq = (q < 2) ? 8 * kte : 8 * kto;
+            if (h < pq && (h >= rq || c >= 2 * nact)) sS[i] = 0.f;
+        }
+    }
+    // the first item's spectrum into registers
+    float4 pf[SZT_PF];
+    int it = blockIdx.x, t = 0, ir = 0;
+    bool act = (it < nitems) && szt_item(g, it, tmask, frk, t, ir);
+    if (act) {
+        const float4* Ot = O + (((size_t)t * nr + ir) * nkz) * nact;
+#pragma unroll
+        for (int u = 0; u < SZT_PF; u++) {
+            const int i = threadIdx.x + u * blockDim.x;
+            if (i < nsp) pf[u] = __ldg(Ot + i);
+        }
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, q = lane >> 2, c4 = lane & 3;
+    const int n0 = 8 * warp, mt = (Z0 + 15) >> 4, sw = 8 * c4;
+    for (; it < nitems; it += gridDim.x) {
+        const bool cur = act;
+        const int tc = t, irc = ir;
+        __syncthreads();  // the previous item's fragments are read
+        if (cur) {
+#pragma unroll
+            for (int u = 0; u < SZT_PF; u++) {
+                const int i = threadIdx.x + u * blockDim.x;
+                if (i < nsp) {
+                    const int k = i / nact, a = i - k * nact;
+                    const int h = k >> 1;
+                    float* A = sS + ((k & 1) ? 2 : 0) * SZT_K * SZT_SS;
+                    float* B = A + SZT_K * SZT_SS;
+                    A[h * SZT_SS + 2 * a] = pf[u].x;
+                    B[h * SZT_SS + 2 * a] = pf[u].y;
+                    A[h * SZT_SS + 2 * a + 1] = pf[u].z;
+                    B[h * SZT_SS + 2 * a + 1] = pf[u].w;
+                }
+            }
+        }
+        __syncthreads();
+        // the next item's spectrum in flight while this one is summed
+        const int nx = it + gridDim.x;
+        act = (nx < nitems) && szt_item(g, nx, tmask, frk, t, ir);
+        if (act) {
+            const float4* Ot = O + (((size_t)t * nr + ir) * nkz) * nact;
+#pragma unroll
+            for (int u = 0; u < SZT_PF; u++) {
+                const int i = threadIdx.x + u * blockDim.x;
+                if (i < nsp) pf[u] = __ldg(Ot + i);
+            }
+        }
+        if (!cur || n0 >= ncp) continue;
+        float accP[4][4], accQ[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; a++)
+#pragma unroll
+            for (int r = 0; r < 4; r++) accP[a][r] = accQ[a][r] = 0.f;
+#pragma unroll
+        for (int part = 0; part < 2; part++) {
+            // even wavenumbers: P += WAe Ae, Q += WBe Be; odd: P += WBo Bo, Q += WAo Ao
+            const uint32_t* WPh = sWh + (part ? 3 : 0) * SZT_K * 64;
+            const uint32_t* WPl = sWl + (part ? 3 : 0) * SZT_K * 64;
+            const uint32_t* WQh = sWh + (part ? 2 : 1) * SZT_K * 64;
+            const uint32_t* WQl = sWl + (part ? 2 : 1) * SZT_K * 64;
+            const float* SP = sS + (part ? 3 : 0) * SZT_K * SZT_SS;
+            const float* SQ = sS + (part ? 2 : 1) * SZT_K * SZT_SS;
+            const int kt = part ? kto : kte;
+            for (int kb = 0; kb < kt; kb++) {
+                const int i0 = 8 * kb + c4, i1 = i0 + 4;
+                uint32_t bPh[2], bPl[2], bQh[2], bQl[2];
+                syn_split(SP[i0 * SZT_SS + n0 + q], bPh[0], bPl[0]);
+                syn_split(SP[i1 * SZT_SS + n0 + q], bPh[1], bPl[1]);
+                syn_split(SQ[i0 * SZT_SS + n0 + q], bQh[0], bQl[0]);
+                syn_split(SQ[i1 * SZT_SS + n0 + q], bQh[1], bQl[1]);
+#pragma unroll
+                for (int a = 0; a < 4; a++) {
+                    if (a >= mt) break;
+                    const int m0 = (16 * a + q) ^ sw, m1 = (16 * a + q + 8) ^ sw;
+                    const int o0 = i0 * 64 + m0, o1 = i0 * 64 + m1, o2 = i1 * 64 + m0, o3 = i1 * 64 + m1;
+                    uint32_t ah[4] = {WPh[o0], WPh[o1], WPh[o2], WPh[o3]};
+                    uint32_t al[4] = {WPl[o0], WPl[o1], WPl[o2], WPl[o3]};
+                    syn_mma(accP[a], al, bPh);
+                    syn_mma(accP[a], ah, bPl);
+                    syn_mma(accP[a], ah, bPh);
+                    ah[0] = WQh[o0]; ah[1] = WQh[o1]; ah[2] = WQh[o2]; ah[3] = WQh[o3];
+                    al[0] = WQl[o0]; al[1] = WQl[o1]; al[2] = WQl[o2]; al[3] = WQl[o3];
+                    syn_mma(accQ[a], al, bQh);
+                    syn_mma(accQ[a], ah, bQl);
+                    syn_mma(accQ[a], ah, bQh);
+                }
+            }
+        }
+        // c0, c1: plane 16 a + q, columns c, c + 1; c2, c3: plane 16 a + q + 8.
+        // Plane z is P + Q and plane ngz - z is P - Q.
+        const int c = n0 + 2 * c4;
+        if (c >= ncp) continue;
+        float* Rt = R + (((size_t)tc * nr + irc) * ngz) * ncp;
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+            if (a >= mt) break;
+#pragma unroll
+            for (int hrow = 0; hrow < 2; hrow++) {
+                const int z = 16 * a + q + 8 * hrow;
+                if (z >= Z0) continue;
+                const float p0 = accP[a][2 * hrow], p1 = accP[a][2 * hrow + 1];
+                const float q0 = accQ[a][2 * hrow], q1 = accQ[a][2 * hrow + 1];
+                *reinterpret_cast<float2*>(Rt + (size_t)z * ncp + c) = make_float2(p0 + q0, p1 + q1);
+                const int zm = ngz - z;
+                if (z >= 1 && zm != z && zm < ngz)
+                    *reinterpret_cast<float2*>(Rt + (size_t)zm * ncp + c) = make_float2(p0 - q0, p1 - q1);
+            }
+        }
+    }
+}
+
 #define SYN_ZB 16
 // 288 threads: the SYN_ZB x njp / 4 (plane, 4-spoke) items of a CTA (528 at
 // 256 spokes) take two passes instead of two and a sliver
@@ -398,10 +614,19 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk) {
               b + 2 * nWe + 2 * nWo + nT, b + 2 * nWe + 2 * nWo + 2 * nT, Z0, KE, KO, njp};
     {
         // the tables, three bank pads of at most 31 floats, the spectrum
-        const size_t sm = sizeof(float) * (2 * nWe + 2 * nWo + 3 * 32 + (size_t)(KE + KO) * 2 * ncp);
-        GX_CUDA(c, cudaFuncSetAttribute(k_synz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        dim3 grid(g.nr, 4);
-        k_synz<<<grid, SYNZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, tb, c->synR, frk);
+        if (gx_synz_tc_ok(g, nact, ncp)) {
+            int sms = 148;
+            GX_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
+            const size_t sm = sizeof(float) * (8 * SZT_K * 64 + 4 * SZT_K * SZT_SS);
+            GX_CUDA(c, cudaFuncSetAttribute(k_synz_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_synz_tc<<<std::min(sms, 4 * g.nr), SYNZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->specO,
+                                                                              tb, c->synR, frk);
+        } else {
+            const size_t sm = sizeof(float) * (2 * nWe + 2 * nWo + 3 * 32 + (size_t)(KE + KO) * 2 * ncp);
+            GX_CUDA(c, cudaFuncSetAttribute(k_synz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            dim3 grid(g.nr, 4);
+            k_synz<<<grid, SYNZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->specO, tb, c->synR, frk);
+        }
         GX_LAUNCHED(c);
     }
     {
