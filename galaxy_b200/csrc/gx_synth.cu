@@ -282,8 +282,10 @@ __device__ __forceinline__ uint32_t syn_tf32(float v) {
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
     return r & 0xffffe000u;
 }
+// not volatile: the accumulator operands carry every dependency, so the
+// compiler may interleave independent products to hide their latency
 __device__ __forceinline__ void syn_mma(float* d, const uint32_t* a, const uint32_t* b) {
-    asm volatile(
+    asm(
         "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
         "{%8,%9}, {%0,%1,%2,%3};\n"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
@@ -441,16 +443,17 @@ __global__ void __launch_bounds__(SYNZ_THREADS, 1) k_synz_tc(DevGeo g, int nact,
                     if (a >= mt) break;
                     const int m0 = (16 * a + q) ^ sw, m1 = (16 * a + q + 8) ^ sw;
                     const int o0 = i0 * 64 + m0, o1 = i0 * 64 + m1, o2 = i1 * 64 + m0, o3 = i1 * 64 + m1;
-                    uint32_t ah[4] = {WPh[o0], WPh[o1], WPh[o2], WPh[o3]};
-                    uint32_t al[4] = {WPl[o0], WPl[o1], WPl[o2], WPl[o3]};
-                    syn_mma(accP[a], al, bPh);
-                    syn_mma(accP[a], ah, bPl);
-                    syn_mma(accP[a], ah, bPh);
-                    ah[0] = WQh[o0]; ah[1] = WQh[o1]; ah[2] = WQh[o2]; ah[3] = WQh[o3];
-                    al[0] = WQl[o0]; al[1] = WQl[o1]; al[2] = WQl[o2]; al[3] = WQl[o3];
-                    syn_mma(accQ[a], al, bQh);
-                    syn_mma(accQ[a], ah, bQl);
-                    syn_mma(accQ[a], ah, bQh);
+                    const uint32_t aph[4] = {WPh[o0], WPh[o1], WPh[o2], WPh[o3]};
+                    const uint32_t apl[4] = {WPl[o0], WPl[o1], WPl[o2], WPl[o3]};
+                    const uint32_t aqh[4] = {WQh[o0], WQh[o1], WQh[o2], WQh[o3]};
+                    const uint32_t aql[4] = {WQl[o0], WQl[o1], WQl[o2], WQl[o3]};
+                    // the P and Q chains interleaved
+                    syn_mma(accP[a], apl, bPh);
+                    syn_mma(accQ[a], aql, bQh);
+                    syn_mma(accP[a], aph, bPl);
+                    syn_mma(accQ[a], aqh, bQl);
+                    syn_mma(accP[a], aph, bPh);
+                    syn_mma(accQ[a], aqh, bQh);
                 }
             }
         }
