@@ -56,13 +56,26 @@ static void* g_na_ptr[256];
 // failures are reported by return code only (no message buffer to fill)
 static inline int na_fail(int rc, const char*) { return rc; }
 
+// the caller's current device, put back on every return path
+struct NaDeviceGuard {
+    int prev = -1;
+    NaDeviceGuard() {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    }
+    ~NaDeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 // Device address of the scratch array on the current device, looked up once
 // per device.  Host code must not pass g_massgn_scratch itself to a kernel:
-// on the host that name is only a stand-in for the device symbol.
-static int na_scratch(void** ptr) {
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256)
-        return na_fail(GX_ERR_CUDA, "gx_massgn_noalloc: no current CUDA device");
+// on the host that name is only a stand-in for the device symbol.  With lazy
+// module loading (CUDA's default) the first lookup on a device also loads
+// this file's module, which is when that device reserves the array.  The
+// cached address is only valid until the device is reset: a caller that
+// runs cudaDeviceReset between calls is not supported.
+static int na_scratch(int dev, void** ptr) {
+    if (dev < 0 || dev >= 256) return na_fail(GX_ERR_CUDA, "gx_massgn_noalloc: device out of range");
     std::lock_guard<std::mutex> lk(g_na_mutex);
     if (!g_na_ptr[dev]) {
         void* p = nullptr;
@@ -73,6 +86,14 @@ static int na_scratch(void** ptr) {
     }
     *ptr = g_na_ptr[dev];
     return GX_OK;
+}
+
+// one launch, its own launch status (not an error left pending by earlier,
+// unrelated work of the process)
+static int na_launch(const void* fn, unsigned grid, cudaStream_t st, void** args) {
+    if (grid == 0) return GX_OK;
+    cudaError_t e = cudaLaunchKernel(fn, dim3(grid), dim3(256), args, 0, st);
+    return (e == cudaSuccess) ? GX_OK : na_fail(GX_ERR_CUDA, "gx_massgn_noalloc: launch failed");
 }
 
 extern "C" int gx_massgn_noalloc(const GxConfig* cfg, const float* d_coords, int64_t n,
@@ -89,22 +110,31 @@ extern "C" int gx_massgn_noalloc(const GxConfig* cfg, const float* d_coords, int
     int rc = setgrd(cfg, &tmp.geo, err);
     if (rc) return na_fail(rc, "gx_massgn_noalloc: invalid grid configuration");
     fill_devgeo(&tmp);
-    const DevGeo& g = tmp.g;
+    DevGeo g = tmp.g;
     if (g.mesh > GX_NOALLOC_MAX_MESH)
         return na_fail(GX_ERR_RANGE, "gx_massgn_noalloc: mesh larger than 4194304 cells");
+    NaDeviceGuard guard;
     if (cudaSetDevice(cfg->device) != cudaSuccess)
         return na_fail(GX_ERR_CUDA, "gx_massgn_noalloc: cannot select the device");
     void* p = nullptr;
-    rc = na_scratch(&p);
+    rc = na_scratch(cfg->device, &p);
     if (rc) return rc;
     unsigned long long* acc = (unsigned long long*)p;
     cudaStream_t st = (cudaStream_t)stream;
-    const int bs = 256;
-    k_na_clear<<<(g.mesh + bs - 1) / bs, bs, 0, st>>>(acc, g.mesh);
-    if (n > 0)
-        k_na_deposit<<<(unsigned)((n + bs - 1) / bs), bs, 0, st>>>(g, d_coords, n, acc);
-    k_na_finish<<<(g.mesh + bs - 1) / bs, bs, 0, st>>>(acc, g.mesh, cfg->pmass, d_mass);
-    if (cudaGetLastError() != cudaSuccess) return na_fail(GX_ERR_CUDA, "gx_massgn_noalloc: launch failed");
+    int mesh = g.mesh;
+    float pmass = cfg->pmass;
+    const unsigned gm = (unsigned)((mesh + 255) / 256);
+    void* a_clear[] = {&acc, &mesh};
+    rc = na_launch((const void*)k_na_clear, gm, st, a_clear);
+    if (rc) return rc;
+    if (n > 0) {
+        void* a_dep[] = {&g, &d_coords, &n, &acc};
+        rc = na_launch((const void*)k_na_deposit, (unsigned)((n + 255) / 256), st, a_dep);
+        if (rc) return rc;
+    }
+    void* a_fin[] = {&acc, &mesh, &pmass, &d_mass};
+    rc = na_launch((const void*)k_na_finish, gm, st, a_fin);
+    if (rc) return rc;
     if (!stream && cudaStreamSynchronize(st) != cudaSuccess)
         return na_fail(GX_ERR_CUDA, "gx_massgn_noalloc: kernel failed");
     return GX_OK;

@@ -177,8 +177,9 @@ int gx_geometry(const GxCtx* ctx, GxGeometry* geo);
 int gx_greenm(GxCtx* ctx);
 
 /* Copy one Green component out (FP64 build rounded as stored), layout
- * [m][kz][is][ir] for 3D and [m][is][ir] for 2D, harmonic/wavenumber ranges
- * as documented in DESIGN.md.  type = GX_GREEN_*.  n = element count. */
+ * [m][kz][is][ir] for 3D and [m][is][ir] for 2D, for m = 0 .. ng-1 and, in
+ * 3D, the ngz + 1 vertical wavenumbers kz = 0 .. ngz of the doubled grid
+ * (GX_GREEN_FZ, a sine transform, is zero at kz = 0 and kz = ngz).  type = GX_GREEN_*.  n = ng * nkz * nr * nr. */
 int gx_green_get(GxCtx* ctx, int type, double* out, int64_t n);
 
 /* loadup: copy n AoS particle records (2*ndim float32 words each) into the
@@ -307,8 +308,14 @@ int gx_comm_init(GxCtx* ctx, const char* id128, int nranks, int rank);
  *    grid with more than 4194304 cells is rejected with GX_ERR_RANGE before
  *    any work is queued.
  *  - The first call on a device looks the array up (cudaGetSymbolAddress)
- *    with that device current; make that first call before any stream
- *    capture.
+ *    with that device current.  Under CUDA's default lazy module loading
+ *    that first call is also when the device loads the module and reserves
+ *    the 32 MiB, so it can fail for lack of memory: make it at set-up, as a
+ *    warm-up call with n = 0, before any stream capture.  The address is
+ *    kept for the life of the process; cudaDeviceReset between calls is not
+ *    supported.
+ *  - The call selects cfg->device while it queues its work and puts the
+ *    caller's current device back before it returns.
  *  - All calls share the array and each call clears it first, so calls
  *    whose work overlaps on the GPU (different streams, threads or
  *    processes sharing a context) race and must be serialised by the

@@ -35,7 +35,9 @@ def parse(path, kset=7, maxm=8, maxn=19):
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python " + os.path.basename(__file__) + " <reference source root>")
+    root = sys.argv[1]
     d = parse(os.path.join(root, "EXAMPLES/Basis/aj07.dat"))
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "aj07.json"), "w") as f:

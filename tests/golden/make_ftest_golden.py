@@ -59,7 +59,9 @@ def parse(root):
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: python " + os.path.basename(__file__) + " <reference source root>")
+    root = sys.argv[1]
     data = parse(root)
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "p3d_ftest.json"), "w") as f:

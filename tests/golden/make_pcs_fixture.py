@@ -16,7 +16,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from galaxy_b200.pcs import Pcs, read_pcs, write_pcs  # noqa: E402
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: python " + os.path.basename(__file__) + " <reference source root>")
+ref = sys.argv[1]
 full = read_pcs(os.path.join(ref, "EXAMPLES", "p2d", "run100.pcs0"))
 head = Pcs((3000, 0, 0), full.mcoor, 1000, full.t, full.pm, full.records[:3000])
 write_pcs(os.path.join(HERE, "run100_head.pcs"), head)

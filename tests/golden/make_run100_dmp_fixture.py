@@ -19,7 +19,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from galaxy_b200.dmp import read_dmp  # noqa: E402
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: python " + os.path.basename(__file__) + " <reference source root>")
+ref = sys.argv[1]
 ex = os.path.join(ref, "EXAMPLES", "p2d")
 d0 = read_dmp(os.path.join(ex, "run100.dmp0"))
 sub = np.arange(0, d0.records.shape[0], 5)

@@ -15,7 +15,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 from galaxy_b200.pcs import Pcs, read_pcs, write_pcs  # noqa: E402
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) < 2:
+    sys.exit("usage: python " + os.path.basename(__file__) + " <reference source root>")
+ref = sys.argv[1]
 full = read_pcs(os.path.join(ref, "EXAMPLES", "p3d", "run200.pcs0"))
 n = 5000
 head = Pcs((n, 0, 0), full.mcoor, n, full.t, full.pm, full.records[::full.n // n][:n])

@@ -63,6 +63,40 @@ def test_noalloc_massgn_matches_masset_twice(case):
     assert np.array_equal(outs[0], outs[1])
 
 
+def test_noalloc_massgn_on_a_caller_stream():
+    """Work queued on a caller's stream (a torch stream handle): the call
+    returns before the work completes, the caller synchronises that stream,
+    and the result equals gx_masset's.  A warm-up call with n = 0 first, as
+    a caller does at set-up; the caller's current device is unchanged."""
+    import torch
+    cfg, d = CASES["3d"]
+    rec, pm = kt_disk(100000, seed=22, rmax=d["rmax"], ndim=d["ndim"], z0=d["z0"],
+                      lscale=d["lscale"])
+    cfg.pmass = pm
+    with Galaxy(cfg) as gal:
+        gal.loadup(rec)
+        gal.masset()
+        ref = gal.grid(GX_GRID_MASS).astype(np.float64)
+        mesh = gal.mesh
+    L = _setup(lib())
+    coords = torch.from_numpy(rec).cuda()
+    out = torch.full((mesh,), -1.0, dtype=torch.float32, device="cuda")
+    st = torch.cuda.Stream()
+    torch.cuda.synchronize()
+    dev = torch.cuda.current_device()
+    assert L.gx_massgn_noalloc(C.byref(cfg), None, 0, out.data_ptr(), st.cuda_stream) == GX_OK
+    st.synchronize()
+    assert float(out.abs().max()) == 0.0  # no particles: an empty mesh
+    rc = L.gx_massgn_noalloc(C.byref(cfg), coords.data_ptr(), rec.shape[0], out.data_ptr(),
+                             st.cuda_stream)
+    assert rc == GX_OK
+    st.synchronize()
+    assert torch.cuda.current_device() == dev
+    m = out.cpu().numpy().astype(np.float64)
+    assert np.abs(m - ref).max() / ref.max() < 2e-6
+    assert abs(m.sum() - ref.sum()) / ref.sum() < 1e-6
+
+
 def test_noalloc_rejects_mesh_beyond_limit():
     import torch
     L = _setup(lib())
