@@ -170,6 +170,10 @@ static int alloc_grids(GxCtx* c) {
         DALLOC(c, c->polar64, 4 * mesh);
         DALLOC(c, c->spec64, 4 * nspec);
         DALLOC(c, c->out64, 16 * nspec);
+        // solve scratch, once per context (a solve allocates nothing)
+        const size_t naz = (size_t)g.nr * g.ngz * c->spec.nact * 2;
+        DALLOC(c, c->az64, naz);
+        DALLOC(c, c->rows64, 4 * naz);
     } else {
         DALLOC(c, c->mass, mesh);
         DALLOC(c, c->field, mesh);
@@ -249,7 +253,7 @@ void gx_destroy(GxCtx* c) {
     void* ptrs[] = {c->green32, c->green64, c->pbuf[0], c->pbuf[1], c->perm, c->origin,
                     c->origin_tmp, c->pkey[0], c->pkey[1], c->pfr, c->p64, c->key64, c->w64, c->acc64, c->ppot,
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
-                    c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->perm_next, c->rowstart,
+                    c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->az64, c->rows64, c->pot64, c->perm_next, c->rowstart,
                     c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->rowtile, c->stage, c->jrk_d,
                     c->errword, c->dsum, c->pzone[0], c->pzone[1], c->zbuf, c->zjrk_d, c->act_d};
     for (void* p : ptrs)
@@ -369,8 +373,8 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     // grow: free old
     void* old[] = {c->pbuf[0], c->pbuf[1], c->perm, c->origin, c->origin_tmp, c->pkey[0], c->pkey[1],
                    c->pfr, c->p64,
-                   c->key64, c->w64, c->acc64, c->ppot, c->pacc, c->perm_next, c->items, c->stage,
-                   c->pzone[0], c->pzone[1]};
+                   c->key64, c->w64, c->acc64, c->pot64, c->ppot, c->pacc, c->perm_next, c->items,
+                   c->stage, c->pzone[0], c->pzone[1]};
     for (void* p : old)
         if (p) cudaFree(p);
     c->pbuf[0] = c->pbuf[1] = nullptr;
@@ -380,7 +384,7 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     c->pzone[0] = c->pzone[1] = nullptr;
     c->p64 = nullptr;
     c->key64 = nullptr;
-    c->w64 = c->acc64 = nullptr;
+    c->w64 = c->acc64 = c->pot64 = nullptr;
     c->ppot = c->pacc = nullptr;
     c->perm_next = nullptr;
     c->items = nullptr;
@@ -394,6 +398,7 @@ static int alloc_particles(GxCtx* c, int64_t n) {
         DALLOC(c, c->key64, cap);
         DALLOC(c, c->w64, 8 * cap);
         DALLOC(c, c->acc64, 3 * cap);
+        DALLOC(c, c->pot64, cap);
         return GX_OK;
     }
     // compensated positions keep a low part of every coordinate after the

@@ -110,6 +110,9 @@ struct GxCtx {
     float* fwdC1 = nullptr;                // azimuthal spectra of every ring-plane row [nrow][ncp]
     double* spec64 = nullptr;
     double* out64 = nullptr;
+    double* az64 = nullptr;                // FP64 path: azimuthal spectra [2][nr*ngz*nact]
+    double* rows64 = nullptr;              // FP64 path: vertically synthesised rows [4][...]
+    double* pot64 = nullptr;               // FP64 path: per-particle potential [cap]
     bool have_mass = false;
     bool have_field = false;
     bool field_pot = false;

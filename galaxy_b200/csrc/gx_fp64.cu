@@ -342,14 +342,6 @@ __global__ void k64_to_f32(const double* __restrict__ a, int64_t n, float* __res
 }
 
 // ---------------------------------------------------------------------------
-static int fp64_scratch(GxCtx* c, double** az, double** rows) {
-    const DevGeo& g = c->g;
-    size_t naz = (size_t)g.nr * g.ngz * c->spec.nact * 2;
-    GX_CUDA(c, cudaMallocAsync((void**)az, sizeof(double) * naz, c->stream));
-    GX_CUDA(c, cudaMallocAsync((void**)rows, sizeof(double) * 4 * naz, c->stream));
-    return GX_OK;
-}
-
 static inline unsigned nblk(int64_t n, int bs) { return (unsigned)((n + bs - 1) / bs); }
 
 int gx_fp64_masset(GxCtx* c) {
@@ -375,9 +367,7 @@ int gx_fp64_findf(GxCtx* c, int lpot, bool) {
     const int nact = c->spec.nact;
     GX_CUDA(c, cudaMemcpyToSymbolAsync(c64_act_m, c->spec.m, sizeof(int) * 260, 0,
                                        cudaMemcpyHostToDevice, c->stream));
-    double *az = nullptr, *rows = nullptr;
-    int rc = fp64_scratch(c, &az, &rows);
-    if (rc) return rc;
+    double *az = c->az64, *rows = c->rows64;
     int tmask = 1 | 2 | (g.ndim == 3 ? 4 : 0) | (lpot ? 8 : 0);
     if (g.ng == 1) tmask &= ~2;
     int64_t n1 = (int64_t)g.nr * g.ngz * nact;
@@ -395,8 +385,6 @@ int gx_fp64_findf(GxCtx* c, int lpot, bool) {
     k64_syn_az<<<nblk(g.mesh, 128), 128, 0, c->stream>>>(g, nact, tmask, rows, c->polar64,
                                                          c->field64);
     GX_LAUNCHED(c);
-    GX_CUDA(c, cudaFreeAsync(az, c->stream));
-    GX_CUDA(c, cudaFreeAsync(rows, c->stream));
     c->have_field = true;
     c->field_pot = lpot != 0;
     return GX_OK;
@@ -406,8 +394,7 @@ int gx_fp64_getacc(GxCtx* c, float* acc, float* pot) {
     const DevGeo& g = c->g;
     const int64_t n = c->n;
     if (n == 0) return GX_OK;
-    double* pot64 = nullptr;
-    GX_CUDA(c, cudaMallocAsync((void**)&pot64, sizeof(double) * n, c->stream));
+    double* pot64 = c->pot64;
     k64_gather<<<nblk(n, 256), 256, 0, c->stream>>>(g, c->p64, c->cap, n, c->field64, c->acc64, pot64);
     GX_LAUNCHED(c);
     k64_to_f32_aos<<<nblk(n, 256), 256, 0, c->stream>>>(c->acc64, c->cap, n, g.ndim, c->pacc);
@@ -418,7 +405,6 @@ int gx_fp64_getacc(GxCtx* c, float* acc, float* pot) {
                                c->stream));
     if (pot)
         GX_CUDA(c, cudaMemcpyAsync(pot, c->ppot, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
-    GX_CUDA(c, cudaFreeAsync(pot64, c->stream));
     return GX_OK;
 }
 
