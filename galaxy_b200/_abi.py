@@ -24,6 +24,7 @@ GX_PREC_MIXED_TC05 = 2
 GX_FLAG_COMPENSATED = 1
 GX_FLAG_QUADRATIC = 2
 GX_FLAG_WHOLE_GRID = 4
+GX_FLAG_SORTED_DEPOSIT = 8
 
 GX_GRID_MASS = 0
 GX_GRID_FR = 1

@@ -411,6 +411,10 @@ extern "C" int gx_adjoint(GxCtx* c, int nsteps, int ckpt_every, double* J_out, f
     const int64_t n = c->n;
     if (n < 1) return c->err = "no particles loaded", GX_ERR_STATE;
     cudaSetDevice(c->dev);
+    {
+        const int rc = gx_dense(c);
+        if (rc) return rc;
+    }
     const DevGeo& g = c->g;
     const int nact = c->spec.nact;
     AdjAct act;

@@ -188,6 +188,8 @@ static int alloc_grids(GxCtx* c) {
         DALLOC(c, c->rowtile, (size_t)4 * ((g.nrow + 1 + ROW_TILE - 1) / ROW_TILE));
         DALLOC(c, c->nitems_d, 4);
         GX_CUDA(c, cudaMemsetAsync(c->rowcnt, 0, sizeof(uint32_t) * NCOPY * (g.nrow + 1), c->stream));
+        int rc = gx_bucket_alloc(c);
+        if (rc) return rc;
     }
     DALLOC(c, c->jrk_d, 4);
     DALLOC(c, c->errword, 4);
@@ -255,7 +257,9 @@ void gx_destroy(GxCtx* c) {
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
                     c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->az64, c->rows64, c->pot64, c->perm_next, c->rowstart,
                     c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->rowtile, c->stage, c->jrk_d,
-                    c->errword, c->dsum, c->pzone[0], c->pzone[1], c->zbuf, c->zjrk_d, c->act_d};
+                    c->errword, c->dsum, c->pzone[0], c->pzone[1], c->zbuf, c->zjrk_d, c->act_d,
+                    c->bk_cap[0], c->bk_cap[1], c->bk_base[0], c->bk_base[1], c->bk_fill[0], c->bk_fill[1],
+                    c->bk_ctl, c->bk_items, c->bk_cnt, c->macc};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (int i = 0; i <= GX_NPHASE; i++)
@@ -374,7 +378,7 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     void* old[] = {c->pbuf[0], c->pbuf[1], c->perm, c->origin, c->origin_tmp, c->pkey[0], c->pkey[1],
                    c->pfr, c->p64,
                    c->key64, c->w64, c->acc64, c->pot64, c->ppot, c->pacc, c->perm_next, c->items,
-                   c->stage, c->pzone[0], c->pzone[1]};
+                   c->stage, c->pzone[0], c->pzone[1], c->bk_items};
     for (void* p : old)
         if (p) cudaFree(p);
     c->pbuf[0] = c->pbuf[1] = nullptr;
@@ -389,7 +393,16 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     c->perm_next = nullptr;
     c->items = nullptr;
     c->stage = nullptr;
+    c->bk_items = nullptr;
+    c->bucketed = false;
     int64_t cap = std::max<int64_t>(n, 1);
+    if (!c->fp64) {
+        // the bucketed store: row segments with 1/8 + 16 slots of slack per
+        // row, then an overflow area that can take every particle
+        c->bk_main = cap + cap / 8 + 16 * ((int64_t)c->g.nrow + 1);
+        cap = c->bk_main + cap + 64;
+        if (cap > (int64_t)INT32_MAX) return c->err = "too many particles for the bucketed store", GX_ERR_RANGE;
+    }
     c->cap = cap;
     DALLOC(c, c->ppot, cap);
     DALLOC(c, c->pacc, 3 * cap);
@@ -418,6 +431,10 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     DALLOC(c, c->items, (size_t)3 * c->maxitems);
     int nq = c->g.quad ? 9 : (c->g.ndim == 3) ? 4 : 2;
     DALLOC(c, c->stage, (size_t)c->maxitems * nq * c->g.na);
+    // fused-pass work items: every row's segment in chunks of 8192, and the
+    // overflow area's
+    c->bk_maxitems = (int64_t)c->g.nrow + 1 + 2 * (n / 8192 + 2);
+    DALLOC(c, c->bk_items, (size_t)c->bk_maxitems);
     return GX_OK;
 }
 
@@ -431,6 +448,7 @@ int gx_loadup(GxCtx* c, const float* coords, int64_t n) {
     if (rc) return rc;
     c->n = n;
     c->have_mass = c->have_field = c->have_keys = false;
+    c->bucketed = false;
     const int nw = 2 * c->g.ndim;
     if (n == 0) return (c->nzones > 1 && !c->fp64) ? gx_zone_loadup(c) : GX_OK;
     float* staging = nullptr;
@@ -467,6 +485,8 @@ int gx_unload(GxCtx* c, float* coords) {
     if (!c || (!coords && c->n > 0)) return GX_ERR_ARG;
     if (c->n == 0) return GX_OK;
     cudaSetDevice(c->dev);
+    int rc = gx_dense(c);
+    if (rc) return rc;
     const int nw = 2 * c->g.ndim;
     const int64_t n = c->n;
     float* staging = nullptr;
@@ -477,7 +497,7 @@ int gx_unload(GxCtx* c, float* coords) {
     else k_soa_to_aos<<<nb, bs, 0, c->stream>>>(c->pbuf[c->cur], c->origin, staging, n, c->cap, nw);
     GX_LAUNCHED(c);
     if (c->nzones > 1) {
-        int rc = gx_zone_unload(c, staging);
+        rc = gx_zone_unload(c, staging);
         if (rc) return rc;
     }
     GX_CUDA(c, cudaMemcpyAsync(coords, staging, sizeof(float) * nw * n, cudaMemcpyDeviceToHost,
@@ -490,7 +510,9 @@ int gx_unload(GxCtx* c, float* coords) {
 int gx_masset(GxCtx* c) {
     if (!c) return GX_ERR_ARG;
     cudaSetDevice(c->dev);
-    int rc = c->fp64 ? gx_fp64_masset(c) : (c->nzones > 1 ? gx_zone_masset(c) : gx_mixed_masset(c));
+    int rc = gx_dense(c);
+    if (rc) return rc;
+    rc = c->fp64 ? gx_fp64_masset(c) : (c->nzones > 1 ? gx_zone_masset(c) : gx_mixed_masset(c));
     if (rc) return rc;
     GX_CUDA(c, cudaStreamSynchronize(c->stream));
     c->have_mass = true;
@@ -524,7 +546,9 @@ int gx_getacc(GxCtx* c, float* acc, float* pot) {
     if (!c || (!acc && c->n > 0)) return GX_ERR_ARG;
     if (!c->have_field) return c->err = "no fields (call gx_findf)", GX_ERR_STATE;
     cudaSetDevice(c->dev);
-    int rc = c->fp64 ? gx_fp64_getacc(c, acc, pot) : gx_mixed_getacc(c, acc, pot);
+    int rc = gx_dense(c);
+    if (rc) return rc;
+    rc = c->fp64 ? gx_fp64_getacc(c, acc, pot) : gx_mixed_getacc(c, acc, pot);
     if (rc) return rc;
     GX_CUDA(c, cudaStreamSynchronize(c->stream));
     return GX_OK;
@@ -537,8 +561,11 @@ int gx_step(GxCtx* c, int nsteps, int phys) {
     cudaSetDevice(c->dev);
     c->launches = 0;
     GX_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-    int rc = c->fp64 ? gx_fp64_step(c, nsteps, phys)
-                     : (c->nzones > 1 ? gx_zone_step(c, nsteps, phys) : gx_mixed_step(c, nsteps, phys));
+    int rc;
+    if (c->fp64) rc = gx_fp64_step(c, nsteps, phys);
+    else if (gx_fast_ok(c)) rc = gx_fast_step(c, nsteps, phys);
+    else if ((rc = gx_dense(c)) == GX_OK)
+        rc = (c->nzones > 1) ? gx_zone_step(c, nsteps, phys) : gx_mixed_step(c, nsteps, phys);
     if (rc) return rc;
     GX_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     GX_CUDA(c, cudaEventSynchronize(c->ev1));

@@ -156,6 +156,23 @@ struct GxCtx {
     int lstep[GX_MAX_ZONES][2] = {};         // step numbers of zold, znew
     bool zones_ready = false;                // zone arrays deposited (gx_masset)
 
+    // bucketed particle store of the fused step (gx_bucket.cu): pbuf[b] holds
+    // one segment of slots per ring-plane row (row nrow: off the grid),
+    // [bk_base[b][r], + bk_cap[b][r]), of which the first
+    // min(bk_fill[b][r], bk_cap[b][r]) are particles, then an overflow area
+    // of bk_ctl[b][0] particles from slot bk_main on
+    bool bucketed = false;
+    int64_t bk_main = 0;
+    int32_t* bk_cap[2] = {nullptr, nullptr};
+    int32_t* bk_base[2] = {nullptr, nullptr};
+    int32_t* bk_fill[2] = {nullptr, nullptr};
+    int32_t* bk_ctl = nullptr;               // [2][4]: overflow count of each buffer; [8] items, [9] work counter
+    int4* bk_items = nullptr;                // work items of pbuf[cur]: row (-1: overflow), first, end slot
+    int64_t bk_maxitems = 0;
+    int32_t* bk_cnt = nullptr;               // [nrow + 1] row counts of the dense store (bucketing)
+    unsigned long long* macc = nullptr;      // [mesh] fixed-point mass (2^-20 of a particle), zero between steps
+    int bk_grid = 0;                         // CTAs of the fused pass
+
     // multi-GPU (gx_comm.cu): NCCL communicator of the particle decomposition
     void* comm = nullptr;
     int nranks = 1, rank = 0;
@@ -208,6 +225,7 @@ struct CellW {
     int key;      // ncl - 1, or -1 when off the grid / in the hole
     float du, dt, dz;  // fractions in the cell; quadratic: coord + 1/2 - index
     int row, jt;  // ring-plane row and spoke of key (set by gx_cell)
+    int ju, iz;   // ring and plane of row (linear scheme; row = ju * ngz + iz)
 };
 
 // floor of a float in [0, 2^23) and the exact fraction v - floor(v), on the
@@ -312,6 +330,7 @@ __device__ __forceinline__ CellW gx_cell_t(const DevGeo& g, float x, float y, fl
     c.key = -1;
     c.du = c.dt = c.dz = 0.f;
     c.row = c.jt = 0;
+    c.ju = c.iz = 0;
     const float r2 = __fadd_rn(__fmul_rn(x, x), __fmul_rn(y, y));
     float rr;
     if (EXACT) {
@@ -352,6 +371,7 @@ __device__ __forceinline__ CellW gx_cell_t(const DevGeo& g, float x, float y, fl
         c.du = u - gx_i2f(ju);
     }
     const int jt = gx_trunc(t, c.dt);
+    c.ju = ju;
     if (!gx_is3<ND>(g)) {
         c.row = ju;
     } else {
@@ -363,6 +383,7 @@ __device__ __forceinline__ CellW gx_cell_t(const DevGeo& g, float x, float y, fl
             c.dz = zz - gx_i2f(jz);
         }
         c.row = ju * g.ngz + jz;
+        c.iz = jz;
     }
     c.key = c.row * g.na + jt;
     // a spoke coordinate that rounded up to na keys the next row's spoke 0,
@@ -371,6 +392,12 @@ __device__ __forceinline__ CellW gx_cell_t(const DevGeo& g, float x, float y, fl
     if (jt >= g.na) {
         c.jt = jt - g.na;
         c.row += 1;
+        if (!gx_is3<ND>(g)) {
+            c.ju += 1;
+        } else if (++c.iz == g.ngz) {
+            c.iz = 0;
+            c.ju += 1;
+        }
     }
     return c;
 }
@@ -646,6 +673,11 @@ int gx_zone_unload(GxCtx* c, float* staging);
 int gx_zone_masset(GxCtx* c);
 int gx_zone_step(GxCtx* c, int nsteps, int phys);
 int gx_comm_reduce_range(GxCtx* c);
+// fused step on the bucketed store (gx_bucket.cu)
+bool gx_fast_ok(const GxCtx* c);  // single zone, linear scheme, mixed, not GX_FLAG_SORTED_DEPOSIT
+int gx_fast_step(GxCtx* c, int nsteps, int phys);
+int gx_dense(GxCtx* c);  // bucketed store -> dense store (no-op when dense)
+int gx_bucket_alloc(GxCtx* c);
 int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk = nullptr);
 int gx_comm_reduce_spectrum(GxCtx* c);
 void gx_comm_destroy(GxCtx* c);

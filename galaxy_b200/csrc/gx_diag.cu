@@ -146,9 +146,11 @@ extern "C" int gx_tmcent(GxCtx* c, int start) {
     const int64_t n = c->n;
     if (n == 0) return GX_OK;
     const float fac = start ? 0.5f : -0.5f;
+    int rc = gx_dense(c);
+    if (rc) return rc;
     if (c->fp64) {
         std::vector<float> tmp((size_t)c->g.ndim * n);
-        int rc = gx_fp64_getacc(c, tmp.data(), nullptr);  // fills acc64
+        rc = gx_fp64_getacc(c, tmp.data(), nullptr);  // fills acc64
         if (rc) return rc;
         k64_tmcent<<<(unsigned)((n + 255) / 256), 256, 0, c->stream>>>(c->g, c->p64, c->cap, n,
                                                                       c->acc64, (double)fac);
@@ -167,6 +169,8 @@ extern "C" int gx_icheck(GxCtx* c, GxDiag* d) {
     if (!c->have_field) return c->err = "no fields (call gx_findf with lpot)", GX_ERR_STATE;
     if (c->fp64) return c->err = "gx_icheck runs on the mixed path", GX_ERR_ARG;
     cudaSetDevice(c->dev);
+    int rc = gx_dense(c);
+    if (rc) return rc;
     const int nb = 148 * 4;
     double* part = nullptr;
     GX_CUDA(c, cudaMallocAsync((void**)&part, sizeof(double) * NDSUM * nb, c->stream));

@@ -63,6 +63,11 @@ extern "C" {
 #define GX_FLAG_WHOLE_GRID  4   /* time-step zones: the field over the whole grid
                                    on every step (the 'wholeg' option, findf.f:41)
                                    instead of partial-grid solves */
+#define GX_FLAG_SORTED_DEPOSIT 8 /* mixed path: step with the row-sorted deposit
+                                   (counting sort of the cell rows, staged
+                                   fixed-point items, combine) instead of the
+                                   fused pass over the bucketed particle store;
+                                   the two give bitwise identical results */
 #define GX_MAX_WEIGHTS     27   /* weights per particle of gx_weight          */
 
 /* grid arrays for gx_get_grid / gx_set_mass */
