@@ -69,13 +69,15 @@ def test_gpu_adjoint_matches_fp64_oracle(ckpt):
         # the context holds the initial particles again
         back = gal.unload()
     assert np.array_equal(back, rec)
-    assert abs(J - J_ref) < 1e-5 * J_ref, (J, J_ref)
+    # measured on a B200: J 1.7e-8, gradient 2.9e-6 (each component <= 3.0e-6),
+    # halo-parameter derivatives <= 8.2e-6, relative to the FP64 oracle
+    assert abs(J - J_ref) < 1e-6 * J_ref, (J, J_ref)
     err = np.linalg.norm(grad - g_ref) / np.linalg.norm(g_ref)
-    assert err < 2e-3, err
+    assert err < 3e-5, err
     for k in range(4):
         ek = np.linalg.norm(grad[:, k] - g_ref[:, k]) / np.linalg.norm(g_ref[:, k])
-        assert ek < 5e-3, (k, ek)
-    assert np.all(np.abs(dth - th_ref) < 2e-3 * np.abs(th_ref)), (dth, th_ref)
+        assert ek < 3e-5, (k, ek)
+    assert np.all(np.abs(dth - th_ref) < 1e-4 * np.abs(th_ref)), (dth, th_ref)
     # time reversal in FP32 over at most ckpt steps stays close to the checkpoints
     assert drift < 1e-3, drift
 
