@@ -259,11 +259,14 @@ void gx_destroy(GxCtx* c) {
                     c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->rowtile, c->stage, c->jrk_d,
                     c->errword, c->dsum, c->pzone[0], c->pzone[1], c->zbuf, c->zjrk_d, c->act_d,
                     c->bk_cap[0], c->bk_cap[1], c->bk_base[0], c->bk_base[1], c->bk_fill[0], c->bk_fill[1],
-                    c->bk_ctl, c->bk_items, c->bk_cnt, c->macc};
+                    c->bk_ctl, c->bk_items, c->bk_cnt, c->macc, c->bq[0], c->bq[1]};
     for (void* p : ptrs)
         if (p) cudaFree(p);
-    for (int i = 0; i <= GX_NPHASE; i++)
-        if (c->pev[i]) cudaEventDestroy(c->pev[i]);
+    for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
+    if (c->bk_side) cudaStreamSynchronize(c->bk_side);
+    for (cudaEvent_t e : c->bk_ev)
+        if (e) cudaEventDestroy(e);
+    if (c->bk_side) cudaStreamDestroy(c->bk_side);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -310,27 +313,40 @@ int gx_green_get(GxCtx* c, int type, double* out, int64_t n) {
 
 }  // extern "C"
 
-// phase marks: a phase runs from its mark to the next mark (or the end);
-// the elapsed time is collected synchronously at the next mark, which is
-// only done in profile mode
-int gx_phase_mark(GxCtx* c, int ph) {
-    if (!c->prof) return GX_OK;
-    int rc = gx_phase_end(c);
-    if (rc) return rc;
-    GX_CUDA(c, cudaEventRecord(c->pev[0], c->stream));
-    c->open_phase = ph;
+// phase marks: a phase runs from its mark to the next mark (or the end).
+// Marks only record events; gx_phase_end waits for the last one and adds
+// up the elapsed times.  Only done in profile mode.
+static int phase_record(GxCtx* c, int ph) {
+    if (c->nmarks == (int)c->pev.size()) {
+        cudaEvent_t e;
+        GX_CUDA(c, cudaEventCreate(&e));
+        c->pev.push_back(e);
+        c->pev_ph.push_back(-1);
+    }
+    GX_CUDA(c, cudaEventRecord(c->pev[c->nmarks], c->stream));
+    c->pev_ph[c->nmarks++] = ph;
     return GX_OK;
 }
 
+int gx_phase_mark(GxCtx* c, int ph) {
+    if (!c->prof) return GX_OK;
+    return phase_record(c, ph);
+}
+
 int gx_phase_end(GxCtx* c) {
-    if (!c->prof || c->open_phase < 0) return GX_OK;
-    GX_CUDA(c, cudaEventRecord(c->pev[1], c->stream));
-    GX_CUDA(c, cudaEventSynchronize(c->pev[1]));
-    float ms = 0.f;
-    GX_CUDA(c, cudaEventElapsedTime(&ms, c->pev[0], c->pev[1]));
-    c->phase_ms[c->open_phase] += ms;
-    c->phase_n[c->open_phase] += 1;
-    c->open_phase = -1;
+    if (!c->prof || c->nmarks == 0) return GX_OK;
+    int rc = phase_record(c, -1);
+    if (rc) return rc;
+    GX_CUDA(c, cudaEventSynchronize(c->pev[c->nmarks - 1]));
+    for (int k = 0; k + 1 < c->nmarks; k++) {
+        const int ph = c->pev_ph[k];
+        if (ph < 0) continue;
+        float ms = 0.f;
+        GX_CUDA(c, cudaEventElapsedTime(&ms, c->pev[k], c->pev[k + 1]));
+        c->phase_ms[ph] += ms;
+        c->phase_n[ph] += 1;
+    }
+    c->nmarks = 0;
     return GX_OK;
 }
 
@@ -394,15 +410,12 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     c->items = nullptr;
     c->stage = nullptr;
     c->bk_items = nullptr;
+    for (int b = 0; b < 2; b++) {
+        if (c->bq[b]) cudaFree(c->bq[b]);
+        c->bq[b] = nullptr;
+    }
     c->bucketed = false;
     int64_t cap = std::max<int64_t>(n, 1);
-    if (!c->fp64) {
-        // the bucketed store: row segments with 1/8 + 16 slots of slack per
-        // row, then an overflow area that can take every particle
-        c->bk_main = cap + cap / 8 + 16 * ((int64_t)c->g.nrow + 1);
-        cap = c->bk_main + cap + 64;
-        if (cap > (int64_t)INT32_MAX) return c->err = "too many particles for the bucketed store", GX_ERR_RANGE;
-    }
     c->cap = cap;
     DALLOC(c, c->ppot, cap);
     DALLOC(c, c->pacc, 3 * cap);
@@ -431,10 +444,16 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     DALLOC(c, c->items, (size_t)3 * c->maxitems);
     int nq = c->g.quad ? 9 : (c->g.ndim == 3) ? 4 : 2;
     DALLOC(c, c->stage, (size_t)c->maxitems * nq * c->g.na);
-    // fused-pass work items: every row's segment in chunks of 8192, and the
-    // overflow area's
-    c->bk_maxitems = (int64_t)c->g.nrow + 1 + 2 * (n / 8192 + 2);
+    // fused-pass work items: every row's segment in chunks of BK_ITEM, and
+    // the overflow area's
+    c->bk_maxitems = (int64_t)c->g.nrow + 1 + 2 * (n / BK_ITEM + 2);
     DALLOC(c, c->bk_items, (size_t)c->bk_maxitems);
+    // the bucketed store: row segments with 1/8 + 16 slots of slack per row,
+    // then an overflow area that can take every particle
+    c->bk_main = cap + cap / 8 + 16 * ((int64_t)c->g.nrow + 1);
+    c->bcap = c->bk_main + cap + 64;
+    if (c->bcap > (int64_t)INT32_MAX) return c->err = "too many particles for the bucketed store", GX_ERR_RANGE;
+    for (int b = 0; b < 2; b++) DALLOC(c, c->bq[b], (size_t)gx_bucket_words(c) * c->bcap);
     return GX_OK;
 }
 
@@ -599,9 +618,8 @@ int gx_host_free(void* ptr) {
 int gx_set_profile(GxCtx* c, int on) {
     if (!c) return GX_ERR_ARG;
     cudaSetDevice(c->dev);
-    if (on && !c->pev[0])
-        for (int i = 0; i <= GX_NPHASE; i++) GX_CUDA(c, cudaEventCreate(&c->pev[i]));
     c->prof = on != 0;
+    c->nmarks = 0;
     for (int i = 0; i < GX_NPHASE; i++) {
         c->phase_ms[i] = 0.f;
         c->phase_n[i] = 0;

@@ -9,7 +9,7 @@
 // step, k_push_bkt, over a store that keeps the particles grouped by the
 // ring-plane row of their cell:
 //
-//   * pbuf[b] holds one segment of slots per row (row nrow: off the grid);
+//   * bq[b] holds one segment of slots per row (row nrow: off the grid);
 //     segment r starts at bk_base[b][r] and has bk_cap[b][r] slots, planned
 //     from the previous step's row counts with 1/8 + 16 slots of slack, so
 //     that a particle that changes row usually finds room in its new row's
@@ -22,11 +22,15 @@
 //     exactly as the reference does (bit-exact keys), writes it into the
 //     segment of its new row in the output buffer (warp-aggregated slot
 //     atomics), and adds its 4 / 8 CIC weights as 2^-20 fixed-point
-//     integers: into int64 shared-memory bins over the window of rows around
-//     the item's row (4 rings, and 4 planes in 3D: every cell a particle of
-//     the row can reach moving less than a cell), or, for corners outside
-//     it, straight into the int64 mesh accumulator.  The bins are flushed
-//     into the accumulator (nonzero bins only) after each item.
+//     integers: into unsigned 32-bit shared-memory bins over the window of
+//     rows around the item's row (4 rings, and 4 planes in 3D: every cell a
+//     particle of the row can reach moving less than a cell), or, for
+//     corners outside it (and the rare negative weight), straight into the
+//     int64 mesh accumulator.  The bins are flushed into the accumulator
+//     (nonzero bins only) after each item.  A bin cannot wrap: the linear
+//     weights that reach it are >= 0 and <= 1 + 1e-4, each particle adds at
+//     most one to a bin, and an item holds at most 4095 particles, so a bin
+//     stays below 4095 (2^20 + 105) < 2^32.
 //   * k_bk_plan (one CTA) turns the output buffer's row counts into its
 //     work items, the next output buffer's segments and the active ring
 //     range (jrad, krad); k_mass_convert turns the accumulator into the mass
@@ -35,23 +39,33 @@
 // Integer sums do not depend on their order, so the mass array is the same
 // integers, converted the same way, as the sort-based deposit of
 // gx_deposit.cu: the fused path is bitwise identical to it, whatever order
-// the atomics resolve in.  Particles keep their load index (origin) next to
-// them; gx_dense() compacts the store back to n contiguous particles for the
-// entry points that walk it that way (unload, getacc, tmcent, icheck, the
-// adjoint, masset).
+// the atomics resolve in.  A particle's record carries its load index;
+// gx_dense() writes the store back to the n contiguous SoA particles of
+// pbuf[cur] for the entry points that walk them that way (unload, getacc,
+// tmcent, icheck, the adjoint, masset).
 #include <algorithm>
 
 #include "gx_common.cuh"
 
 #define BK_FIXQ 1048576.0f  // 2^20: the fixed-point quantum of gx_deposit.cu
-#define BK_ITEM 8192        // particles per work item
-#define BK_SPARSE 64        // items with fewer particles add straight into the mesh
+#define BK_SPARSE 256       // items with fewer particles add straight into the mesh
 #define BK_THREADS 256
-#define PLAN_THREADS 1024
+#define PLAN_THREADS 512
 #define PLAN_ROWS 8         // rows per plan thread per pass
+#ifndef BK_MINB
+#define BK_MINB 5           // resident CTAs per SM the register budget is set for
+#endif
 
 __device__ __forceinline__ void red_add_s64(unsigned long long* a, int v) {
     atomicAdd(a, (unsigned long long)(long long)v);  // two's complement sum
+}
+
+// round(w 2^20) to the nearest integer, ties to even, for |w 2^20| < 2^22:
+// adding 1.5 2^23 leaves the rounded integer in the low mantissa bits (the
+// product by a power of two is exact, so one FMA rounds once, exactly as
+// __float2int_rn(w * 2^20) does), on the FMA pipe instead of a conversion
+__device__ __forceinline__ int bk_fix(float w) {
+    return __float_as_int(fmaf(w, BK_FIXQ, 12582912.0f)) - 0x4B400000;
 }
 
 // ---------------------------------------------------------------------------
@@ -73,8 +87,10 @@ __device__ __forceinline__ void plan_scan2(int a, int b, int& ea, int& eb, int& 
         wb[warp] = xb;
     }
     __syncthreads();
+    constexpr int NWP = PLAN_THREADS / 32;  // warps (<= 32): lanes past them hold zeros
+    static_assert(NWP <= 32, "one warp scans the warp totals");
     if (warp == 0) {
-        int va = wa[lane], vb = wb[lane];
+        int va = (lane < NWP) ? wa[lane] : 0, vb = (lane < NWP) ? wb[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int ya = __shfl_up_sync(0xffffffffu, va, o), yb = __shfl_up_sync(0xffffffffu, vb, o);
@@ -83,55 +99,70 @@ __device__ __forceinline__ void plan_scan2(int a, int b, int& ea, int& eb, int& 
                 vb += yb;
             }
         }
-        wa[lane] = va;
-        wb[lane] = vb;
+        if (lane < NWP) {
+            wa[lane] = va;
+            wb[lane] = vb;
+        }
     }
     __syncthreads();
     const int pa = warp ? wa[warp - 1] : 0, pb = warp ? wb[warp - 1] : 0;
     ea = pa + xa - a;
     eb = pb + xb - b;
-    ta = wa[PLAN_THREADS / 32 - 1];
-    tb = wb[PLAN_THREADS / 32 - 1];
+    ta = wa[NWP - 1];
+    tb = wb[NWP - 1];
     __syncthreads();
 }
 
 // The plan of one step, one CTA:
 //  * with fill_o: the work items of the buffer just written (fill_o, cap_o,
-//    base_o, overflow count *ovf_o at slot ovf_base), the active ring range
-//    of its particles (jrad = first ring + 1, krad = min(last ring + 2, nr),
-//    as massgn tracks them), and ctl[0] = items, ctl[1] = 0 (work counter);
+//    base_o, overflow count *ovf_o at slot ovf_base; each item: row, first
+//    slot, end slot, ring of the row), and ctl[0] = items, ctl[1] = 0 (the
+//    work counter);
 //  * the segments of the buffer to be written next from the row counts
 //    want: cap_n = want + want/8 + 16 (0 for empty rows), base_n their
 //    exclusive sum; its fill counters and overflow count cleared.
+// The row tables are padded with zeros to a multiple of PLAN_THREADS x
+// PLAN_ROWS entries, so that every thread moves its eight consecutive rows
+// with two 16-byte loads per table, all issued before they are used.
+__device__ __forceinline__ void ld8(const int32_t* __restrict__ p, int r0, int* v) {
+    const int4 a = __ldg(reinterpret_cast<const int4*>(p + r0));
+    const int4 b = __ldg(reinterpret_cast<const int4*>(p + r0 + 4));
+    v[0] = a.x; v[1] = a.y; v[2] = a.z; v[3] = a.w;
+    v[4] = b.x; v[5] = b.y; v[6] = b.z; v[7] = b.w;
+}
+__device__ __forceinline__ void st8(int32_t* __restrict__ p, int r0, const int* v) {
+    reinterpret_cast<int4*>(p + r0)[0] = make_int4(v[0], v[1], v[2], v[3]);
+    reinterpret_cast<int4*>(p + r0)[1] = make_int4(v[4], v[5], v[6], v[7]);
+}
+static_assert(PLAN_ROWS == 8, "ld8 / st8 move eight rows");
+
 __global__ void __launch_bounds__(PLAN_THREADS) k_bk_plan(
-    int nrow1, int nr, int ngz, const int32_t* __restrict__ fill_o, const int32_t* __restrict__ cap_o,
+    int nrow1, int ngz, const int32_t* __restrict__ fill_o, const int32_t* __restrict__ cap_o,
     const int32_t* __restrict__ base_o, const int32_t* __restrict__ ovf_o, int64_t ovf_base,
-    int4* __restrict__ items, int32_t* __restrict__ ctl, int32_t* __restrict__ jrk,
+    int4* __restrict__ items, int32_t* __restrict__ ctl,
     const int32_t* __restrict__ want, int32_t* __restrict__ cap_n, int32_t* __restrict__ base_n,
     int32_t* __restrict__ fill_n, int32_t* __restrict__ ovf_n) {
-    __shared__ int s_mn[PLAN_THREADS / 32], s_mx[PLAN_THREADS / 32];
-    const int nrow = nrow1 - 1;
-    int carry_cap = 0, carry_it = 0, rmin = 0x7fffffff, rmax = -1;
+    int carry_cap = 0, carry_it = 0;
     for (int c0 = 0; c0 < nrow1; c0 += PLAN_THREADS * PLAN_ROWS) {
         const int r0 = c0 + threadIdx.x * PLAN_ROWS;
-        int capv[PLAN_ROWS], nit[PLAN_ROWS], val[PLAN_ROWS];
+        int wv[PLAN_ROWS], fv[PLAN_ROWS], cv[PLAN_ROWS], bv[PLAN_ROWS];
+        ld8(want, r0, wv);
+        if (fill_o) {
+            ld8(fill_o, r0, fv);
+            ld8(cap_o, r0, cv);
+            ld8(base_o, r0, bv);
+        }
+        int capv[PLAN_ROWS], nit[PLAN_ROWS], val[PLAN_ROWS], zero[PLAN_ROWS];
         int scap = 0, snit = 0;
 #pragma unroll
         for (int k = 0; k < PLAN_ROWS; k++) {
-            const int r = r0 + k;
-            capv[k] = nit[k] = val[k] = 0;
-            if (r < nrow1) {
-                const int w = want[r];
-                capv[k] = w + (w >> 3) + (w > 0 ? 16 : 0);
-                if (fill_o) {
-                    const int f = fill_o[r];
-                    val[k] = min(f, cap_o[r]);
-                    nit[k] = (val[k] + BK_ITEM - 1) / BK_ITEM;
-                    if (f > 0 && r < nrow) {
-                        rmin = min(rmin, r);
-                        rmax = max(rmax, r);
-                    }
-                }
+            const int w = wv[k];
+            zero[k] = 0;
+            capv[k] = w + (w >> 3) + (w > 0 ? 16 : 0);
+            val[k] = nit[k] = 0;
+            if (fill_o) {
+                val[k] = min(fv[k], cv[k]);
+                nit[k] = (val[k] + BK_ITEM - 1) / BK_ITEM;
             }
             scap += capv[k];
             snit += nit[k];
@@ -140,56 +171,35 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_bk_plan(
         plan_scan2(scap, snit, ecap, eit, tcap, tit);
         ecap += carry_cap;
         eit += carry_it;
+        int basev[PLAN_ROWS];
 #pragma unroll
         for (int k = 0; k < PLAN_ROWS; k++) {
-            const int r = r0 + k;
-            if (r >= nrow1) break;
-            cap_n[r] = capv[k];
-            base_n[r] = ecap;
-            fill_n[r] = 0;
+            basev[k] = ecap;
             ecap += capv[k];
-            if (fill_o) {
-                const int b = base_o[r];
+        }
+        st8(cap_n, r0, capv);
+        st8(base_n, r0, basev);
+        st8(fill_n, r0, zero);
+        if (fill_o) {
+#pragma unroll
+            for (int k = 0; k < PLAN_ROWS; k++) {
+                const int ring = (r0 + k) / ngz;
                 for (int q = 0; q < nit[k]; q++)
-                    items[eit + q] = make_int4(r, b + q * BK_ITEM, b + min((q + 1) * BK_ITEM, val[k]), 0);
+                    items[eit + q] = make_int4(r0 + k, bv[k] + q * BK_ITEM,
+                                               bv[k] + min((q + 1) * BK_ITEM, val[k]), ring);
                 eit += nit[k];
             }
         }
         carry_cap += tcap;
         carry_it += tit;
     }
-    if (fill_o) {
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
-            rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-        }
-        if (lane == 0) {
-            s_mn[warp] = rmin;
-            s_mx[warp] = rmax;
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            for (int w = 0; w < PLAN_THREADS / 32; w++) {
-                rmin = min(rmin, s_mn[w]);
-                rmax = max(rmax, s_mx[w]);
-            }
-            if (rmax >= 0) {
-                jrk[0] = rmin / ngz + 1;
-                jrk[1] = min(rmax / ngz + 2, nr);
-            } else {
-                jrk[0] = nr;
-                jrk[1] = 0;
-            }
-            const int ov = *ovf_o;
-            int it = carry_it;
-            for (int q = 0; q * BK_ITEM < ov; q++, it++)
-                items[it] = make_int4(-1, (int)ovf_base + q * BK_ITEM,
-                                      (int)ovf_base + min((q + 1) * BK_ITEM, ov), 0);
-            ctl[0] = it;
-            ctl[1] = 0;
-        }
+    if (fill_o && threadIdx.x == 0) {
+        const int ov = *ovf_o;
+        int it = carry_it;
+        for (int q = 0; q * BK_ITEM < ov; q++, it++)
+            items[it] = make_int4(-1, (int)ovf_base + q * BK_ITEM, (int)ovf_base + min((q + 1) * BK_ITEM, ov), 0);
+        ctl[0] = it;
+        ctl[1] = 0;
     }
     if (threadIdx.x == 0) *ovf_n = 0;
 }
@@ -226,26 +236,67 @@ __device__ __forceinline__ int64_t bk_slot(bool act, uint32_t rk, const int32_t*
     return dst;
 }
 
+// A particle of the bucketed store is one record of R float4 words, planes
+// of bcap records each (word plane q of record s at Q[q * bcap + s]): its NP
+// floats (x, y[, z], vx, vy[, vz][, the compensated low parts]) then its load
+// index as float bits, zero-padded: two 16-byte accesses per particle in 3D
+// instead of seven 4-byte ones, each with its own 64-bit address.
+template <int NP>
+struct Rec {
+    static constexpr int R = (NP + 1 + 3) / 4;
+};
+
+template <int NP>
+__device__ __forceinline__ void rec_load(const float4* __restrict__ Q, int64_t bcap, int64_t s, float* P,
+                                         int32_t& o) {
+    constexpr int R = Rec<NP>::R;
+    float w[4 * R];
+#pragma unroll
+    for (int q = 0; q < R; q++) {
+        const float4 v = __ldg(Q + q * bcap + s);
+        w[4 * q] = v.x;
+        w[4 * q + 1] = v.y;
+        w[4 * q + 2] = v.z;
+        w[4 * q + 3] = v.w;
+    }
+#pragma unroll
+    for (int k = 0; k < NP; k++) P[k] = w[k];
+    o = __float_as_int(w[NP]);
+}
+
+template <int NP>
+__device__ __forceinline__ void rec_store(float4* __restrict__ Q, int64_t bcap, int64_t s, const float* P,
+                                          int32_t o) {
+    constexpr int R = Rec<NP>::R;
+    float w[4 * R];
+#pragma unroll
+    for (int k = 0; k < 4 * R; k++) w[k] = (k < NP) ? P[k] : 0.f;
+    w[NP] = __int_as_float(o);
+#pragma unroll
+    for (int q = 0; q < R; q++) Q[q * bcap + s] = make_float4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+}
+
 // The fused particle pass of one step.  Persistent CTAs take work items from
 // a counter.  bins: int64 [WROWS][na] over the item's window, zero between
 // items.  Window of an item of row (ir, iz): rings ir - 1 .. ir + 2 and, in
 // 3D, planes iz - 1 .. iz + 2 (bin row 4 a + b for ring ir - 1 + a, plane
 // iz - 1 + b); 2D: rows ir - 1 .. ir + 2.
 template <int ND, bool COMP>
-__global__ void __launch_bounds__(BK_THREADS) k_push_bkt(
-    DevGeo g, const float* __restrict__ Pin, float* __restrict__ Pout, int64_t cap,
-    const int32_t* __restrict__ oin, int32_t* __restrict__ oout, const float4* __restrict__ F,
+__global__ void __launch_bounds__(BK_THREADS, BK_MINB) k_push_bkt(
+    DevGeo g, const float4* __restrict__ Qin, float4* __restrict__ Qout, int64_t bcap,
+    const float4* __restrict__ F,
     const int4* __restrict__ items, int32_t* __restrict__ ctl, const int32_t* __restrict__ cap_o,
     const int32_t* __restrict__ base_o, int32_t* __restrict__ fill_o, int32_t* __restrict__ ovf_o,
     int64_t ovf_base, unsigned long long* __restrict__ acc) {
-    extern __shared__ __align__(16) unsigned long long bins[];
+    extern __shared__ __align__(16) uint32_t bins[];
     __shared__ int s_item;
     constexpr bool d3 = ND == 3;
     constexpr int WROWS = d3 ? 16 : 4;
     constexpr int NW = 2 * ND;
     const int na = g.na, ngz = d3 ? g.ngz : 1, nrow = g.nrow;
     const int nit = ctl[0];
-    for (int i = threadIdx.x; i < WROWS * na; i += BK_THREADS) bins[i] = 0ull;
+    int rmin_l = 0x7fffffff, rmax_l = -1;  // ring range of this lane's new cells
+    for (int i = threadIdx.x; i < WROWS * na; i += BK_THREADS) bins[i] = 0u;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(ctl + 1, 1);
         __syncthreads();  // also orders the previous item's flush before these deposits
@@ -254,19 +305,22 @@ __global__ void __launch_bounds__(BK_THREADS) k_push_bkt(
         const int4 I = items[it];
         const int row = I.x, s0 = I.y, s1 = I.z;
         const bool win = row >= 0 && row < nrow && (s1 - s0) >= BK_SPARSE;
-        // ring and plane of the item's row: the window's origin is one below
-        const int wir = d3 ? row / ngz : row;
+        // ring and plane of the item's row (the plan stores the ring): the
+        // window's origin is one below
+        const int wir = I.w;
         const int wiz = d3 ? row - wir * ngz : 0;
+        constexpr int NP = NW + (COMP ? ND : 0);
+        constexpr int NQC = d3 ? 4 : 2;  // corner rows of a cell
         for (int b0 = s0; b0 < s1; b0 += BK_THREADS) {
             const int s = b0 + threadIdx.x;
             const bool act = s < s1;
-            uint32_t rk = 0;
-            float P[NW + (COMP ? ND : 0)];
+            float P[NP];
             int32_t o = 0;
+            CellW cn;
+            cn.key = -1;
+            uint32_t rk = 0;
             if (act) {
-#pragma unroll
-                for (int k = 0; k < NW + (COMP ? ND : 0); k++) P[k] = Pin[(size_t)k * cap + s];
-                o = oin[s];
+                rec_load<NP>(Qin, bcap, s, P, o);
                 float &x = P[0], &y = P[1];
                 float z = d3 ? P[2] : 0.f;
                 const CellW cw = gx_cell_t<false, ND>(g, x, y, z, true);
@@ -287,85 +341,157 @@ __global__ void __launch_bounds__(BK_THREADS) k_push_bkt(
                     if (d3) P[2] += P[ND + 2];
                 }
                 z = d3 ? P[2] : 0.f;
-                const CellW cn = gx_cell_t<true, ND>(g, x, y, z, false);
+                cn = gx_cell_t<true, ND>(g, x, y, z, false);
                 rk = (cn.key >= 0) ? (uint32_t)cn.row : (uint32_t)nrow;
                 if (cn.key >= 0) {
-                    float w[8];
-                    gx_weights<ND>(g, cn, w);
-                    const int jt0 = cn.jt, jt1 = (cn.jt == na - 1) ? 0 : cn.jt + 1;
-                    // the corner rows: row, row + 1 (the next plane, or ring in
-                    // 2D), and in 3D row + ngz, row + ngz + 1, with their
-                    // window coordinates (a, b)
-                    int fr[4], wa[4], wb[4];
-                    fr[0] = cn.row;
-                    fr[1] = cn.row + 1;
-                    if (d3) {
-                        int ju1 = cn.ju, iz1 = cn.iz + 1;
-                        if (iz1 == ngz) {
-                            iz1 = 0;
-                            ju1 += 1;
-                        }
-                        wa[0] = cn.ju - wir + 1;
-                        wb[0] = cn.iz - wiz + 1;
-                        wa[1] = ju1 - wir + 1;
-                        wb[1] = iz1 - wiz + 1;
-                        fr[2] = cn.row + ngz;
-                        fr[3] = cn.row + ngz + 1;
-                        wa[2] = wa[0] + 1;
-                        wb[2] = wb[0];
-                        wa[3] = wa[1] + 1;
-                        wb[3] = wb[1];
-                    } else {
-                        wa[0] = cn.row - row + 1;
-                        wa[1] = wa[0] + 1;
-                        wb[0] = wb[1] = 0;
-                    }
-                    constexpr int NQ = d3 ? 4 : 2;
+                    rmin_l = min(rmin_l, cn.ju);
+                    rmax_l = max(rmax_l, cn.ju);
+                }
+            }
+            // the row's slot: warp-aggregated atomic on its fill counter,
+            // issued before the deposit so that its latency overlaps it
+            const unsigned lane = threadIdx.x & 31;
+            const uint32_t am = __ballot_sync(0xffffffffu, act);
+            const uint32_t peers = __match_any_sync(0xffffffffu, act ? rk : 0xffffffffu) & am;
+            const int leader = __ffs(peers) - 1;
+            int bslot = 0, capr = 0, baser = 0;
+            if (act && (int)lane == leader) bslot = atomicAdd(fill_o + rk, __popc(peers));
+            if (act) {
+                capr = __ldg(cap_o + rk);
+                baser = __ldg(base_o + rk);
+            }
+            // the common case: every corner inside the window (the new cell
+            // in its inner 3 x 3 rows, or 3 rows in 2D, no plane wrap, inside
+            // the mesh) and no negative weight: eight shared-memory adds
+            int va[8];
+            bool fast = false;
+            if (act && cn.key >= 0) {
+                float w[8];
+                gx_weights<ND>(g, cn, w);
+                int neg = 0;
 #pragma unroll
-                    for (int q = 0; q < NQ; q++) {
-                        if (fr[q] >= nrow) continue;  // past the mesh end: dropped, as massgn does
-                        const int v0 = __float2int_rn(w[2 * q] * BK_FIXQ);
-                        const int v1 = __float2int_rn(w[2 * q + 1] * BK_FIXQ);
-                        const bool inw = win && wa[q] >= 0 && wa[q] < 4 && wb[q] >= 0 && wb[q] < 4;
-                        if (inw) {
-                            unsigned long long* br = bins + (size_t)(d3 ? 4 * wa[q] + wb[q] : wa[q]) * na;
-                            if (v0) atomicAdd(br + jt0, (unsigned long long)(long long)v0);
-                            if (v1) atomicAdd(br + jt1, (unsigned long long)(long long)v1);
-                        } else {
-                            unsigned long long* ar = acc + (size_t)fr[q] * na;
-                            if (v0) red_add_s64(ar + jt0, v0);
-                            if (v1) red_add_s64(ar + jt1, v1);
-                        }
+                for (int k = 0; k < 2 * NQC; k++) {
+                    va[k] = bk_fix(w[k]);
+                    neg |= va[k];
+                }
+                const int a0 = d3 ? cn.ju - wir + 1 : cn.row - row + 1;
+                const int b0 = d3 ? cn.iz - wiz + 1 : 0;
+                fast = win && neg >= 0 && (unsigned)a0 <= 2u && (unsigned)b0 <= 2u &&
+                       (d3 ? (cn.iz + 1 < ngz && cn.ju + 1 < g.nr) : cn.row + 1 < nrow);
+                if (fast) {
+                    const int jt0 = cn.jt, jt1 = (cn.jt == na - 1) ? 0 : cn.jt + 1;
+                    uint32_t* b = bins + (d3 ? 4 * a0 + b0 : a0) * na;
+#pragma unroll
+                    for (int q = 0; q < NQC; q++) {
+                        // corner row q: + 1 (next plane / ring), + ngz (next ring): bin rows + 1, + 4
+                        uint32_t* br = b + (d3 ? (q & 1) + 4 * (q >> 1) : q) * na;
+                        atomicAdd(br + jt0, (uint32_t)va[2 * q]);
+                        atomicAdd(br + jt1, (uint32_t)va[2 * q + 1]);
                     }
                 }
             }
-            const int64_t dst = bk_slot(act, rk, cap_o, base_o, fill_o, ovf_o, ovf_base);
-            if (act) {
+            if (act && cn.key >= 0 && !fast) {
+                const int jt0 = cn.jt, jt1 = (cn.jt == na - 1) ? 0 : cn.jt + 1;
+                // the corner rows: row, row + 1 (the next plane, or ring in
+                // 2D), and in 3D row + ngz, row + ngz + 1, with their window
+                // coordinates (a, b)
+                int fr[4], wa[4], wb[4];
+                fr[0] = cn.row;
+                fr[1] = cn.row + 1;
+                if (d3) {
+                    int ju1 = cn.ju, iz1 = cn.iz + 1;
+                    if (iz1 == ngz) {
+                        iz1 = 0;
+                        ju1 += 1;
+                    }
+                    wa[0] = cn.ju - wir + 1;
+                    wb[0] = cn.iz - wiz + 1;
+                    wa[1] = ju1 - wir + 1;
+                    wb[1] = iz1 - wiz + 1;
+                    fr[2] = cn.row + ngz;
+                    fr[3] = cn.row + ngz + 1;
+                    wa[2] = wa[0] + 1;
+                    wb[2] = wb[0];
+                    wa[3] = wa[1] + 1;
+                    wb[3] = wb[1];
+                } else {
+                    wa[0] = cn.row - row + 1;
+                    wa[1] = wa[0] + 1;
+                    wb[0] = wb[1] = 0;
+                }
+                constexpr int NQ = d3 ? 4 : 2;
 #pragma unroll
-                for (int k = 0; k < NW + (COMP ? ND : 0); k++) Pout[(size_t)k * cap + dst] = P[k];
-                oout[dst] = o;
+                for (int q = 0; q < NQ; q++) {
+                    if (fr[q] >= nrow) continue;  // past the mesh end: dropped, as massgn does
+                    const int v0 = va[2 * q];
+                    const int v1 = va[2 * q + 1];
+                    const bool inw = win && wa[q] >= 0 && wa[q] < 4 && wb[q] >= 0 && wb[q] < 4;
+                    unsigned long long* ar = acc + (size_t)fr[q] * na;
+                    uint32_t* br = bins + (inw ? (d3 ? 4 * wa[q] + wb[q] : wa[q]) * na : 0);
+                    if (inw && v0 > 0) atomicAdd(br + jt0, (uint32_t)v0);
+                    else if (v0) red_add_s64(ar + jt0, v0);
+                    if (inw && v1 > 0) atomicAdd(br + jt1, (uint32_t)v1);
+                    else if (v1) red_add_s64(ar + jt1, v1);
+                }
             }
+            bslot = __shfl_sync(0xffffffffu, bslot, leader < 0 ? 0 : leader);
+            const int slot = bslot + __popc(peers & lanemask_lt());
+            int64_t dst = (int64_t)baser + slot;
+            const bool ovf = act && slot >= capr;
+            const uint32_t om = __ballot_sync(0xffffffffu, ovf);
+            if (om) {
+                const int ol = __ffs(om) - 1;
+                int ob = 0;
+                if ((int)lane == ol) ob = atomicAdd(ovf_o, __popc(om));
+                ob = __shfl_sync(0xffffffffu, ob, ol);
+                if (ovf) dst = ovf_base + ob + __popc(om & lanemask_lt());
+            }
+            if (act) rec_store<NP>(Qout, bcap, dst, P, o);
         }
         if (win) {
             __syncthreads();
-            for (int i = threadIdx.x; i < WROWS * na; i += BK_THREADS) {
-                const unsigned long long v = bins[i];
-                if (v) {
-                    const int wr = i / na, j = i - wr * na;
-                    const int R = d3 ? (wir - 1 + (wr >> 2)) * ngz + (wiz - 1 + (wr & 3)) : wir - 1 + wr;
-                    atomicAdd(acc + (size_t)R * na + j, v);
-                    bins[i] = 0ull;
+#pragma unroll 4
+            for (int wr = 0; wr < WROWS; wr++) {
+                const int R = d3 ? (wir - 1 + (wr >> 2)) * ngz + (wiz - 1 + (wr & 3)) : wir - 1 + wr;
+                uint32_t* br = bins + wr * na;
+                for (int j = threadIdx.x; j < na; j += BK_THREADS) {
+                    const uint32_t v = br[j];
+                    if (v) {
+                        atomicAdd(acc + (size_t)R * na + j, (unsigned long long)v);
+                        br[j] = 0u;
+                    }
                 }
             }
         }
         __syncthreads();  // s_item is rewritten by thread 0 next
+    }
+    // the ring range of the new cells (massgn's jrad / krad): one atomic
+    // pair per warp
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        rmin_l = min(rmin_l, __shfl_xor_sync(0xffffffffu, rmin_l, o));
+        rmax_l = max(rmax_l, __shfl_xor_sync(0xffffffffu, rmax_l, o));
+    }
+    if ((threadIdx.x & 31) == 0 && rmax_l >= 0) {
+        atomicMin(ctl + 5, rmin_l);
+        atomicMax(ctl + 6, rmax_l);
     }
 }
 
 // mass = pmass 2^-20 acc (as k_mass_combine forms it); acc cleared for the
 // next step.  Two cells per thread (mesh is even: na is).
 __global__ void k_mass_convert(unsigned long long* __restrict__ acc, float* __restrict__ mass, int mesh,
-                               float pm) {
+                               float pm, int32_t* __restrict__ rng, int32_t* __restrict__ jrk, int nr) {
+    // the active ring range of the new mass, as massgn tracks it (jrad =
+    // first ring + 1, krad = min(last ring + 2, nr), 1-based), from the ring
+    // range the push gathered (rng[0], rng[1]), which is reset for the next
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        const int mn = rng[0], mx = rng[1];
+        jrk[0] = (mx >= 0) ? mn + 1 : nr;
+        jrk[1] = (mx >= 0) ? min(mx + 2, nr) : 0;
+        rng[0] = 0x7fffffff;
+        rng[1] = -1;
+    }
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     if (i >= mesh) return;
     ulonglong2 v = *reinterpret_cast<const ulonglong2*>(acc + i);
@@ -395,25 +521,28 @@ __global__ void k_bk_rows(DevGeo g, const float* __restrict__ P, int64_t cap, in
     if (act && (peers & lanemask_lt()) == 0) atomicAdd(cnt + rk, (int)__popc(peers));
 }
 
-__global__ void k_bk_scatter(const float* __restrict__ Pin, float* __restrict__ Pout, int64_t cap, int64_t n,
-                             int nplanes, const int32_t* __restrict__ oin, int32_t* __restrict__ oout,
-                             const int32_t* __restrict__ rows, const int32_t* __restrict__ cap_o,
-                             const int32_t* __restrict__ base_o, int32_t* __restrict__ fill_o,
-                             int32_t* __restrict__ ovf_o, int64_t ovf_base) {
+template <int NP>
+__global__ void k_bk_scatter(const float* __restrict__ P, int64_t cap, int64_t n, const int32_t* __restrict__ oin,
+                             float4* __restrict__ Qout, int64_t bcap, const int32_t* __restrict__ rows,
+                             const int32_t* __restrict__ cap_o, const int32_t* __restrict__ base_o,
+                             int32_t* __restrict__ fill_o, int32_t* __restrict__ ovf_o, int64_t ovf_base) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     const bool act = i < n;
     const uint32_t rk = act ? (uint32_t)rows[i] : 0u;
     const int64_t dst = bk_slot(act, rk, cap_o, base_o, fill_o, ovf_o, ovf_base);
     if (!act) return;
-    for (int k = 0; k < nplanes; k++) Pout[(size_t)k * cap + dst] = Pin[(size_t)k * cap + i];
-    oout[dst] = oin[i];
+    float w[NP];
+#pragma unroll
+    for (int k = 0; k < NP; k++) w[k] = P[(size_t)k * cap + i];
+    rec_store<NP>(Qout, bcap, dst, w, oin[i]);
 }
 
-// bucketed store -> n contiguous particles, item by item (CTA-reserved ranges)
-__global__ void k_bk_densify(const float* __restrict__ Pin, float* __restrict__ Pout, int64_t cap,
-                             int nplanes, const int32_t* __restrict__ oin, int32_t* __restrict__ oout,
-                             const int4* __restrict__ items, const int32_t* __restrict__ ctl,
-                             int32_t* __restrict__ dense_ctr) {
+// bucketed store -> n contiguous particles (SoA planes and load index),
+// item by item (CTA-reserved ranges)
+template <int NP>
+__global__ void k_bk_densify(const float4* __restrict__ Qin, int64_t bcap, float* __restrict__ P, int64_t cap,
+                             int32_t* __restrict__ oout, const int4* __restrict__ items,
+                             const int32_t* __restrict__ ctl, int32_t* __restrict__ dense_ctr) {
     __shared__ int s_d0;
     const int nit = ctl[0];
     for (int it = blockIdx.x; it < nit; it += gridDim.x) {
@@ -423,8 +552,12 @@ __global__ void k_bk_densify(const float* __restrict__ Pin, float* __restrict__ 
         const int d0 = s_d0;
         for (int s = I.y + threadIdx.x; s < I.z; s += blockDim.x) {
             const int64_t d = d0 + (s - I.y);
-            for (int k = 0; k < nplanes; k++) Pout[(size_t)k * cap + d] = Pin[(size_t)k * cap + s];
-            oout[d] = oin[s];
+            float w[NP];
+            int32_t o;
+            rec_load<NP>(Qin, bcap, s, w, o);
+#pragma unroll
+            for (int k = 0; k < NP; k++) P[(size_t)k * cap + d] = w[k];
+            oout[d] = o;
         }
         __syncthreads();
     }
@@ -436,6 +569,12 @@ bool gx_fast_ok(const GxCtx* c) {
 }
 
 static inline int bk_nplanes(const GxCtx* c) { return 2 * c->g.ndim + (c->g.comp ? c->g.ndim : 0); }
+
+// float4 words of one record of the bucketed store
+int gx_bucket_words(const GxCtx* c) { return (bk_nplanes(c) + 1 + 3) / 4; }
+
+static inline size_t bk_npad(const GxCtx* c);
+static int bk_plan(GxCtx* c, int out, bool with_items, cudaStream_t st);
 
 template <typename T>
 static int bk_alloc(GxCtx* c, T** p, size_t count) {
@@ -449,8 +588,13 @@ static int bk_alloc(GxCtx* c, T** p, size_t count) {
 }
 
 // row tables and the mass accumulator (grid-sized, once per context)
+static inline size_t bk_npad(const GxCtx* c) {
+    const size_t per = (size_t)PLAN_THREADS * PLAN_ROWS;
+    return ((size_t)c->g.nrow + 1 + per - 1) / per * per;
+}
+
 int gx_bucket_alloc(GxCtx* c) {
-    const size_t nrow1 = (size_t)c->g.nrow + 1;
+    const size_t nrow1 = bk_npad(c);
     int rc = 0;
     for (int b = 0; b < 2 && !rc; b++) {
         rc = rc ? rc : bk_alloc(c, &c->bk_cap[b], nrow1);
@@ -461,50 +605,73 @@ int gx_bucket_alloc(GxCtx* c) {
     rc = rc ? rc : bk_alloc(c, &c->bk_cnt, nrow1);
     rc = rc ? rc : bk_alloc(c, &c->macc, (size_t)c->g.mesh);
     if (rc) return rc;
+    for (int b = 0; b < 2; b++) {
+        GX_CUDA(c, cudaMemsetAsync(c->bk_fill[b], 0, sizeof(int32_t) * nrow1, c->stream));
+        GX_CUDA(c, cudaMemsetAsync(c->bk_cap[b], 0, sizeof(int32_t) * nrow1, c->stream));
+        GX_CUDA(c, cudaMemsetAsync(c->bk_base[b], 0, sizeof(int32_t) * nrow1, c->stream));
+    }
     GX_CUDA(c, cudaMemsetAsync(c->macc, 0, sizeof(unsigned long long) * c->g.mesh, c->stream));
-    GX_CUDA(c, cudaMemsetAsync(c->bk_ctl, 0, sizeof(int32_t) * 16, c->stream));
+    const int32_t ctl0[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0x7fffffff, -1, 0};
+    GX_CUDA(c, cudaMemcpyAsync(c->bk_ctl, ctl0, sizeof ctl0, cudaMemcpyHostToDevice, c->stream));
+    GX_CUDA(c, cudaStreamSynchronize(c->stream));
     return GX_OK;
 }
 
-static int bk_plan(GxCtx* c, int out, bool with_items) {
+static int bk_plan(GxCtx* c, int out, bool with_items, cudaStream_t st) {
     const DevGeo& g = c->g;
     const int nxt = out ^ 1;
-    k_bk_plan<<<1, PLAN_THREADS, 0, c->stream>>>(
-        g.nrow + 1, g.nr, g.ngz, with_items ? c->bk_fill[out] : nullptr, c->bk_cap[out], c->bk_base[out],
-        c->bk_ctl + 4 * out, c->bk_main, c->bk_items, c->bk_ctl + 8, c->jrk_d,
+    k_bk_plan<<<1, PLAN_THREADS, 0, st>>>(
+        g.nrow + 1, g.ngz, with_items ? c->bk_fill[out] : nullptr, c->bk_cap[out], c->bk_base[out],
+        c->bk_ctl + 4 * out, c->bk_main, c->bk_items, c->bk_ctl + 8,
         with_items ? c->bk_fill[out] : c->bk_cnt, c->bk_cap[nxt], c->bk_base[nxt], c->bk_fill[nxt],
         c->bk_ctl + 4 * nxt);
     GX_LAUNCHED(c);
     return GX_OK;
 }
 
-// dense pbuf[cur] -> bucketed pbuf[cur ^ 1] (becomes cur)
+template <int NP>
+static void bk_scatter_launch(GxCtx* c, unsigned nb, int b) {
+    k_bk_scatter<NP><<<nb, 256, 0, c->stream>>>(c->pbuf[c->cur], c->cap, c->n, c->origin, c->bq[b], c->bcap,
+                                                c->pkey[0], c->bk_cap[b], c->bk_base[b], c->bk_fill[b],
+                                                c->bk_ctl + 4 * b, c->bk_main);
+}
+
+template <int NP>
+static void bk_densify_launch(GxCtx* c, int32_t* ctr) {
+    k_bk_densify<NP><<<148 * 8, 256, 0, c->stream>>>(c->bq[c->bcur], c->bcap, c->pbuf[c->cur], c->cap,
+                                                     c->origin, c->bk_items, c->bk_ctl + 8, ctr);
+}
+
+// the dense store pbuf[cur] -> the bucketed store bq[b], b = bcur ^ 1
+// (becomes bcur); the dense store is left as it was, and is stale from the
+// first fused step on
 static int gx_bucketize(GxCtx* c) {
     const DevGeo& g = c->g;
     const int64_t n = c->n;
-    const int cur = c->cur, nxt = cur ^ 1;
+    const int b = c->bcur ^ 1;
     const unsigned nb = (unsigned)((std::max<int64_t>(n, 1) + 255) / 256);
-    GX_CUDA(c, cudaMemsetAsync(c->bk_cnt, 0, sizeof(int32_t) * (g.nrow + 1), c->stream));
+    GX_CUDA(c, cudaMemsetAsync(c->bk_cnt, 0, sizeof(int32_t) * bk_npad(c), c->stream));
     if (n > 0) {
         auto kr = (g.ndim == 3) ? k_bk_rows<3> : k_bk_rows<2>;
-        kr<<<nb, 256, 0, c->stream>>>(g, c->pbuf[cur], c->cap, n, c->pkey[0], c->bk_cnt);
+        kr<<<nb, 256, 0, c->stream>>>(g, c->pbuf[c->cur], c->cap, n, c->pkey[0], c->bk_cnt);
         GX_LAUNCHED(c);
     }
-    // segments of pbuf[nxt] from the exact counts (with_items = false plans
-    // the layout of buffer "out ^ 1" = nxt from want = bk_cnt)
-    int rc = bk_plan(c, cur, false);
+    // segments of bq[b] from the exact counts (with_items = false plans the
+    // layout of buffer "out ^ 1" = b from want = bk_cnt)
+    int rc = bk_plan(c, b ^ 1, false, c->stream);
     if (rc) return rc;
     if (n > 0) {
-        k_bk_scatter<<<nb, 256, 0, c->stream>>>(c->pbuf[cur], c->pbuf[nxt], c->cap, n, bk_nplanes(c), c->origin,
-                                                c->origin_tmp, c->pkey[0], c->bk_cap[nxt], c->bk_base[nxt],
-                                                c->bk_fill[nxt], c->bk_ctl + 4 * nxt, c->bk_main);
+        switch (bk_nplanes(c)) {
+            case 4: bk_scatter_launch<4>(c, nb, b); break;
+            case 6: bk_scatter_launch<6>(c, nb, b); break;
+            default: bk_scatter_launch<9>(c, nb, b); break;
+        }
         GX_LAUNCHED(c);
     }
-    // items of pbuf[nxt]; segments of pbuf[cur] for the first fused pass
-    rc = bk_plan(c, nxt, true);
+    // items of bq[b]; segments of bq[b ^ 1] for the first fused pass
+    rc = bk_plan(c, b, true, c->stream);
     if (rc) return rc;
-    std::swap(c->origin, c->origin_tmp);
-    c->cur = nxt;
+    c->bcur = b;
     c->bucketed = true;
     c->have_keys = false;
     return GX_OK;
@@ -515,20 +682,23 @@ __global__ void k_bk_iota(int32_t* p, int64_t n) {
     if (i < n) p[i] = (int32_t)i;
 }
 
+// bucketed store -> the dense store pbuf[cur] (its SoA planes and load
+// index), in the store's row order; the processing order becomes the
+// identity
 int gx_dense(GxCtx* c) {
     if (!c->bucketed) return GX_OK;
-    const int cur = c->cur, nxt = cur ^ 1;
     int32_t* ctr = c->bk_ctl + 12;
     GX_CUDA(c, cudaMemsetAsync(ctr, 0, sizeof(int32_t), c->stream));
-    k_bk_densify<<<148 * 8, 256, 0, c->stream>>>(c->pbuf[cur], c->pbuf[nxt], c->cap, bk_nplanes(c), c->origin,
-                                                 c->origin_tmp, c->bk_items, c->bk_ctl + 8, ctr);
+    switch (bk_nplanes(c)) {
+        case 4: bk_densify_launch<4>(c, ctr); break;
+        case 6: bk_densify_launch<6>(c, ctr); break;
+        default: bk_densify_launch<9>(c, ctr); break;
+    }
     GX_LAUNCHED(c);
     if (c->n > 0) {
         k_bk_iota<<<(unsigned)((c->n + 255) / 256), 256, 0, c->stream>>>(c->perm, c->n);
         GX_LAUNCHED(c);
     }
-    std::swap(c->origin, c->origin_tmp);
-    c->cur = nxt;
     c->bucketed = false;
     c->have_keys = false;
     return GX_OK;
@@ -537,7 +707,7 @@ int gx_dense(GxCtx* c) {
 template <int ND, bool COMP>
 static int bk_launch_push(GxCtx* c, int cur, int nxt) {
     const DevGeo& g = c->g;
-    const size_t sm = sizeof(unsigned long long) * (ND == 3 ? 16 : 4) * g.na;
+    const size_t sm = sizeof(uint32_t) * (ND == 3 ? 16 : 4) * g.na;
     auto kp = k_push_bkt<ND, COMP>;
     GX_CUDA(c, cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     if (!c->bk_grid) {
@@ -546,17 +716,31 @@ static int bk_launch_push(GxCtx* c, int cur, int nxt) {
         GX_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
         c->bk_grid = std::max(1, per) * sms;
     }
-    kp<<<c->bk_grid, BK_THREADS, sm, c->stream>>>(g, c->pbuf[cur], c->pbuf[nxt], c->cap, c->origin,
-                                                  c->origin_tmp, c->field, c->bk_items, c->bk_ctl + 8,
-                                                  c->bk_cap[nxt], c->bk_base[nxt], c->bk_fill[nxt],
-                                                  c->bk_ctl + 4 * nxt, c->bk_main, c->macc);
+    kp<<<c->bk_grid, BK_THREADS, sm, c->stream>>>(g, c->bq[cur], c->bq[nxt], c->bcap, c->field, c->bk_items,
+                                                  c->bk_ctl + 8, c->bk_cap[nxt], c->bk_base[nxt],
+                                                  c->bk_fill[nxt], c->bk_ctl + 4 * nxt, c->bk_main, c->macc);
     GX_LAUNCHED(c);
+    return GX_OK;
+}
+
+// the main stream waits for the plan queued on the side stream
+static int bk_join(GxCtx* c) {
+    if (!c->bk_pending) return GX_OK;
+    GX_CUDA(c, cudaStreamWaitEvent(c->stream, c->bk_ev[1], 0));
+    c->bk_pending = false;
     return GX_OK;
 }
 
 int gx_fast_step(GxCtx* c, int nsteps, int phys) {
     const DevGeo& g = c->g;
     int rc;
+    if (!c->bk_side) {
+        int lo = 0, hi = 0;
+        GX_CUDA(c, cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        GX_CUDA(c, cudaStreamCreateWithPriority(&c->bk_side, cudaStreamNonBlocking, hi));
+        GX_CUDA(c, cudaEventCreateWithFlags(&c->bk_ev[0], cudaEventDisableTiming));
+        GX_CUDA(c, cudaEventCreateWithFlags(&c->bk_ev[1], cudaEventDisableTiming));
+    }
     if (!c->bucketed) {
         rc = gx_bucketize(c);
         if (rc) return rc;
@@ -565,24 +749,39 @@ int gx_fast_step(GxCtx* c, int nsteps, int phys) {
         const bool last = (s == nsteps - 1);
         rc = gx_mixed_findf(c, phys && last, true);
         if (rc) return rc;
-        const int cur = c->cur, nxt = cur ^ 1;
+        const int cur = c->bcur, nxt = cur ^ 1;
+        rc = bk_join(c);
+        if (rc) return rc;
         rc = gx_phase_mark(c, PH_PUSH);
         if (rc) return rc;
         if (g.ndim == 3) rc = g.comp ? bk_launch_push<3, true>(c, cur, nxt) : bk_launch_push<3, false>(c, cur, nxt);
         else rc = g.comp ? bk_launch_push<2, true>(c, cur, nxt) : bk_launch_push<2, false>(c, cur, nxt);
         if (rc) return rc;
-        rc = gx_phase_mark(c, PH_SORT);
-        if (rc) return rc;
-        rc = bk_plan(c, nxt, true);
-        if (rc) return rc;
+        if (c->prof) {
+            // profile mode: the plan in line, so that it has a phase time
+            rc = gx_phase_mark(c, PH_SORT);
+            if (rc) return rc;
+            rc = bk_plan(c, nxt, true, c->stream);
+            if (rc) return rc;
+        } else {
+            // the plan needs only the push: it runs on the side stream while
+            // the next field solve runs, and the next push waits for it
+            GX_CUDA(c, cudaEventRecord(c->bk_ev[0], c->stream));
+            GX_CUDA(c, cudaStreamWaitEvent(c->bk_side, c->bk_ev[0], 0));
+            rc = bk_plan(c, nxt, true, c->bk_side);
+            if (rc) return rc;
+            GX_CUDA(c, cudaEventRecord(c->bk_ev[1], c->bk_side));
+            c->bk_pending = true;
+        }
         rc = gx_phase_mark(c, PH_COMBINE);
         if (rc) return rc;
-        k_mass_convert<<<(unsigned)((g.mesh / 2 + 255) / 256), 256, 0, c->stream>>>(c->macc, c->mass, g.mesh,
-                                                                                   g.pmass);
+        k_mass_convert<<<(unsigned)((g.mesh / 2 + 255) / 256), 256, 0, c->stream>>>(
+            c->macc, c->mass, g.mesh, g.pmass, c->bk_ctl + 13, c->jrk_d, g.nr);
         GX_LAUNCHED(c);
-        std::swap(c->origin, c->origin_tmp);
-        c->cur = nxt;
+        c->bcur = nxt;
     }
+    rc = bk_join(c);
+    if (rc) return rc;
     rc = gx_phase_end(c);
     if (rc) return rc;
     c->have_field = false;

@@ -15,6 +15,7 @@
 // ---------------------------------------------------------------------------
 // particles per deposit work item (bounds the fixed-point bin sums)
 #define DEP_CH 2047  // particles per deposit item (int32 bins: see gx_deposit.cu)
+#define BK_ITEM 4095 // particles per work item of the fused pass (u32 bins: see gx_bucket.cu)
 // striped copies of the row counters (copy = block index mod NCOPY); spreads
 // the integer atomics of row-sorted particles over NCOPY addresses per row
 #define NCOPY 32
@@ -136,12 +137,15 @@ struct GxCtx {
     // diagnostics scratch
     double* dsum = nullptr;
 
-    // phase timing (gx_set_profile): events around the phases of a step
+    // phase timing (gx_set_profile): an event at every phase mark, recorded
+    // without waiting, read back at gx_phase_end (so the kernels still run
+    // back to back and a phase's time holds no host launch gap)
     bool prof = false;
-    cudaEvent_t pev[GX_NPHASE + 1] = {};
+    std::vector<cudaEvent_t> pev;          // event pool
+    std::vector<int> pev_ph;               // phase opened by each recorded mark (-1: end)
+    int nmarks = 0;
     float phase_ms[GX_NPHASE] = {};
     int64_t phase_n[GX_NPHASE] = {};
-    int open_phase = -1;
 
     // time-step zones (gx_zones.cu); nzones = 1 is the single-zone step
     int nzones = 1;
@@ -156,22 +160,29 @@ struct GxCtx {
     int lstep[GX_MAX_ZONES][2] = {};         // step numbers of zold, znew
     bool zones_ready = false;                // zone arrays deposited (gx_masset)
 
-    // bucketed particle store of the fused step (gx_bucket.cu): pbuf[b] holds
+    // bucketed particle store of the fused step (gx_bucket.cu): bq[b] holds
     // one segment of slots per ring-plane row (row nrow: off the grid),
     // [bk_base[b][r], + bk_cap[b][r]), of which the first
     // min(bk_fill[b][r], bk_cap[b][r]) are particles, then an overflow area
     // of bk_ctl[b][0] particles from slot bk_main on
     bool bucketed = false;
+    float4* bq[2] = {nullptr, nullptr};       // records of R float4 words, R planes of bcap each
+    int64_t bcap = 0;                         // records per plane: bk_main + an overflow area of n
+    int bcur = 0;                             // the bucketed store's current buffer
     int64_t bk_main = 0;
     int32_t* bk_cap[2] = {nullptr, nullptr};
     int32_t* bk_base[2] = {nullptr, nullptr};
     int32_t* bk_fill[2] = {nullptr, nullptr};
-    int32_t* bk_ctl = nullptr;               // [2][4]: overflow count of each buffer; [8] items, [9] work counter
+    int32_t* bk_ctl = nullptr;               // [2][4]: overflow count of each buffer; [8] items, [9] work
+                                             // counter, [12] compaction counter, [13..14] ring range
     int4* bk_items = nullptr;                // work items of pbuf[cur]: row (-1: overflow), first, end slot
     int64_t bk_maxitems = 0;
     int32_t* bk_cnt = nullptr;               // [nrow + 1] row counts of the dense store (bucketing)
     unsigned long long* macc = nullptr;      // [mesh] fixed-point mass (2^-20 of a particle), zero between steps
     int bk_grid = 0;                         // CTAs of the fused pass
+    cudaStream_t bk_side = nullptr;          // the plan's stream (overlaps the field solve)
+    cudaEvent_t bk_ev[2] = {nullptr, nullptr};  // push done (main), plan done (side)
+    bool bk_pending = false;                 // a plan on bk_side the main stream has not joined
 
     // multi-GPU (gx_comm.cu): NCCL communicator of the particle decomposition
     void* comm = nullptr;
@@ -678,6 +689,7 @@ bool gx_fast_ok(const GxCtx* c);  // single zone, linear scheme, mixed, not GX_F
 int gx_fast_step(GxCtx* c, int nsteps, int phys);
 int gx_dense(GxCtx* c);  // bucketed store -> dense store (no-op when dense)
 int gx_bucket_alloc(GxCtx* c);
+int gx_bucket_words(const GxCtx* c);  // float4 words per record of the bucketed store
 int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk = nullptr);
 int gx_comm_reduce_spectrum(GxCtx* c);
 void gx_comm_destroy(GxCtx* c);
