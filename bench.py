@@ -389,7 +389,7 @@ def run_sfp(n=20_000_000, reps=5):
     from galaxy_b200.sfp import Basis, Sfp
     basis = Basis.from_json(os.path.join(ROOT, "tests", "golden", "aj07.json"), maxm=8, maxn=19)
     pos = exp_disk(n, seed=12345)
-    out = {"workload": "sfp2d-aj07-m0..8-n0..19-20M"}
+    out = {"workload": f"sfp2d-aj07-m0..8-n0..19-{n // 1_000_000}M"}
     with Sfp(basis, 6.0) as s:
         s.load(pos)
         s.sum(1.0 / n, 0)
@@ -468,6 +468,12 @@ def run_ensemble(ndisc=64, steps=1000, loop_steps=20, seed=12345):
         err = max(err, float(np.abs(p_ens[d][:, :2] - ref).max() / np.abs(ref).max()))
     rate = ntot * steps / (ms * 1e-3)
     rate_loop = ntot * loop_steps / (t_loop * 1e-3)
+    # algorithmic bytes of one ensemble step: every particle's phase space read
+    # and written (2 x 2 x 2 x 4 B) and each disc's mass and (fx, fy) grids
+    # written and read once (64 x 128 cells x 4 B x (2 + 2 x 2))
+    peak, src = peaks()
+    eb = 32 * ntot + ndisc * 64 * 128 * 4 * 6
+    ach = eb / (ms / steps * 1e-3) / 1e9
     return {"workload": f"ensemble2d-{ndisc}x64x128-{ntot}", "discs": ndisc, "particles": ntot,
             "steps": steps, "ms_per_step": round(ms / steps, 4), "particle_steps_per_s": rate,
             "launches_per_step": launches / steps, "cuda_graph": conf["graph"],
@@ -476,7 +482,10 @@ def run_ensemble(ndisc=64, steps=1000, loop_steps=20, seed=12345):
                              "ms_per_step_all_discs": round(t_loop / loop_steps, 4)},
             "speedup_vs_per_run_loop": round(rate / rate_loop, 2),
             "max_pos_rel_diff_vs_per_run_loop": err,
-            "a2_final_abs_mean": float(np.abs(a2[-1]).mean())}
+            "a2_final_abs_mean": float(np.abs(a2[-1]).mean()),
+            "roofline": {"kernel": "k_ens_step", "bound": "hbm", "achieved": round(ach, 1), "peak": peak,
+                         "unit": "GB/s", "frac": round(ach / peak, 4), "algorithmic_bytes": eb,
+                         "peak_source": src}}
 
 
 def run_adjoint(n=1_000_000, steps=400, ckpt=50, n_check=20_000, steps_check=50):
@@ -585,8 +594,14 @@ def main():
     ap.add_argument("--no-sfp", action="store_true")
     ap.add_argument("--no-ens", action="store_true")
     ap.add_argument("--no-adj", action="store_true")
+    ap.add_argument("--sfp-only", action="store_true",
+                    help="run only the SFP coefficient sum and print its JSON (profiling)")
+    ap.add_argument("--sfp-n", type=int, default=20_000_000, help="particles of the SFP sum")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.sfp_only:
+        print(json.dumps(run_sfp(args.sfp_n)))
+        return
     w = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
