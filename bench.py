@@ -165,13 +165,13 @@ def phase_bytes(cfg, geo, n):
     spec = nact * nkz * geo.nr * 16
     ntypes = 3 if d == 3 else 2
     return {
-        "push": n * 2 * 2 * d * 4,                        # phase space read + write
+        # the fused pass: phase space read + written, the mass it deposits
+        "push": n * 2 * 2 * d * 4 + mesh * 4,
         "conv": npairs * geo.nr * geo.nr * 4 + spec * (1 + ntypes),
         "syn": spec * ntypes + mesh * 16,                 # spectra in, float4 field out
         "fwd": mesh * 4 + spec,
-        "deposit": n * (d * 4 + 4) + mesh * 4,            # positions + order in, mass out
-        "sort": n * 8 * 2,                                # (row key, index) in and out
-        "combine": mesh * 4,
+        "sort": (geo.nr * geo.ngz + 1) * 4 * 6,           # the plan: row tables in and out
+        "combine": mesh * (8 + 4),                        # fixed-point mass in, mass out
     }
 
 
@@ -181,8 +181,8 @@ def step_bytes(cfg, geo, n):
     return n * 2 * 2 * cfg.ndim * 4 + npairs * geo.nr * geo.nr * 4 + geo.mesh * 4 * (2 + 2 * nf)
 
 
-KERNEL_OF = {"push": "k_push", "conv": "k_conv", "syn": "k_syn3", "fwd": "k_fwd3",
-             "deposit": "k_deposit", "sort": "k_sort_scatter", "combine": "k_mass_combine"}
+KERNEL_OF = {"push": "k_push_bkt", "conv": "k_conv_bulk", "syn": "k_synz_tc+k_synaz",
+             "fwd": "k_fwd_az+k_fwd_z", "sort": "k_bk_plan", "combine": "k_mass_convert"}
 
 
 def ncu_traffic(workload):
@@ -202,6 +202,7 @@ def run_ours(args, w, rank, world, comm):
     rec, pm = make_ic(w, n, seed=12345 + rank)
     out = {}
     cfg = make_cfg(w, GX_PREC_MIXED)
+    cfg.flags = args.flags
     cfg.pmass = pm / world          # the ranks' discs together carry the disc mass
     cfg.device = int(os.environ.get("LOCAL_RANK", 0))
     gal = Galaxy(cfg)
@@ -589,6 +590,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT, choices=sorted(WORKLOADS))
     ap.add_argument("--n", type=int, default=0, help="particles per GPU (default: workload)")
+    ap.add_argument("--flags", type=int, default=0,
+                    help="context flags GX_FLAG_* of the timed context (e.g. 8: the sorted deposit)")
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-sfp", action="store_true")
@@ -610,6 +613,8 @@ def main():
             "harmonics": f"0..{w['ng'] - 1}", "particles_per_gpu": n, "dt": w["dt"],
             "softening": w["softl"], "rings": f"log-spaced {w['r0']}..{w['r1']}",
             "l2": "inputs larger than L2 (no flush)"}
+    if args.flags:
+        wcfg["flags"] = args.flags
     if args.impl == "reference":
         if rank != 0:
             return

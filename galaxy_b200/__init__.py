@@ -19,7 +19,8 @@ from ._abi import (GxConfig, GxDiag, GxGeometry, make_config, GX_OK, GX_PREC_FP6
                    GX_SOFT_SPLINE, GX_GRID_MASS, GX_GRID_FR, GX_GRID_FT, GX_GRID_FZ,
                    GX_GRID_POT, GX_GRID_FX, GX_GRID_FY, GX_GREEN_FR, GX_GREEN_FT,
                    GX_GREEN_FZ, GX_GREEN_POT, GX_FLAG_COMPENSATED,
-                   GX_FLAG_QUADRATIC, GX_FLAG_WHOLE_GRID, GX_FLAG_SORTED_DEPOSIT)
+                   GX_FLAG_QUADRATIC, GX_FLAG_WHOLE_GRID, GX_FLAG_SORTED_DEPOSIT,
+                   GX_FLAG_PLANE_SPLIT)
 
 __all__ = ["Galaxy", "GxError", "GxConfig", "GxDiag", "GxGeometry", "make_config", "lib",
            "LIB_PATH"]
@@ -67,6 +68,7 @@ def lib():
         L.gx_last_launch_count.argtypes = [P, C.POINTER(C.c_int64)]
         L.gx_comm_unique_id.argtypes = [C.c_char_p]
         L.gx_comm_init.argtypes = [P, C.c_char_p, C.c_int, C.c_int]
+        L.gx_comm_host.argtypes = [P, C.c_int, C.c_int, P, P]
         L.gx_host_alloc.argtypes = [i64, C.POINTER(P)]
         L.gx_host_free.argtypes = [P]
         L.gx_set_profile.argtypes = [P, C.c_int]

@@ -255,7 +255,7 @@ void gx_destroy(GxCtx* c) {
     void* ptrs[] = {c->green32, c->green64, c->pbuf[0], c->pbuf[1], c->perm, c->origin,
                     c->origin_tmp, c->pkey[0], c->pkey[1], c->pfr, c->p64, c->key64, c->w64, c->acc64, c->ppot,
                     c->pacc, c->mass, c->mass64, c->field, c->polar, c->field64, c->polar64,
-                    c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->az64, c->rows64, c->pot64, c->perm_next, c->rowstart,
+                    c->specS, c->specO, c->syntab, c->synR, c->fwdtab, c->fwdC1, c->spec64, c->out64, c->az64, c->rows64, c->pot64, c->stagebuf, c->perm_next, c->rowstart,
                     c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->rowtile, c->stage, c->jrk_d,
                     c->errword, c->dsum, c->pzone[0], c->pzone[1], c->zbuf, c->zjrk_d, c->act_d,
                     c->bk_cap[0], c->bk_cap[1], c->bk_base[0], c->bk_base[1], c->bk_fill[0], c->bk_fill[1],
@@ -406,6 +406,8 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     c->key64 = nullptr;
     c->w64 = c->acc64 = c->pot64 = nullptr;
     c->ppot = c->pacc = nullptr;
+    if (c->stagebuf) cudaFree(c->stagebuf);
+    c->stagebuf = nullptr;
     c->perm_next = nullptr;
     c->items = nullptr;
     c->stage = nullptr;
@@ -419,6 +421,9 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     c->cap = cap;
     DALLOC(c, c->ppot, cap);
     DALLOC(c, c->pacc, 3 * cap);
+    // staging of the host records (AoS) for loadup and unload, once per
+    // capacity: a per-call allocation would map and unmap it every time
+    DALLOC(c, c->stagebuf, (size_t)nw * cap);
     if (c->fp64) {
         DALLOC(c, c->p64, nw * cap);
         DALLOC(c, c->key64, cap);
@@ -470,8 +475,7 @@ int gx_loadup(GxCtx* c, const float* coords, int64_t n) {
     c->bucketed = false;
     const int nw = 2 * c->g.ndim;
     if (n == 0) return (c->nzones > 1 && !c->fp64) ? gx_zone_loadup(c) : GX_OK;
-    float* staging = nullptr;
-    GX_CUDA(c, cudaMallocAsync((void**)&staging, sizeof(float) * nw * n, c->stream));
+    float* staging = c->stagebuf;
     GX_CUDA(c, cudaMemcpyAsync(staging, coords, sizeof(float) * nw * n, cudaMemcpyHostToDevice,
                                c->stream));
     int bs = 256;
@@ -495,7 +499,6 @@ int gx_loadup(GxCtx* c, const float* coords, int64_t n) {
             if (rc) return rc;
         }
     }
-    GX_CUDA(c, cudaFreeAsync(staging, c->stream));
     GX_CUDA(c, cudaStreamSynchronize(c->stream));
     return GX_OK;
 }
@@ -508,8 +511,7 @@ int gx_unload(GxCtx* c, float* coords) {
     if (rc) return rc;
     const int nw = 2 * c->g.ndim;
     const int64_t n = c->n;
-    float* staging = nullptr;
-    GX_CUDA(c, cudaMallocAsync((void**)&staging, sizeof(float) * nw * n, c->stream));
+    float* staging = c->stagebuf;
     int bs = 256;
     int64_t nb = (n + bs - 1) / bs;
     if (c->fp64) k_soa64_to_aos<<<nb, bs, 0, c->stream>>>(c->p64, staging, n, c->cap, nw);
@@ -521,7 +523,6 @@ int gx_unload(GxCtx* c, float* coords) {
     }
     GX_CUDA(c, cudaMemcpyAsync(coords, staging, sizeof(float) * nw * n, cudaMemcpyDeviceToHost,
                                c->stream));
-    GX_CUDA(c, cudaFreeAsync(staging, c->stream));
     GX_CUDA(c, cudaStreamSynchronize(c->stream));
     return GX_OK;
 }

@@ -89,6 +89,7 @@ extern "C" int gx_comm_init(GxCtx* c, const char* id128, int nranks, int rank) {
     ncclComm_t comm = nullptr;
     GX_NCCL(c, a->commInitRank(&comm, nranks, id, rank));
     c->comm = comm;
+    c->host_fn = nullptr;
     c->nranks = nranks;
     c->rank = rank;
     return GX_OK;
@@ -104,9 +105,40 @@ void gx_comm_destroy(GxCtx* c) {
     c->comm = nullptr;
 }
 
+extern "C" int gx_comm_host(GxCtx* c, int nranks, int rank, gx_host_reduce_fn fn, void* user) {
+    if (!c || !fn || nranks < 1 || rank < 0 || rank >= nranks) return GX_ERR_ARG;
+    if (c->fp64) return c->err = "the multi-GPU exchange runs on the mixed path", GX_ERR_ARG;
+    gx_comm_destroy(c);
+    c->host_fn = fn;
+    c->host_user = user;
+    c->nranks = nranks;
+    c->rank = rank;
+    return GX_OK;
+}
+
+// one exchange through the host: device -> host, the caller's reduction,
+// host -> device (all on the context stream, synchronised)
+static int host_reduce(GxCtx* c, void* dptr, int64_t count, int dtype, int op) {
+    const size_t bytes = (size_t)count * 4;
+    if (c->host_buf.size() < bytes) c->host_buf.resize(bytes);
+    void* h = c->host_buf.data();
+    GX_CUDA(c, cudaMemcpyAsync(h, dptr, bytes, cudaMemcpyDeviceToHost, c->stream));
+    GX_CUDA(c, cudaStreamSynchronize(c->stream));
+    if (c->host_fn(c->host_user, op, dtype, h, count) != 0)
+        return c->err = "the host reduction of the ranks failed", GX_ERR_STATE;
+    GX_CUDA(c, cudaMemcpyAsync(dptr, h, bytes, cudaMemcpyHostToDevice, c->stream));
+    GX_CUDA(c, cudaStreamSynchronize(c->stream));
+    return GX_OK;
+}
+
 // MIN/MAX of the 1-based active ring range (massum.f:54-65)
 int gx_comm_reduce_range(GxCtx* c) {
-    if (!c->comm || c->nranks < 2) return GX_OK;
+    if (c->nranks < 2) return GX_OK;
+    if (c->host_fn) {
+        int rc = host_reduce(c, c->jrk_d, 1, GX_DT_INT32, GX_OP_MIN);
+        return rc ? rc : host_reduce(c, c->jrk_d + 1, 1, GX_DT_INT32, GX_OP_MAX);
+    }
+    if (!c->comm) return GX_OK;
     NcclApi* a = nccl();
     GX_NCCL(c, a->allReduce(c->jrk_d, c->jrk_d, 1, ncclInt32, ncclMin, (ncclComm_t)c->comm,
                             c->stream));
@@ -115,12 +147,31 @@ int gx_comm_reduce_range(GxCtx* c) {
     return GX_OK;
 }
 
+static int reduce_sum_f32(GxCtx* c, float* p, size_t count) {
+    if (c->nranks < 2) return GX_OK;
+    if (c->host_fn) return host_reduce(c, p, (int64_t)count, GX_DT_FLOAT32, GX_OP_SUM);
+    if (!c->comm) return GX_OK;
+    NcclApi* a = nccl();
+    GX_NCCL(c, a->allReduce(p, p, count, ncclFloat32, ncclSum, (ncclComm_t)c->comm, c->stream));
+    return GX_OK;
+}
+
 // sum of the forward spectrum over ranks (p2manlp.f:208, p3manlp.f:102)
 int gx_comm_reduce_spectrum(GxCtx* c) {
-    if (!c->comm || c->nranks < 2) return GX_OK;
-    NcclApi* a = nccl();
-    const size_t count = (size_t)4 * c->spec.nact * c->g.nkz * c->g.nr;
-    GX_NCCL(c, a->allReduce(c->specS, c->specS, count, ncclFloat32, ncclSum, (ncclComm_t)c->comm,
-                            c->stream));
-    return GX_OK;
+    return reduce_sum_f32(c, reinterpret_cast<float*>(c->specS),
+                          (size_t)4 * c->spec.nact * c->g.nkz * c->g.nr);
+}
+
+// the plane split's exchange: every rank contracted its own vertical
+// wavenumbers and left the others zero, so the sum over ranks is every
+// rank's full contracted spectrum (p3convp.f:276-326 sends and receives
+// the planes)
+int gx_comm_reduce_conv(GxCtx* c) {
+    return reduce_sum_f32(c, reinterpret_cast<float*>(c->specO),
+                          (size_t)4 * 4 * c->spec.nact * c->g.nkz * c->g.nr);
+}
+
+bool gx_plane_split(const GxCtx* c) {
+    return (c->cfg.flags & GX_FLAG_PLANE_SPLIT) && c->nranks > 1 && c->g.ndim == 3 &&
+           (c->comm || c->host_fn);
 }

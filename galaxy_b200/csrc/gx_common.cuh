@@ -93,6 +93,7 @@ struct GxCtx {
     double* w64 = nullptr;                 // [8][cap]
     double* acc64 = nullptr;               // [3][cap]
     float* ppot = nullptr;                 // per-particle potential (analysis)
+    float* stagebuf = nullptr;             // [2 ndim][cap] host record staging (loadup, unload)
     float* pacc = nullptr;                 // per-particle acceleration (getacc)
 
     // grids
@@ -187,6 +188,9 @@ struct GxCtx {
     // multi-GPU (gx_comm.cu): NCCL communicator of the particle decomposition
     void* comm = nullptr;
     int nranks = 1, rank = 0;
+    gx_host_reduce_fn host_fn = nullptr;     // exchanges through the host (gx_comm_host)
+    void* host_user = nullptr;
+    std::vector<char> host_buf;
 };
 
 // record the start of phase ph (prof mode) and close the previous one
@@ -692,4 +696,6 @@ int gx_bucket_alloc(GxCtx* c);
 int gx_bucket_words(const GxCtx* c);  // float4 words per record of the bucketed store
 int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk = nullptr);
 int gx_comm_reduce_spectrum(GxCtx* c);
+int gx_comm_reduce_conv(GxCtx* c);    // sum of the contracted spectra (plane split)
+bool gx_plane_split(const GxCtx* c);
 void gx_comm_destroy(GxCtx* c);

@@ -70,6 +70,7 @@ __device__ __forceinline__ void consumer_sync() {
 struct ConvArgs {
     DevGeo g;
     int nact, tmask, nitems, rows_per_tile, nst;
+    int nkr, ksplit, krank;  // plane split: this rank's kz are krank + ksplit q, q < nkr
     const float* G;
     const float4* S;
     float4* O;
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB) k_conv_bulk(ConvArgs A) 
         int tile = 0, li = 0, s_issued = 0;
         bool ok = true;
         for (int it = blockIdx.x; ok && it < A.nitems; it += gridDim.x, li++) {
-            const int a = it / nkz, k = it - a * nkz, m = A.act_m[a];
+            const int a = it / A.nkr, k = A.krank + A.ksplit * (it - a * A.nkr), m = A.act_m[a];
             // the item's spectrum into its half of the double buffer
             const int sb = li & 1;
             if (li >= 2 && !mbar_wait(&sempty[sb], ((li >> 1) - 1) & 1)) {
@@ -165,7 +166,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, MINB) k_conv_bulk(ConvArgs A) 
     int tile = 0, li = 0;
     bool dead = false;
     for (int it = blockIdx.x; it < A.nitems; it += gridDim.x, li++) {
-        const int a = it / nkz, k = it - a * nkz, m = A.act_m[a];
+        const int a = it / A.nkr, k = A.krank + A.ksplit * (it - a * A.nkr), m = A.act_m[a];
         const float4* Sb = Sbuf + (li & 1) * nr;
         if (!dead && !mbar_wait(&sfull[li & 1], (li >> 1) & 1)) {
             atomicExch(A.errword, 3);
@@ -283,7 +284,17 @@ int gx_conv_bulk(GxCtx* c, int nact, int tmask) {
     A.g = g;
     A.nact = nact;
     A.tmask = tmask;
-    A.nitems = nact * g.nkz;
+    // with the plane split this rank contracts the kz with kz mod nranks ==
+    // rank (p3convp.f:180-190: the planes iz with mod(iz - jz, numprocs) ==
+    // myid, jz = 1) and leaves the rest of the output zero for the ranks' sum
+    const bool split = gx_plane_split(c);
+    A.ksplit = split ? c->nranks : 1;
+    A.krank = split ? c->rank : 0;
+    A.nkr = (g.nkz - A.krank + A.ksplit - 1) / A.ksplit;
+    A.nitems = nact * A.nkr;
+    if (split)
+        GX_CUDA(c, cudaMemsetAsync(c->specO, 0, sizeof(float4) * 4 * (size_t)nact * g.nkz * g.nr, c->stream));
+    if (A.nitems == 0) return GX_OK;
     A.rows_per_tile = R;
     A.nst = nst;
     A.G = c->green32;

@@ -472,6 +472,10 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* fr
     if (gx_conv_bulk_ok(g)) {
         rc = gx_conv_bulk(c, nact, tmask);
         if (rc) return rc;
+        if (gx_plane_split(c)) {
+            rc = gx_comm_reduce_conv(c);
+            if (rc) return rc;
+        }
     } else {
         size_t sm = sizeof(float4) * (size_t)g.nr * 9;
         dim3 grid(nact, g.nkz);

@@ -63,6 +63,12 @@ extern "C" {
 #define GX_FLAG_WHOLE_GRID  4   /* time-step zones: the field over the whole grid
                                    on every step (the 'wholeg' option, findf.f:41)
                                    instead of partial-grid solves */
+#define GX_FLAG_PLANE_SPLIT 16  /* 3D mixed path on nranks > 1: each rank runs the
+                                   radial contraction only for the vertical
+                                   wavenumbers kz with kz mod nranks == rank and the
+                                   ranks sum the contracted spectra (the reference's
+                                   MPI plane split, SRC/lib15_mpi/p3convp.f:180-190,
+                                   276-326); needs nr a multiple of 4, <= 128 */
 #define GX_FLAG_SORTED_DEPOSIT 8 /* mixed path: step with the row-sorted deposit
                                    (counting sort of the cell rows, staged
                                    fixed-point items, combine) instead of the
@@ -299,6 +305,23 @@ int gx_last_launch_count(const GxCtx* ctx, int64_t* n);
  * gx_comm_init with them.  Mixed path only. */
 int gx_comm_unique_id(char* id128);
 int gx_comm_init(GxCtx* ctx, const char* id128, int nranks, int rank);
+
+/* The same exchanges through the host, for ranks that communicate through a
+ * host process group (e.g. torch.distributed over gloo): the library copies
+ * each buffer to host memory, calls fn(user, op, dtype, data, count) to
+ * reduce the count elements at data in place over all ranks, and copies the
+ * result back.  op is GX_OP_SUM, GX_OP_MIN or GX_OP_MAX; dtype GX_DT_INT32
+ * or GX_DT_FLOAT32; fn returns 0 on success.  Every rank must make the same
+ * calls in the same order (as it must with NCCL).  Replaces a communicator
+ * bound by gx_comm_init.  Mixed path only.  (massum.f:54-65, p2manlp.f:208,
+ * p3manlp.f:102, p3convp.f:276-326 exchange the same quantities over MPI.) */
+#define GX_OP_SUM 0
+#define GX_OP_MIN 1
+#define GX_OP_MAX 2
+#define GX_DT_INT32 0
+#define GX_DT_FLOAT32 1
+typedef int (*gx_host_reduce_fn)(void* user, int op, int dtype, void* data, int64_t count);
+int gx_comm_host(GxCtx* ctx, int nranks, int rank, gx_host_reduce_fn fn, void* user);
 
 /* massgn + scaled without allocating memory.  No counterpart in the
  * reference: it is for callers that may not allocate device memory when they

@@ -117,11 +117,12 @@ def test_bench3_masset_fields_force_potential_vs_fp64_oracle(bench3):
                       gal.grid(GX_GRID_POT)]).astype(np.float64)
         gal.findf(True)
         acc, pot = gal.getacc()
-    # against the FP32 mirror (the same FP32 cells as the reference): the
-    # fixed-point quantum 2^-20 of a particle and the mirror's FP32 sums
+    # against the FP32 mirror (the same FP32 cells as the reference; the cell
+    # fractions come from the fast FP32 log and atan2, within ~2e-5 of the
+    # mirror's at 128 rings and 256 spokes, the keys bit for bit)
     ref32, _ = ox.masset(cfg, rec, prec=32)
     ref32 = ref32.astype(np.float64)
-    assert np.abs(m - ref32).max() / ref32.max() < 4e-6
+    assert np.abs(m - ref32).max() / ref32.max() < 2e-5
     # against FP64 cells: the FP32 cell coordinates (u = log r / alpha up to
     # 128 rings carries ~1e-5 absolute) move weight between cells by that
     # much per particle; the L2 error is what reaches the field
@@ -197,8 +198,8 @@ def test_bench2_200_steps_track_oracle_fp64(precision, tol):
 # grids the tensor-core vertical synthesis does not take: 68 even
 # wavenumbers (ngz = 135), and 81 spectral columns (m = 0..40)
 FALLBACK = {
-    "ngz135": dict(nr=16, na=32, ngz=135, dzg=0.02, ng=5),
-    "m0..40": dict(nr=16, na=128, ngz=15, dzg=0.1, ng=41),
+    "ngz135": dict(nr=32, na=32, ngz=135, dzg=0.02, ng=5),
+    "m0..40": dict(nr=32, na=128, ngz=15, dzg=0.1, ng=41),
 }
 
 
