@@ -259,7 +259,7 @@ void gx_destroy(GxCtx* c) {
                     c->items, c->nitems_d, c->rowitem, c->rowcnt, c->rowfill, c->rowbase, c->rowtot, c->rowtile, c->stage, c->jrk_d,
                     c->errword, c->dsum, c->pzone[0], c->pzone[1], c->zbuf, c->zjrk_d, c->act_d,
                     c->bk_cap[0], c->bk_cap[1], c->bk_base[0], c->bk_base[1], c->bk_fill[0], c->bk_fill[1],
-                    c->bk_ctl, c->bk_items, c->bk_cnt, c->macc, c->bq[0], c->bq[1]};
+                    c->bk_ctl, c->bk_items, c->bk_cnt, c->macc, c->bq[0], c->bq[1], c->zr_d};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     for (cudaEvent_t e : c->pev) cudaEventDestroy(e);
@@ -473,6 +473,7 @@ int gx_loadup(GxCtx* c, const float* coords, int64_t n) {
     c->n = n;
     c->have_mass = c->have_field = c->have_keys = false;
     c->bucketed = false;
+    c->zr_valid = false;
     const int nw = 2 * c->g.ndim;
     if (n == 0) return (c->nzones > 1 && !c->fp64) ? gx_zone_loadup(c) : GX_OK;
     float* staging = c->stagebuf;
@@ -532,6 +533,7 @@ int gx_masset(GxCtx* c) {
     cudaSetDevice(c->dev);
     int rc = gx_dense(c);
     if (rc) return rc;
+    c->zr_valid = false;
     rc = c->fp64 ? gx_fp64_masset(c) : (c->nzones > 1 ? gx_zone_masset(c) : gx_mixed_masset(c));
     if (rc) return rc;
     GX_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -584,8 +586,10 @@ int gx_step(GxCtx* c, int nsteps, int phys) {
     int rc;
     if (c->fp64) rc = gx_fp64_step(c, nsteps, phys);
     else if (gx_fast_ok(c)) rc = gx_fast_step(c, nsteps, phys);
-    else if ((rc = gx_dense(c)) == GX_OK)
+    else if ((rc = gx_dense(c)) == GX_OK) {
+        c->zr_valid = false;
         rc = (c->nzones > 1) ? gx_zone_step(c, nsteps, phys) : gx_mixed_step(c, nsteps, phys);
+    }
     if (rc) return rc;
     GX_CUDA(c, cudaEventRecord(c->ev1, c->stream));
     GX_CUDA(c, cudaEventSynchronize(c->ev1));

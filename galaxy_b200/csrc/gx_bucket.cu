@@ -296,6 +296,7 @@ __global__ void __launch_bounds__(BK_THREADS, BK_MINB) k_push_bkt(
     const int na = g.na, ngz = d3 ? g.ngz : 1, nrow = g.nrow;
     const int nit = ctl[0];
     int rmin_l = 0x7fffffff, rmax_l = -1;  // ring range of this lane's new cells
+    int zmin_l = 0x7fffffff, zmax_l = -1;  // and their plane range (3D)
     for (int i = threadIdx.x; i < WROWS * na; i += BK_THREADS) bins[i] = 0u;
     for (;;) {
         if (threadIdx.x == 0) s_item = atomicAdd(ctl + 1, 1);
@@ -346,6 +347,10 @@ __global__ void __launch_bounds__(BK_THREADS, BK_MINB) k_push_bkt(
                 if (cn.key >= 0) {
                     rmin_l = min(rmin_l, cn.ju);
                     rmax_l = max(rmax_l, cn.ju);
+                    if (d3) {
+                        zmin_l = min(zmin_l, cn.iz);
+                        zmax_l = max(zmax_l, cn.iz);
+                    }
                 }
             }
             // the row's slot: warp-aggregated atomic on its fill counter,
@@ -471,26 +476,40 @@ __global__ void __launch_bounds__(BK_THREADS, BK_MINB) k_push_bkt(
     for (int o = 16; o > 0; o >>= 1) {
         rmin_l = min(rmin_l, __shfl_xor_sync(0xffffffffu, rmin_l, o));
         rmax_l = max(rmax_l, __shfl_xor_sync(0xffffffffu, rmax_l, o));
+        zmin_l = min(zmin_l, __shfl_xor_sync(0xffffffffu, zmin_l, o));
+        zmax_l = max(zmax_l, __shfl_xor_sync(0xffffffffu, zmax_l, o));
     }
     if ((threadIdx.x & 31) == 0 && rmax_l >= 0) {
         atomicMin(ctl + 5, rmin_l);
         atomicMax(ctl + 6, rmax_l);
+        if (d3) {
+            atomicMin(ctl + 2, zmin_l);
+            atomicMax(ctl + 3, zmax_l);
+        }
     }
 }
 
 // mass = pmass 2^-20 acc (as k_mass_combine forms it); acc cleared for the
 // next step.  Two cells per thread (mesh is even: na is).
 __global__ void k_mass_convert(unsigned long long* __restrict__ acc, float* __restrict__ mass, int mesh,
-                               float pm, int32_t* __restrict__ rng, int32_t* __restrict__ jrk, int nr) {
+                               float pm, int32_t* __restrict__ rng, int32_t* __restrict__ jrk, int nr,
+                               int32_t* __restrict__ zrng, int32_t* __restrict__ zr, int ngz) {
     // the active ring range of the new mass, as massgn tracks it (jrad =
     // first ring + 1, krad = min(last ring + 2, nr), 1-based), from the ring
-    // range the push gathered (rng[0], rng[1]), which is reset for the next
+    // range the push gathered (rng[0], rng[1]); the planes holding mass
+    // (the cells' planes and the next, clamped) from its plane range; both
+    // reset for the next pass
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         const int mn = rng[0], mx = rng[1];
         jrk[0] = (mx >= 0) ? mn + 1 : nr;
         jrk[1] = (mx >= 0) ? min(mx + 2, nr) : 0;
         rng[0] = 0x7fffffff;
         rng[1] = -1;
+        const int zn = zrng[0], zx = zrng[1];
+        zr[0] = (zx >= 0) ? zn : ngz;
+        zr[1] = (zx >= 0) ? min(zx + 1, ngz - 1) : -1;
+        zrng[0] = 0x7fffffff;
+        zrng[1] = -1;
     }
     const int i = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     if (i >= mesh) return;
@@ -604,6 +623,7 @@ int gx_bucket_alloc(GxCtx* c) {
     rc = rc ? rc : bk_alloc(c, &c->bk_ctl, 16);
     rc = rc ? rc : bk_alloc(c, &c->bk_cnt, nrow1);
     rc = rc ? rc : bk_alloc(c, &c->macc, (size_t)c->g.mesh);
+    rc = rc ? rc : bk_alloc(c, &c->zr_d, 4);
     if (rc) return rc;
     for (int b = 0; b < 2; b++) {
         GX_CUDA(c, cudaMemsetAsync(c->bk_fill[b], 0, sizeof(int32_t) * nrow1, c->stream));
@@ -611,7 +631,7 @@ int gx_bucket_alloc(GxCtx* c) {
         GX_CUDA(c, cudaMemsetAsync(c->bk_base[b], 0, sizeof(int32_t) * nrow1, c->stream));
     }
     GX_CUDA(c, cudaMemsetAsync(c->macc, 0, sizeof(unsigned long long) * c->g.mesh, c->stream));
-    const int32_t ctl0[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0x7fffffff, -1, 0};
+    const int32_t ctl0[16] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0x7fffffff, -1, 0, 0x7fffffff, -1, 0};
     GX_CUDA(c, cudaMemcpyAsync(c->bk_ctl, ctl0, sizeof ctl0, cudaMemcpyHostToDevice, c->stream));
     GX_CUDA(c, cudaStreamSynchronize(c->stream));
     return GX_OK;
@@ -747,7 +767,9 @@ int gx_fast_step(GxCtx* c, int nsteps, int phys) {
     }
     for (int s = 0; s < nsteps; s++) {
         const bool last = (s == nsteps - 1);
-        rc = gx_mixed_findf(c, phys && last, true);
+        // once the mass is a fused pass's, the solve knows the planes that
+        // hold it, and the field is needed only where the particles are
+        rc = gx_mixed_findf(c, phys && last, true, nullptr, (c->zr_valid && g.ndim == 3) ? c->zr_d : nullptr);
         if (rc) return rc;
         const int cur = c->bcur, nxt = cur ^ 1;
         rc = bk_join(c);
@@ -776,8 +798,10 @@ int gx_fast_step(GxCtx* c, int nsteps, int phys) {
         rc = gx_phase_mark(c, PH_COMBINE);
         if (rc) return rc;
         k_mass_convert<<<(unsigned)((g.mesh / 2 + 255) / 256), 256, 0, c->stream>>>(
-            c->macc, c->mass, g.mesh, g.pmass, c->bk_ctl + 13, c->jrk_d, g.nr);
+            c->macc, c->mass, g.mesh, g.pmass, c->bk_ctl + 13, c->jrk_d, g.nr, c->bk_ctl + 10, c->zr_d,
+            g.ngz);
         GX_LAUNCHED(c);
+        c->zr_valid = true;
         c->bcur = nxt;
     }
     rc = bk_join(c);

@@ -147,6 +147,20 @@ int gx_comm_reduce_range(GxCtx* c) {
     return GX_OK;
 }
 
+// MIN/MAX of the planes holding mass (the step's own solve skips the rest)
+int gx_comm_reduce_planes(GxCtx* c, int32_t* zr) {
+    if (c->nranks < 2) return GX_OK;
+    if (c->host_fn) {
+        int rc = host_reduce(c, zr, 1, GX_DT_INT32, GX_OP_MIN);
+        return rc ? rc : host_reduce(c, zr + 1, 1, GX_DT_INT32, GX_OP_MAX);
+    }
+    if (!c->comm) return GX_OK;
+    NcclApi* a = nccl();
+    GX_NCCL(c, a->allReduce(zr, zr, 1, ncclInt32, ncclMin, (ncclComm_t)c->comm, c->stream));
+    GX_NCCL(c, a->allReduce(zr + 1, zr + 1, 1, ncclInt32, ncclMax, (ncclComm_t)c->comm, c->stream));
+    return GX_OK;
+}
+
 static int reduce_sum_f32(GxCtx* c, float* p, size_t count) {
     if (c->nranks < 2) return GX_OK;
     if (c->host_fn) return host_reduce(c, p, (int64_t)count, GX_DT_FLOAT32, GX_OP_SUM);

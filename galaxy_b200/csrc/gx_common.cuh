@@ -175,11 +175,15 @@ struct GxCtx {
     int32_t* bk_base[2] = {nullptr, nullptr};
     int32_t* bk_fill[2] = {nullptr, nullptr};
     int32_t* bk_ctl = nullptr;               // [2][4]: overflow count of each buffer; [8] items, [9] work
-                                             // counter, [12] compaction counter, [13..14] ring range
+                                             // counter, [10..11] plane range, [12] compaction counter,
+                                             // [13..14] ring range (of the pass's new cells)
     int4* bk_items = nullptr;                // work items of pbuf[cur]: row (-1: overflow), first, end slot
     int64_t bk_maxitems = 0;
     int32_t* bk_cnt = nullptr;               // [nrow + 1] row counts of the dense store (bucketing)
     unsigned long long* macc = nullptr;      // [mesh] fixed-point mass (2^-20 of a particle), zero between steps
+    int32_t* zr_d = nullptr;                 // [2] first, last plane holding the fused pass's mass
+                                             // (ngz, -1 when empty)
+    bool zr_valid = false;                   // the mass array is the fused pass's (zr_d describes it)
     int bk_grid = 0;                         // CTAs of the fused pass
     cudaStream_t bk_side = nullptr;          // the plan's stream (overlaps the field solve)
     cudaEvent_t bk_ev[2] = {nullptr, nullptr};  // push done (main), plan done (side)
@@ -666,7 +670,12 @@ void fill_devgeo(GxCtx* c);
 int gx_green_build_dev(GxCtx* c);
 int gx_mixed_masset(GxCtx* c);
 // frk: device [2] 1-based field ring range of a partial-grid solve, or null
-int gx_mixed_findf(GxCtx* c, int lpot, bool polcat, const int32_t* frk = nullptr);
+// zr: device [2] first and last plane holding mass (the step's own solve:
+// the forward transforms skip the planes outside, the azimuthal synthesis
+// covers them one plane wider, the planes the next particle pass reads), or
+// null for the whole grid
+int gx_mixed_findf(GxCtx* c, int lpot, bool polcat, const int32_t* frk = nullptr,
+                   const int32_t* zr = nullptr);
 int gx_mixed_getacc(GxCtx* c, float* acc, float* pot);
 int gx_mixed_step(GxCtx* c, int nsteps, int phys);
 int gx_mixed_sort_deposit(GxCtx* c);
@@ -694,8 +703,10 @@ int gx_fast_step(GxCtx* c, int nsteps, int phys);
 int gx_dense(GxCtx* c);  // bucketed store -> dense store (no-op when dense)
 int gx_bucket_alloc(GxCtx* c);
 int gx_bucket_words(const GxCtx* c);  // float4 words per record of the bucketed store
-int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk = nullptr);
+int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk = nullptr,
+                 const int32_t* zr = nullptr);
 int gx_comm_reduce_spectrum(GxCtx* c);
 int gx_comm_reduce_conv(GxCtx* c);    // sum of the contracted spectra (plane split)
+int gx_comm_reduce_planes(GxCtx* c, int32_t* zr);  // MIN/MAX of the plane range of the mass
 bool gx_plane_split(const GxCtx* c);
 void gx_comm_destroy(GxCtx* c);

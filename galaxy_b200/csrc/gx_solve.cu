@@ -150,6 +150,7 @@ __global__ void k_fwdtab(DevGeo g, int nact, int ncp, float* __restrict__ Taz, f
 // vertical part zeroes their spectrum).
 #define FWD_RB 32
 __global__ void __launch_bounds__(288) k_fwd_az(DevGeo g, int ncp, const int32_t* __restrict__ jrk,
+                                                const int32_t* __restrict__ zr,
                                                 const float* __restrict__ mass,
                                                 const float* __restrict__ Taz,
                                                 float* __restrict__ C1) {
@@ -159,6 +160,17 @@ __global__ void __launch_bounds__(288) k_fwd_az(DevGeo g, int ncp, const int32_t
     const int rlo = (max(jrk[0], 1) - 1) * ngz, rhi = min(jrk[1], nr) * ngz;  // active rows [rlo, rhi)
     if (row0 + FWD_RB <= rlo || row0 >= rhi) return;
     const int nrows = min(FWD_RB, g.nrow - row0);
+    if (zr) {
+        // only blocks with a row in the planes the vertical part sums (the
+        // planes holding mass, the first rounded down to a multiple of 4)
+        const int zs = zr[0] & ~3, ze = zr[1];
+        int in = 0;
+        if ((int)threadIdx.x < nrows) {
+            const int iz = (row0 + (int)threadIdx.x) % ngz;
+            in = iz >= zs && iz <= ze;
+        }
+        if (!__syncthreads_or(in)) return;
+    }
     const int ldx = na + 1;
     float* X = sm;                 // [FWD_RB][na + 1]
     float* T = X + FWD_RB * ldx;   // [na][ncp]
@@ -225,10 +237,17 @@ __global__ void __launch_bounds__(288) k_fwd_az(DevGeo g, int ncp, const int32_t
 #define FWD_KR 32
 __global__ void __launch_bounds__(288) k_fwd_z(DevGeo g, int nact, int ncp,
                                                const int32_t* __restrict__ jrk,
+                                               const int32_t* __restrict__ zr,
                                                const float* __restrict__ C1,
                                                const float* __restrict__ Tz, float4* __restrict__ S) {
     extern __shared__ __align__(16) float sm[];
     const int ngz = g.ngz, nkz = g.nkz, nr = g.nr;
+    // the planes summed: all, or those holding mass with the first rounded
+    // down to a multiple of 4, so that every lane of the K split below sums
+    // the same planes in the same order as over the whole grid (the others
+    // add exact zeros): the spectrum is bitwise the whole-grid one
+    const int zs = zr ? (zr[0] & ~3) : 0;
+    const int nzs = zr ? max(zr[1] - zs + 1, 0) : ngz;
     const int ir = blockIdx.x, kr0 = blockIdx.y * FWD_KR;   // first output row (2 kz0)
     const int nrow_out = min(FWD_KR, 2 * nkz - kr0);
     if (ir < jrk[0] - 1 || ir > min(jrk[1], nr) - 1) {
@@ -240,13 +259,13 @@ __global__ void __launch_bounds__(288) k_fwd_z(DevGeo g, int nact, int ncp,
         }
         return;
     }
-    float* B = sm;                      // [ngz][ncp]
-    float* Tk = B + ngz * ncp;          // [FWD_KR][ngz]
+    float* B = sm;                      // [nzs][ncp]
+    float* Tk = B + ngz * ncp;          // [FWD_KR][nzs]
     // several loads in flight per thread: the prologue is latency-bound
     {
-        const float4* src = reinterpret_cast<const float4*>(C1 + (size_t)ir * ngz * ncp);
+        const float4* src = reinterpret_cast<const float4*>(C1 + ((size_t)ir * ngz + zs) * ncp);
         float4* dst = reinterpret_cast<float4*>(B);
-        const int n4 = ngz * ncp / 4;
+        const int n4 = nzs * ncp / 4;
         for (int b = threadIdx.x; b < n4; b += 4 * blockDim.x) {
             float4 v[4];
 #pragma unroll
@@ -261,21 +280,21 @@ __global__ void __launch_bounds__(288) k_fwd_z(DevGeo g, int nact, int ncp,
             }
         }
     }
-    for (int b = threadIdx.x; b < FWD_KR * ngz; b += 4 * blockDim.x) {
+    for (int b = threadIdx.x; b < FWD_KR * nzs; b += 4 * blockDim.x) {
         float v[4];
 #pragma unroll
         for (int u = 0; u < 4; u++) {
-            const int i = b + u * blockDim.x;
-            v[u] = (i < nrow_out * ngz) ? __ldg(Tz + (size_t)kr0 * ngz + i) : 0.f;
+            const int i = b + u * blockDim.x, r = i / max(nzs, 1), z = i - r * nzs;
+            v[u] = (i < nrow_out * nzs) ? __ldg(Tz + (size_t)(kr0 + r) * ngz + zs + z) : 0.f;
         }
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             const int i = b + u * blockDim.x;
-            if (i < FWD_KR * ngz) Tk[i] = v[u];
+            if (i < FWD_KR * nzs) Tk[i] = v[u];
         }
     }
     __syncthreads();
-    sgemm44_sk<4>(nrow_out, ncp, ngz, Tk, ngz, B, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
+    sgemm44_sk<4>(nrow_out, ncp, nzs, Tk, nzs, B, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
         // rows r0 = 2k, 2k+1, 2k+2, 2k+3 (relative to kr0); cols c0 = 2a .. 2a+3
 #pragma unroll
         for (int dk = 0; dk < 2; dk++) {
@@ -420,7 +439,7 @@ int gx_conv_bulk(GxCtx* c, int nact, int tmask);
 
 // ---------------------------------------------------------------------------
 // findf for the mixed path: mass -> field (and optional polar copy)
-int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* frk) {
+int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* frk, const int32_t* zr) {
     const DevGeo& g = c->g;
     const int nact = c->spec.nact;
     if (nact == 0) return c->err = "no active harmonics", GX_ERR_ARG;
@@ -437,6 +456,11 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* fr
     if (rc) return rc;
     rc = gx_comm_reduce_range(c);
     if (rc) return rc;
+    if (g.ndim != 3) zr = nullptr;
+    if (zr) {
+        rc = gx_comm_reduce_planes(c, const_cast<int32_t*>(zr));
+        if (rc) return rc;
+    }
     if (g.ndim == 3) {
         const size_t ntaz = (size_t)g.na * ncp, ntz = (size_t)ru4(2 * g.nkz) * g.ngz;
         if (!c->fwdtab) {
@@ -449,13 +473,13 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* fr
         if (!c->fwdC1) GX_CUDA(c, cudaMalloc((void**)&c->fwdC1, sizeof(float) * (size_t)g.nrow * ncp));
         size_t sm = sizeof(float) * ((size_t)FWD_RB * (g.na + 1) + ntaz);
         GX_CUDA(c, cudaFuncSetAttribute(k_fwd_az, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_fwd_az<<<(g.nrow + FWD_RB - 1) / FWD_RB, 288, sm, c->stream>>>(g, ncp, c->jrk_d, c->mass,
+        k_fwd_az<<<(g.nrow + FWD_RB - 1) / FWD_RB, 288, sm, c->stream>>>(g, ncp, c->jrk_d, zr, c->mass,
                                                                          c->fwdtab, c->fwdC1);
         GX_LAUNCHED(c);
         sm = sizeof(float) * ((size_t)g.ngz * ncp + (size_t)FWD_KR * g.ngz);
         GX_CUDA(c, cudaFuncSetAttribute(k_fwd_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         dim3 gz(g.nr, (2 * g.nkz + FWD_KR - 1) / FWD_KR);
-        k_fwd_z<<<gz, 288, sm, c->stream>>>(g, nact, ncp, c->jrk_d, c->fwdC1, c->fwdtab + ntaz,
+        k_fwd_z<<<gz, 288, sm, c->stream>>>(g, nact, ncp, c->jrk_d, zr, c->fwdC1, c->fwdtab + ntaz,
                                             c->specS);
         GX_LAUNCHED(c);
     } else {
@@ -491,7 +515,7 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* fr
     }
     rc = gx_phase_mark(c, PH_SYN);
     if (rc) return rc;
-    rc = gx_synthesis(c, tmask, polar, frk);
+    rc = gx_synthesis(c, tmask, polar, frk, zr);
     if (rc) return rc;
     rc = gx_phase_end(c);
     if (rc) return rc;
@@ -560,6 +584,7 @@ extern "C" int gx_get_grid(GxCtx* c, int which, float* out) {
 extern "C" int gx_set_mass(GxCtx* c, const float* mass) {
     if (!c || !mass) return GX_ERR_ARG;
     cudaSetDevice(c->dev);
+    c->zr_valid = false;
     const DevGeo& g = c->g;
     const int mesh = g.mesh;
     // active ring range of the installed masses (p3ckst.f sets jrad/krad)

@@ -317,10 +317,21 @@ __device__ __forceinline__ bool szt_item(const DevGeo& g, int it, int tmask, con
 __global__ void __launch_bounds__(SYNZ_THREADS, 1) k_synz_tc(DevGeo g, int nact, int ncp, int tmask,
                                                              const float4* __restrict__ O, SynTab tb,
                                                              float* __restrict__ R,
-                                                             const int32_t* __restrict__ frk) {
+                                                             const int32_t* __restrict__ frk,
+                                                             const int32_t* __restrict__ zr) {
     extern __shared__ __align__(16) float sm[];
     const int nr = g.nr, nkz = g.nkz, ngz = g.ngz;
     const int Z0 = tb.Z0, KE = tb.KE, KO = tb.KO, nz4 = ru4s(Z0);
+    // the planes wanted (all, or those the next particle pass reads: the
+    // planes holding mass, one wider each side); a tile of 16 planes z is
+    // summed when z or its mirror ngz - z is wanted
+    const int zlo = zr ? max(zr[0] - 1, 0) : 0, zhi = zr ? min(zr[1] + 1, ngz - 1) : ngz - 1;
+    bool need[4];
+#pragma unroll
+    for (int a = 0; a < 4; a++) {
+        const int z0 = 16 * a, z1 = min(16 * a + 15, Z0 - 1);
+        need[a] = (z0 <= zhi && z1 >= zlo) || (ngz - z1 <= zhi && ngz - z0 >= zlo);
+    }
     const int kte = (KE + 7) >> 3, kto = (KO + 7) >> 3;  // k-steps of 8 per parity
     const int nitems = 4 * nr, nsp = nkz * nact;
     uint32_t* sWh = reinterpret_cast<uint32_t*>(sm);  // [4][SZT_K][64]: WAe, WBe, WAo, WBo, TF32 hi
@@ -441,6 +452,7 @@ __global__ void __launch_bounds__(SYNZ_THREADS, 1) k_synz_tc(DevGeo g, int nact,
 #pragma unroll
                 for (int a = 0; a < 4; a++) {
                     if (a >= mt) break;
+                    if (!need[a]) continue;
                     const int m0 = (16 * a + q) ^ sw, m1 = (16 * a + q + 8) ^ sw;
                     const int o0 = i0 * 64 + m0, o1 = i0 * 64 + m1, o2 = i1 * 64 + m0, o3 = i1 * 64 + m1;
                     const uint32_t aph[4] = {WPh[o0], WPh[o1], WPh[o2], WPh[o3]};
@@ -465,6 +477,7 @@ __global__ void __launch_bounds__(SYNZ_THREADS, 1) k_synz_tc(DevGeo g, int nact,
 #pragma unroll
         for (int a = 0; a < 4; a++) {
             if (a >= mt) break;
+            if (!need[a]) continue;
 #pragma unroll
             for (int hrow = 0; hrow < 2; hrow++) {
                 const int z = 16 * a + q + 8 * hrow;
@@ -488,12 +501,22 @@ __global__ void __launch_bounds__(SYNZ_THREADS, 1) k_synz_tc(DevGeo g, int nact,
 __global__ void __launch_bounds__(SYNAZ_THREADS) k_synaz(DevGeo g, int nact, int ncp, int tmask,
                                               const float* __restrict__ R, SynTab tb,
                                               float4* __restrict__ F, float* __restrict__ polar,
-                                              const int32_t* __restrict__ frk) {
+                                              const int32_t* __restrict__ frk,
+                                              const int32_t* __restrict__ zr) {
     extern __shared__ __align__(16) float sm[];
     const int ir = blockIdx.x, zb = blockIdx.y * SYN_ZB;
     if (frk && (ir + 1 < frk[0] || ir + 1 > frk[1])) return;  // rings no moving particle reads
     const int nr = g.nr, ngz = g.ngz, na = g.na, njp = tb.njp;
-    const int nz = min(SYN_ZB, ngz - zb);
+    // with zr, only the planes the next particle pass reads: those holding
+    // mass, one wider each side (a particle's interpolation cell may sit one
+    // plane off its deposit cell); the block's planes [zb0, zb1)
+    int zb0 = zb, zb1 = min(zb + SYN_ZB, ngz);
+    if (zr) {
+        zb0 = max(zb0, zr[0] - 1);
+        zb1 = min(zb1, zr[1] + 2);
+        if (zb1 <= zb0) return;
+    }
+    const int nz = zb1 - zb0;
     float* TC = sm;                      // [nact][njp]
     float* TS = TC + nact * njp;
     float* CS = TS + nact * njp;         // [2][njp]
@@ -526,7 +549,7 @@ __global__ void __launch_bounds__(SYNAZ_THREADS) k_synaz(DevGeo g, int nact, int
             const int z = rem / ncp, c = rem - z * ncp;
             v[u] = 0.f;
             if (i < 4 * SYN_ZB * ncp && ((tmask >> t) & 1) && z < nz)
-                v[u] = __ldg(R + (((size_t)t * nr + ir) * ngz + zb + z) * ncp + c);
+                v[u] = __ldg(R + (((size_t)t * nr + ir) * ngz + zb0 + z) * ncp + c);
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {
@@ -555,7 +578,7 @@ __global__ void __launch_bounds__(SYNAZ_THREADS) k_synaz(DevGeo g, int nact, int
                 S[t][0] += rs * ts.x; S[t][1] += rs * ts.y; S[t][2] += rs * ts.z; S[t][3] += rs * ts.w;
             }
         }
-        const size_t rowb = ((size_t)ir * ngz + zb + z) * na;
+        const size_t rowb = ((size_t)ir * ngz + zb0 + z) * na;
 #pragma unroll
         for (int q = 0; q < 4; q++) {
             const int j = j0 + q;
@@ -589,7 +612,7 @@ __global__ void __launch_bounds__(SYNAZ_THREADS) k_synaz(DevGeo g, int nact, int
 }
 
 // ---------------------------------------------------------------------------
-int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk) {
+int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk, const int32_t* zr) {
     const DevGeo& g = c->g;
     const int nact = c->spec.nact;
     const int ncp = ru4s(2 * nact);
@@ -623,7 +646,7 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk) {
             const size_t sm = sizeof(float) * (8 * SZT_K * 64 + 4 * SZT_K * SZT_SS);
             GX_CUDA(c, cudaFuncSetAttribute(k_synz_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
             k_synz_tc<<<std::min(sms, 4 * g.nr), SYNZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->specO,
-                                                                              tb, c->synR, frk);
+                                                                              tb, c->synR, frk, zr);
         } else {
             const size_t sm = sizeof(float) * (2 * nWe + 2 * nWo + 3 * 32 + (size_t)(KE + KO) * 2 * ncp);
             GX_CUDA(c, cudaFuncSetAttribute(k_synz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -636,7 +659,8 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk) {
         const size_t sm = sizeof(float) * (2 * nT + 2 * (size_t)njp + (size_t)4 * SYN_ZB * ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_synaz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         dim3 grid(g.nr, (g.ngz + SYN_ZB - 1) / SYN_ZB);
-        k_synaz<<<grid, SYNAZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->synR, tb, c->field, polar, frk);
+        k_synaz<<<grid, SYNAZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->synR, tb, c->field, polar, frk,
+                                                        g.ndim == 3 ? zr : nullptr);
         GX_LAUNCHED(c);
     }
     return GX_OK;
