@@ -600,10 +600,16 @@ def main():
     ap.add_argument("--sfp-only", action="store_true",
                     help="run only the SFP coefficient sum and print its JSON (profiling)")
     ap.add_argument("--sfp-n", type=int, default=20_000_000, help="particles of the SFP sum")
+    ap.add_argument("--ens-only", action="store_true",
+                    help="run only the batched ensemble and print its JSON (profiling)")
+    ap.add_argument("--ens-steps", type=int, default=1000, help="steps of the batched ensemble")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.sfp_only:
         print(json.dumps(run_sfp(args.sfp_n)))
+        return
+    if args.ens_only:
+        print(json.dumps(run_ensemble(steps=args.ens_steps)))
         return
     w = WORKLOADS[args.workload]
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -282,8 +282,11 @@ __global__ void __launch_bounds__(1024) k_ens_step(EnsArgs A) {
             float x = X[p], y = Y[p];
             if (A.mode == 1) {
                 float vx = VX[p], vy = VY[p];
-                // grdacc.f:40-84 at the old position, halo (frhalo.f:55-56)
-                const CellW cw = gx_cell(g, x, y, 0.f, true);
+                // grdacc.f:40-84 at the old position, halo (frhalo.f:55-56);
+                // the interpolation cell from the fast FP32 arithmetic, as the
+                // single-disc pass forms it (the field is continuous across a
+                // cell boundary, so a cell off by rounding changes nothing)
+                const CellW cw = gx_cell_t<false, 2>(g, x, y, 0.f, true);
                 float ax = 0.f, ay = 0.f;
                 if (cw.key >= 0) {
                     float w[8];
@@ -330,12 +333,16 @@ __global__ void __launch_bounds__(1024) k_ens_step(EnsArgs A) {
                 gx_corners(g, cn.key, ic);
 #pragma unroll
                 for (int k = 0; k < 4; k++)
-                    if (ic[k] >= 0)
-                        atomicAdd(&bins[ic[k]], (unsigned long long)(long long)__float2int_rn(w[k] * ENS_FIXQ));
+                    if (ic[k] >= 0) {
+                        // round(w 2^20), ties to even, by one FMA with 1.5 2^23
+                        const int v = __float_as_int(fmaf(w[k], ENS_FIXQ, 12582912.0f)) - 0x4B400000;
+                        atomicAdd(&bins[ic[k]], (unsigned long long)(long long)v);
+                    }
                 const double xd = x, yd = y, r2 = xd * xd + yd * yd;
                 if (r2 > 0.0) {
-                    sc += (xd * xd - yd * yd) / r2;
-                    ss += 2.0 * xd * yd / r2;
+                    const double inv = 1.0 / r2;
+                    sc += (xd * xd - yd * yd) * inv;
+                    ss += 2.0 * xd * yd * inv;
                 }
                 sn += 1.0;
             }
