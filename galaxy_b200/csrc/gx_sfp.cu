@@ -13,13 +13,15 @@
 // factors through the moment matrix
 //     M[d][c] = sum_p T_d(x_p) g_c(p),  g = (1, p^e cos m phi, p^e sin m phi)
 // and C[n, m, .] = sum_d a_nmd M[d][c(m, .)].  M is a GEMM with K = N
-// (particles): it runs on the tensor cores with mma.sync m16n8k8 TF32,
-// each operand split hi + lo (three products, FP32 accumulate per warp over
-// a chunk of particles, chunks summed in FP64).  The fragments are formed
-// in registers from each lane's particles: no shared-memory staging of
-// per-particle features, which would otherwise bound the kernel.
+// (particles): it runs on the tensor cores with mma.sync m16n8k16 FP16,
+// each operand split into an FP16 hi and lo part (three products, FP32
+// accumulate per warp over a chunk of particles, chunks summed in FP64).
+// Each lane computes its particle's features once and stores them as a row
+// of the warp's shared-memory tiles; transposing tile loads (ldmatrix
+// .trans) turn those rows into the MMA fragments.
 // a_nmd are formed once on the host in FP64 from the roots and
 // coefficients of the basis (Chebyshev interpolation at 64 nodes).
+#include <cuda_fp16.h>
 #include <math.h>
 #include <string.h>
 
@@ -30,6 +32,7 @@
 #include "gx_common.cuh"
 
 #define SFP_CHUNK 1024  // particles per warp-chunk (FP32 accumulation span)
+#define SFP_MAXMOM (64 * 48)  // moments: [D][NCP] (D <= 64, NCP <= 32), or the tcgen05 path's raw [64][48]
 
 struct GxSfp {
     GxSfpBasis b;
@@ -49,7 +52,8 @@ struct GxSfp {
     float* part = nullptr;      // per-warp partial moments
     double* mom = nullptr;      // [D][NCP] FP64 moments
     double* qc = nullptr;       // device force series [2][maxm+1][D]
-    double* upart = nullptr;    // per-CTA FP64 partial moments of the tcgen05 path
+    double* upart = nullptr;    // per-CTA FP64 partial rows of the tcgen05 path
+    double* slab = nullptr;     // [2 nsm][nmom] FP64 first-stage sums of the partials
     int32_t* errword = nullptr; // device error word (bounded waits)
     int nsm = 0;
     float last_ms = 0.f;
@@ -101,38 +105,90 @@ __device__ __forceinline__ uint32_t f2tf32(float v) {
     return r & 0xffffe000u;
 }
 
-__device__ __forceinline__ void mma_tf32(float* d, const uint32_t* a, const uint32_t* b) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+// one m16n8k16 FP16 product with FP32 accumulation, D += A B
+__device__ __forceinline__ void mma_f16(float* d, const uint32_t* a, const uint32_t* b) {
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
         "{%8,%9}, {%0,%1,%2,%3};\n"
         : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+// the same with D = A B (no accumulator input)
+__device__ __forceinline__ void mma_f16_0(float* d, const uint32_t* a, const uint32_t* b) {
+    asm("mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, "
+        "{%8,%9}, {%10,%10,%10,%10};\n"
+        : "=f"(d[0]), "=f"(d[1]), "=f"(d[2]), "=f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]), "f"(0.f));
+}
+// four / two transposed 8 x 8 FP16 tiles (rows of 16 bytes at the lanes' addresses)
+__device__ __forceinline__ void ldsm_t4(uint32_t* r, uint32_t addr) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_t2(uint32_t* r, uint32_t addr) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];"
+                 : "=r"(r[0]), "=r"(r[1])
+                 : "r"(addr));
+}
+// v0 + v1 split into FP16 pairs: hi = (v0, v1) to nearest, lo = their
+// remainders to nearest (v = hi + lo to ~2^-22 relative, or 2^-25 absolute
+// where lo falls below the FP16 normal range); v0 at the lower address
+__device__ __forceinline__ void split_h2(float v0, float v1, uint32_t& hi, uint32_t& lo) {
+    const __half2 h = __floats2half2_rn(v0, v1);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(v0 - hf.x, v1 - hf.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
 }
 
 // Moments of one SFP_CHUNK of particles per warp; part[warp][d][c].
 // Rounds of 32 particles: lane l computes the features of particle l once --
 // T_d(x) for d < D by the three-term recurrence, and g_n (n >= 1) =
 // p^e cos m phi, p^e sin m phi (e = m mod 2) from repeated multiplication of
-// (x, y) / r -- into the warp's shared-memory tiles Ts[32][D + 8] and
-// Gs[32][GSTR] (padded so that the fragment loads below hit 32 distinct
-// banks).  Column c = 0 (g_0 = 1) is the plain sum of T_d, taken on the CUDA
-// cores (lane d); columns 1 .. NB*8 come from mma.sync m16n8k8 TF32 with the
-// operands split hi/lo (3 products), FP32 accumulation over the chunk.
-#define SFP_GSTR 24  // >= 8 NB, and 24 p mod 32 spreads c4 over banks
+// (x, y) / r -- splits each into an FP16 hi and lo part and writes them as
+// row l of the warp's shared-memory tiles Th, Tl [32][D + 8] and Gh, Gl
+// [32][GS] (row strides of 80 / 144 / 48 bytes put the eight 16-byte rows of
+// a transposed 8 x 8 tile load on distinct banks).  ldmatrix .trans turns
+// the particle-major rows into the fragments of M[d][n] = sum_k T_d(k) g_n(k)
+// for mma.sync m16n8k16 (A = T, 16 d x 16 particles; B = g, 16 particles x 8
+// columns), three products per hi/lo pair (hi hi, hi lo, lo hi), FP32
+// accumulation over the chunk.  Column c = 0 (g_0 = 1) is the plain sum of
+// T_d, one-signed for most d: on the tensor cores (a B fragment of ones in
+// registers, products hi 1 and lo 1) it starts from zero in every round of
+// 32 particles, whose sum (|.| <= 32) the tensor cores' FP32 accumulation
+// keeps to ~2^-18, and the rounds are added on the CUDA cores (rounded to
+// nearest).  Accumulated over a whole chunk in the tensor cores, this
+// column's sums of ~1000 would lose ~1e-5 to the accumulation's truncation.
+// The recurrences
+// start from sw = 1 for particles inside the basis edge (p <= 1) and 0 for
+// the rest, which makes every feature of an outside particle zero.
 template <int MT, int NB>
-__global__ void __launch_bounds__(256) k_sfp_moments(const float* __restrict__ X,
+__global__ void __launch_bounds__(256, MT == 2 ? 3 : 1) k_sfp_moments(const float* __restrict__ X,
                                                      const float* __restrict__ Y, int64_t n,
                                                      float inv_maxr, int maxm, int NCP,
                                                      float* __restrict__ part) {
-    constexpr int D = MT * 16, TSTR = D + 8;
-    extern __shared__ __align__(16) float sfs[];
+    constexpr int D = MT * 16, TS = D + 8, GS = (NB == 3) ? 40 : 24;
+    constexpr int WARP_HALVES = 2 * 32 * (TS + GS);
+    static_assert(8 * NB <= GS, "g tile width");
+    extern __shared__ __align__(16) __half sfh[];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    float* Ts = sfs + (size_t)wib * 32 * (TSTR + SFP_GSTR);
-    float* Gs = Ts + 32 * TSTR;
+    __half* Th = sfh + (size_t)wib * WARP_HALVES;
+    __half* Tl = Th + 32 * TS;
+    __half* Gh = Tl + 32 * TS;
+    __half* Gl = Gh + 32 * GS;
     const int64_t wid = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t base = wid * SFP_CHUNK;
     if (base >= n) return;
-    const int q = lane >> 2, c4 = lane & 3;
+    // ldmatrix row addresses: lane = 8 j + i supplies row i of tile j
+    const int li = lane & 7, lj = lane >> 3;
+    // A tile (16 d x 16 particles) at d0 = 16 a, particles 16 kb: tile j holds
+    // particles 8 (j >> 1) .. + 7 and d = 8 (j & 1) .. + 7
+    const uint32_t aoff = (uint32_t)(((li + 8 * (lj >> 1)) * TS + 8 * (lj & 1)) * 2);
+    // B tiles of column blocks u, u + 1: tile j holds particles 8 (j & 1) ..
+    // + 7 and columns 8 u + 8 (j >> 1) .. + 7
+    const uint32_t boff = (uint32_t)(((li + 8 * (lj & 1)) * GS + 8 * (lj >> 1)) * 2);
+    const uint32_t sTh = (uint32_t)__cvta_generic_to_shared(Th), sTl = (uint32_t)__cvta_generic_to_shared(Tl);
+    const uint32_t sGh = (uint32_t)__cvta_generic_to_shared(Gh), sGl = (uint32_t)__cvta_generic_to_shared(Gl);
     float acc[MT][NB][4];
 #pragma unroll
     for (int a = 0; a < MT; a++)
@@ -140,127 +196,163 @@ __global__ void __launch_bounds__(256) k_sfp_moments(const float* __restrict__ X
         for (int u = 0; u < NB; u++)
 #pragma unroll
             for (int i = 0; i < 4; i++) acc[a][u][i] = 0.f;
-    float col0[MT / 2 > 0 ? MT / 2 : 1];  // lane d (+32): sum of T_d
+    float run0[MT][2];  // column 0, rows 16 a + q and 16 a + q + 8 (lanes with c4 = 0)
 #pragma unroll
-    for (int h = 0; h < (MT / 2 > 0 ? MT / 2 : 1); h++) col0[h] = 0.f;
+    for (int a = 0; a < MT; a++) run0[a][0] = run0[a][1] = 0.f;
+    // B fragment of the column block (1, 0, ..., 0): b = B[2 c4 .. + 1][q], ones at q = 0
+    const uint32_t ones[2] = {lane < 4 ? 0x3C003C00u : 0u, lane < 4 ? 0x3C003C00u : 0u};
     const int64_t end = min(base + (int64_t)SFP_CHUNK, n);
+    // the coordinates of the next round are loaded one round ahead
+    // (raw values: they are scaled where they are used, a round later)
+    bool nin = base + lane < end;
+    float nx = 0.f, ny = 0.f;
+    if (nin) {
+        nx = __ldg(X + base + lane);
+        ny = __ldg(Y + base + lane);
+    }
     for (int64_t r0 = base; r0 < end; r0 += 32) {
-        // ---- features of particle r0 + lane
+        // ---- features of particle r0 + lane, split into row lane of the tiles
         {
-            const int64_t i = r0 + lane;
-            float px = 2.f, py = 0.f;  // outside the basis edge: no contribution
-            if (i < end) {
-                px = __ldg(X + i) * inv_maxr;
-                py = __ldg(Y + i) * inv_maxr;
+            // a lane past the end stands outside the basis edge: no contribution
+            const float px = nin ? nx * inv_maxr : 2.f, py = nin ? ny * inv_maxr : 0.f;
+            nin = r0 + 32 + lane < end;
+            if (nin) {
+                nx = __ldg(X + r0 + 32 + lane);
+                ny = __ldg(Y + r0 + 32 + lane);
             }
             const float p2 = px * px + py * py;
             const bool act = p2 <= 1.0f;
-            const float xc = 2.f * p2 - 1.f;
-            float* tr = Ts + lane * TSTR;
-            float tm2 = 1.f, tm1 = xc;
-            float4 v;
+            const float sw = act ? 1.f : 0.f;
+            const float xc = act ? 2.f * p2 - 1.f : 0.f, x2 = 2.f * xc;
+            // T_{d+2} = y2 T_d - T_{d-2} (y2 = 2 T_2(x)): the even and the odd
+            // terms are two independent recurrences
+            const float y2 = 2.f * fmaf(x2, xc, -1.f);
+            float T[D];
+            T[0] = sw;
+            T[1] = sw * xc;
+            T[2] = fmaf(x2, T[1], -T[0]);
+            T[3] = fmaf(x2, T[2], -T[1]);
 #pragma unroll
-            for (int d = 0; d < D; d += 4) {
-                float t4[4];
+            for (int d = 4; d < D; d++) T[d] = fmaf(y2, T[d - 2], -T[d - 4]);
 #pragma unroll
-                for (int k = 0; k < 4; k++) {
-                    const int dd = d + k;
-                    float t;
-                    if (dd == 0) t = 1.f;
-                    else if (dd == 1) t = xc;
-                    else {
-                        t = 2.f * xc * tm1 - tm2;
-                        tm2 = tm1;
-                        tm1 = t;
-                    }
-                    t4[k] = act ? t : 0.f;
-                }
-                v = make_float4(t4[0], t4[1], t4[2], t4[3]);
-                *reinterpret_cast<float4*>(tr + d) = v;
+            for (int d = 0; d < D; d += 8) {
+                uint4 h, l;
+                split_h2(T[d], T[d + 1], h.x, l.x);
+                split_h2(T[d + 2], T[d + 3], h.y, l.y);
+                split_h2(T[d + 4], T[d + 5], h.z, l.z);
+                split_h2(T[d + 6], T[d + 7], h.w, l.w);
+                *reinterpret_cast<uint4*>(Th + lane * TS + d) = h;
+                *reinterpret_cast<uint4*>(Tl + lane * TS + d) = l;
             }
-            const float pr = sqrtf(p2);
-            const float cr = pr > 0.f ? px / pr : 1.f, ci = pr > 0.f ? py / pr : 0.f;
-            float* gr = Gs + lane * SFP_GSTR;
-            float zr = 1.f, zi = 0.f;
+            // |p| and the direction (x, y) / |p| from one reciprocal square root
+            const float rs = (act && p2 > 0.f) ? rsqrtf(p2) : 0.f;
+            const float pr = p2 * rs;
+            const bool dir = rs > 0.f;
+            const float cr = dir ? px * rs : 1.f, ci = dir ? py * rs : 0.f;
+            float zr = sw, zi = 0.f;
 #pragma unroll
-            for (int u = 0; u < NB * 8; u += 2) {
-                const int m = u / 2 + 1;
-                float gc = 0.f, gs = 0.f;
-                if (m <= maxm) {
-                    const float nr = zr * cr - zi * ci;
-                    zi = zr * ci + zi * cr;
-                    zr = nr;
-                    const float f = (m & 1) ? pr : 1.f;
-                    gc = act ? zr * f : 0.f;
-                    gs = act ? zi * f : 0.f;
+            for (int u = 0; u < NB * 8; u += 8) {
+                float g[8];
+#pragma unroll
+                for (int k = 0; k < 8; k += 2) {
+                    const int m = (u + k) / 2 + 1;
+                    float gc = 0.f, gs = 0.f;
+                    if (m <= maxm) {
+                        const float nr = zr * cr - zi * ci;
+                        zi = zr * ci + zi * cr;
+                        zr = nr;
+                        gc = (m & 1) ? zr * pr : zr;
+                        gs = (m & 1) ? zi * pr : zi;
+                    }
+                    g[k] = gc;
+                    g[k + 1] = gs;
                 }
-                gr[u] = gc;
-                gr[u + 1] = gs;
+                uint4 h, l;
+                split_h2(g[0], g[1], h.x, l.x);
+                split_h2(g[2], g[3], h.y, l.y);
+                split_h2(g[4], g[5], h.z, l.z);
+                split_h2(g[6], g[7], h.w, l.w);
+                *reinterpret_cast<uint4*>(Gh + lane * GS + u) = h;
+                *reinterpret_cast<uint4*>(Gl + lane * GS + u) = l;
             }
         }
         __syncwarp();
-        // ---- column 0 on the CUDA cores
-#pragma unroll 8
-        for (int pp = 0; pp < 32; pp++) {
+        // ---- columns 1 .. 8 NB on the tensor cores, 2 k-blocks of 16 particles
+        float f0[MT][4];  // column 0 of this round
 #pragma unroll
-            for (int h = 0; h < (MT / 2 > 0 ? MT / 2 : 1); h++) col0[h] += Ts[pp * TSTR + lane + 32 * h];
-        }
-        // ---- columns 1 .. 8 NB on the tensor cores, 4 k-blocks of 8 particles
-#pragma unroll
-        for (int kb = 0; kb < 4; kb++) {
-            const float* t0 = Ts + (8 * kb + c4) * TSTR;
-            const float* t1 = t0 + 4 * TSTR;
-            const float* g0 = Gs + (8 * kb + c4) * SFP_GSTR;
-            const float* g1 = g0 + 4 * SFP_GSTR;
+        for (int kb = 0; kb < 2; kb++) {
             uint32_t bh[NB][2], bl[NB][2];
+            const uint32_t kbA = (uint32_t)(16 * kb * TS * 2), kbB = (uint32_t)(16 * kb * GS * 2);
 #pragma unroll
-            for (int u = 0; u < NB; u++) {
-                const float v0 = g0[8 * u + q], v1 = g1[8 * u + q];
-                bh[u][0] = f2tf32(v0);
-                bl[u][0] = f2tf32(v0 - __uint_as_float(bh[u][0]));
-                bh[u][1] = f2tf32(v1);
-                bl[u][1] = f2tf32(v1 - __uint_as_float(bh[u][1]));
+            for (int u = 0; u < NB; u += 2) {
+                if (u + 1 < NB) {
+                    uint32_t r[4];
+                    ldsm_t4(r, sGh + kbB + boff + 16 * u);
+                    bh[u][0] = r[0]; bh[u][1] = r[1]; bh[u + 1][0] = r[2]; bh[u + 1][1] = r[3];
+                    ldsm_t4(r, sGl + kbB + boff + 16 * u);
+                    bl[u][0] = r[0]; bl[u][1] = r[1]; bl[u + 1][0] = r[2]; bl[u + 1][1] = r[3];
+                } else {
+                    ldsm_t2(bh[u], sGh + kbB + boff + 16 * u);
+                    ldsm_t2(bl[u], sGl + kbB + boff + 16 * u);
+                }
+            }
+            uint32_t ah[MT][4], al[MT][4];
+#pragma unroll
+            for (int a = 0; a < MT; a++) {
+                ldsm_t4(ah[a], sTh + kbA + aoff + 32 * a);
+                ldsm_t4(al[a], sTl + kbA + aoff + 32 * a);
             }
 #pragma unroll
             for (int a = 0; a < MT; a++) {
-                // a0 = A[q][c4], a1 = A[q+8][c4], a2 = A[q][c4+4], a3 = A[q+8][c4+4]
-                const float v[4] = {t0[16 * a + q], t0[16 * a + q + 8], t1[16 * a + q], t1[16 * a + q + 8]};
-                uint32_t ah[4], al[4];
-#pragma unroll
-                for (int i = 0; i < 4; i++) {
-                    ah[i] = f2tf32(v[i]);
-                    al[i] = f2tf32(v[i] - __uint_as_float(ah[i]));
-                }
-#pragma unroll
-                for (int u = 0; u < NB; u++) {
-                    mma_tf32(acc[a][u], al, bh[u]);
-                    mma_tf32(acc[a][u], ah, bl[u]);
-                    mma_tf32(acc[a][u], ah, bh[u]);
-                }
+                if (kb == 0) mma_f16_0(f0[a], ah[a], ones);
+                else mma_f16(f0[a], ah[a], ones);
             }
+#pragma unroll
+            for (int a = 0; a < MT; a++)
+#pragma unroll
+                for (int u = 0; u < NB; u++) mma_f16(acc[a][u], al[a], bh[u]);
+#pragma unroll
+            for (int a = 0; a < MT; a++)
+#pragma unroll
+                for (int u = 0; u < NB; u++) mma_f16(acc[a][u], ah[a], bl[u]);
+#pragma unroll
+            for (int a = 0; a < MT; a++)
+#pragma unroll
+                for (int u = 0; u < NB; u++) mma_f16(acc[a][u], ah[a], bh[u]);
+#pragma unroll
+            for (int a = 0; a < MT; a++) mma_f16(f0[a], al[a], ones);
+        }
+#pragma unroll
+        for (int a = 0; a < MT; a++) {
+            run0[a][0] += f0[a][0];
+            run0[a][1] += f0[a][2];
         }
         __syncwarp();
     }
     // c0 = D[q][2c4], c1 = D[q][2c4+1], c2 = D[q+8][2c4], c3 = D[q+8][2c4+1]; column
     // n of the product is feature column n + 1
+    const int q = lane >> 2, c4 = lane & 3;
     float* dst = part + wid * (size_t)D * NCP;
 #pragma unroll
     for (int a = 0; a < MT; a++)
 #pragma unroll
         for (int u = 0; u < NB; u++) {
-            const int r0 = a * 16 + q, cc = u * 8 + 2 * c4 + 1;
+            const int rr = a * 16 + q, cc = u * 8 + 2 * c4 + 1;
             if (cc < NCP) {
-                dst[r0 * NCP + cc] = acc[a][u][0];
-                dst[(r0 + 8) * NCP + cc] = acc[a][u][2];
+                dst[rr * NCP + cc] = acc[a][u][0];
+                dst[(rr + 8) * NCP + cc] = acc[a][u][2];
             }
             if (cc + 1 < NCP) {
-                dst[r0 * NCP + cc + 1] = acc[a][u][1];
-                dst[(r0 + 8) * NCP + cc + 1] = acc[a][u][3];
+                dst[rr * NCP + cc + 1] = acc[a][u][1];
+                dst[(rr + 8) * NCP + cc + 1] = acc[a][u][3];
             }
         }
 #pragma unroll
-    for (int h = 0; h < (MT / 2 > 0 ? MT / 2 : 1); h++)
-        if (lane + 32 * h < D) dst[(lane + 32 * h) * NCP] = col0[h];
+    for (int a = 0; a < MT; a++)
+        if (c4 == 0) {
+            dst[(a * 16 + q) * NCP] = run0[a][0];
+            dst[(a * 16 + q + 8) * NCP] = run0[a][1];
+        }
     // columns past the products
     for (int i = lane; i < D * (NCP - 1 - 8 * NB); i += 32) {
         const int d = i / (NCP - 1 - 8 * NB), c = 1 + 8 * NB + (i - d * (NCP - 1 - 8 * NB));
@@ -284,6 +376,26 @@ __global__ void k_sfp_reduce(const T* __restrict__ part, int64_t nwarp, int nmom
         __syncthreads();
     }
     if (threadIdx.x == 0) mom[i] = sh[0];
+}
+
+// First stage of the coalesced FP64 sum of per-warp (or per-block) partial
+// rows: block b sums rows [b rpb, (b + 1) rpb) of part[nrow][nmom] in a
+// fixed order, each thread a set of moment columns (consecutive threads on
+// consecutive columns); k_sfp_reduce then sums the nslab rows of out.
+template <typename T>
+__global__ void k_sfp_slab(const T* __restrict__ part, int64_t nrow, int nmom, int64_t rpb,
+                           double* __restrict__ out) {
+    const int64_t r0 = blockIdx.x * rpb, r1 = min(nrow, r0 + rpb);
+    for (int i = threadIdx.x; i < nmom; i += blockDim.x) {
+        double s0 = 0.0, s1 = 0.0;
+        int64_t r = r0;
+        for (; r + 1 < r1; r += 2) {
+            s0 += (double)part[r * nmom + i];
+            s1 += (double)part[(r + 1) * nmom + i];
+        }
+        if (r < r1) s0 += (double)part[r * nmom + i];
+        out[blockIdx.x * (int64_t)nmom + i] = s0 + s1;
+    }
 }
 
 // plain FP64 moments on CUDA cores: features staged per block, one thread
@@ -428,9 +540,10 @@ extern "C" int gx_sfp_init(const GxSfpBasis* b, double maxr, int device, GxSfp**
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&s->e0);
     if (e == cudaSuccess) e = cudaEventCreate(&s->e1);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&s->mom, sizeof(double) * 64 * 32);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s->mom, sizeof(double) * SFP_MAXMOM);
     if (e == cudaSuccess) e = cudaDeviceGetAttribute(&s->nsm, cudaDevAttrMultiProcessorCount, device);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&s->upart, sizeof(double) * (size_t)s->nsm * 32 * 32);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s->upart, sizeof(double) * (size_t)s->nsm * SFP_MAXMOM);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&s->slab, sizeof(double) * (size_t)2 * s->nsm * SFP_MAXMOM);
     if (e == cudaSuccess) e = cudaMalloc((void**)&s->errword, sizeof(int32_t));
     if (e == cudaSuccess) e = cudaMemset(s->errword, 0, sizeof(int32_t));
     if (e != cudaSuccess) {
@@ -446,7 +559,7 @@ extern "C" void gx_sfp_destroy(GxSfp* s) {
     if (!s) return;
     cudaSetDevice(s->dev);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    void* p[] = {s->xy, s->part, s->mom, s->qc, s->upart, s->errword};
+    void* p[] = {s->xy, s->part, s->mom, s->qc, s->upart, s->slab, s->errword};
     for (void* q : p)
         if (q) cudaFree(q);
     if (s->e0) cudaEventDestroy(s->e0);
@@ -495,65 +608,76 @@ extern "C" int gx_sfp_load(GxSfp* s, const float* coords, int64_t n, int stride)
 // ---------------------------------------------------------------------------
 // Moments on the 5th-generation tensor cores (tcgen05, TMEM accumulator).
 //
-// One tcgen05.mma.cta_group::1.kind::tf32 per 8 particles, M = 128, N = 40,
-// K = 8, both operands K-major in shared memory without swizzle:
-//   A rows 0..31   T_d hi (TF32 part of T_d(x_p)), rows 32..63 T_d lo
-//   (T_d - hi); rows 64..127 are not used (the tile of the next K-block,
-//   read by the MMA, never read back).
-//   B rows  0      g_0 = 1, rows 1..16 g_n hi, rows 17..32 g_n lo, 33..39 0.
-// D[m][n] in TMEM then holds every product of the hi/lo split:
-//   M[d][0] = D[d][0] + D[d+32][0],
-//   M[d][c] = D[d][c] + D[d][c+16] + D[d+32][c] + D[d+32][c+16]  (c = 1..16).
-// Layout of a K-block tile (UMMA canonical K-major, no swizzle): core
-// matrices of 8 rows x 16 bytes; the two 16-byte halves of K are LBO = 144
-// bytes apart, 8-row groups SBO = 288 bytes apart; consecutive K-blocks of a
-// round are 2336 (A) / 1440 (B) bytes apart.  These strides put the 32
-// scalar stores of a warp (4 K-blocks x 8 particles) on 32 distinct banks.
-// A CTA of 256 threads takes rounds of 128 particles (two threads per
-// particle: one writes its T rows, the other its g rows),
-// triple-buffered; one thread issues the 16 MMAs of a round and commits
-// them to the buffer's mbarrier.  Every UM_DRAIN rounds the accumulator is
-// drained into FP64 shared memory (warps 0 and 1 read TMEM lanes 0..63)
-// and the next MMA starts it afresh.  Waits are bounded; on time-out the
-// CTA raises the error word, waits (bounded) for its MMAs, frees its TMEM.
-#define UM_T 128          // particles per round
-#define UM_THREADS 256    // threads 0..127 write the T rows, 128..255 the g rows
-#define UM_KB (UM_T / 8)  // K-blocks per round
-#define UM_N 40
-#define UM_LBO 144
-#define UM_SBO 288
-#define UM_SA 2336        // A bytes per K-block (8 groups x 288 + 32)
-#define UM_SB 1440        // B bytes per K-block (5 groups x 288)
-#define UM_ABYTES (UM_KB * UM_SA + 8 * UM_SBO)  // + the rows 64..127 of the last K-block
-#define UM_BUFBYTES (UM_ABYTES + UM_KB * UM_SB)
+// One tcgen05.mma.cta_group::1.kind::f16 per 16 particles, M = 128, N = 48,
+// K = 16, FP32 accumulation in TMEM, both operands MN-major in shared
+// memory without swizzle, so that every particle's features are 16-byte
+// row vectors (one st.shared.v4 per 8 values):
+//   A rows  0..15  T_d hi (FP16) for even d = 2i, rows 16..31 for odd
+//   d = 2i + 1; rows 32..63 the lo parts (T_d - hi) in the same order;
+//   rows 64..127 are not used (the descriptor's M blocks 8..15 fall on the
+//   next K-block, read by the MMA, never read back).
+//   B columns 0..15 g_n hi (n = 1..16: cos m phi, sin m phi, m = 1..8,
+//   times p for odd m), 16..31 the lo parts, 32 g_0 = 1, 33..47 zero.
+// D[r][c] in TMEM then holds every product of the hi/lo split:
+//   M[d][0] = D[h][32] + D[h + 32][32],
+//   M[d][c] = D[h][c-1] + D[h][c+15] + D[h+32][c-1] + D[h+32][c+15]
+// with h = d / 2 for even d and 16 + d / 2 for odd d (summed on the host).
+// Canonical MN-major layout: a core matrix is 8 K-rows (particles) of 16
+// bytes (8 consecutive M or N elements), 128 bytes contiguous; M / N blocks
+// of 8 are SBO = 128 bytes apart, K-blocks of 8 particles LBO = 1024 (A) /
+// 768 (B) bytes apart.  A warp's 32 particles write 4 K-blocks: the 8 lanes
+// of a K-block fill one 128-byte core matrix, so the stores are conflict
+// free.
+// A CTA (one per SM) has 16 producer warps, two threads per particle: the
+// "even" thread runs T_0, T_2, .. (T_{d+2} = 2 T_2 T_d - T_{d-2}) and g for
+// m = 1..4, the "odd" thread T_1, T_3, .. and g for m = 5..8 (from z^4) and
+// the column of ones.  Rounds of 256 particles, three stages; warp 18 waits
+// for a stage, issues its 16 MMAs and commits them to the stage's empty
+// barrier.  The accumulator alternates between two TMEM regions, one per
+// group of UM_DRAIN rounds (1024 particles): after a group's last MMA the
+// issuer commits to that region's barrier, and warps 16 and 17 (TMEM lanes
+// 0..31 and 32..63) add it in FP64 into the CTA's partial rows in global
+// memory, then release the region, while the MMAs of the next group run
+// into the other one.  Waits are bounded; on time-out the CTA raises the
+// error word, waits (bounded) for its issued MMAs and frees its TMEM.
+#define UM_T 256                    // particles per round
+#define UM_PROD 512                 // producer threads (two per particle)
+#define UM_THREADS (UM_PROD + 96)   // + drain warps 16, 17 and the issue warp 18
+#define UM_KB (UM_T / 8)            // K-blocks per round
+#define UM_N 48
+#define UM_AKB 1024                 // A bytes per K-block (8 blocks x 128)
+#define UM_BKB 768                  // B bytes per K-block (6 blocks x 128)
+#define UM_ABYTES (UM_KB * UM_AKB + UM_AKB)  // + M blocks 8..15 of the last K-block
+#define UM_BUFBYTES (UM_ABYTES + UM_KB * UM_BKB)
 #define UM_NBUF 3
-#define UM_DRAIN 8
-#define UM_TMEM_COLS 64
+#define UM_DRAIN 4                  // rounds per accumulator group
+#define UM_TMEM_COLS 128            // two regions of UM_N columns, 64 apart
+#define UM_NRAW (64 * UM_N)         // partial row entries per CTA
+static_assert(UM_NRAW <= SFP_MAXMOM, "raw rows fit the moment buffers");
 #define UM_SPIN (1u << 22)
 
 __device__ __forceinline__ uint32_t um_smem(const void* p) {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
-__device__ __forceinline__ uint32_t um_off(int r, int k) {
-    return (uint32_t)((r >> 3) * UM_SBO + (k >> 2) * UM_LBO + (r & 7) * 16 + (k & 3) * 4);
-}
-// shared-memory matrix descriptor: start, LBO, SBO (16-byte units), version 1
-__device__ __forceinline__ uint64_t um_desc(uint32_t saddr) {
+// shared-memory matrix descriptor: start, LBO (K-block stride), SBO (M / N
+// block stride), in 16-byte units; version 1, base offset 0, no swizzle
+__device__ __forceinline__ uint64_t um_desc(uint32_t saddr, uint32_t lbo) {
     uint64_t d = 0;
     d |= (uint64_t)((saddr >> 4) & 0x3FFF);
-    d |= (uint64_t)((UM_LBO >> 4) & 0x3FFF) << 16;
-    d |= (uint64_t)((UM_SBO >> 4) & 0x3FFF) << 32;
-    d |= (uint64_t)1 << 46;  // version
-    return d;                // base offset 0, legacy LBO mode, no swizzle
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((128u >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
 }
-// instruction descriptor: D F32, A and B TF32, both K-major, N = 40, M = 128
-#define UM_IDESC ((1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(UM_N >> 3) << 17) | (8u << 24))
+// instruction descriptor: D F32, A and B F16, both MN-major, N = 48, M = 128
+#define UM_IDESC ((1u << 4) | (0u << 7) | (0u << 10) | (1u << 15) | (1u << 16) | \
+                  ((uint32_t)(UM_N >> 3) << 17) | (8u << 24))
 
 __device__ __forceinline__ void um_mma(uint32_t tmem_d, uint64_t ad, uint64_t bd, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %3, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %4, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %4, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem_d),
         "l"(ad), "l"(bd), "r"(accumulate), "r"(UM_IDESC), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
         : "memory");
 }
@@ -577,6 +701,18 @@ __device__ __forceinline__ bool um_wait(uint64_t* b, uint32_t parity) {
         if (um_try(b, parity)) return true;
     return false;
 }
+// the same for the issue and drain warps, which wait most of the time: a
+// short sleep between tries leaves the issue slots to the producers
+__device__ __forceinline__ bool um_wait_idle(uint64_t* b, uint32_t parity) {
+    for (uint32_t i = 0; i < UM_SPIN; i++) {
+        if (um_try(b, parity)) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void um_arrive(uint64_t* b) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(um_smem(b)) : "memory");
+}
 __device__ __forceinline__ void um_fence_before() {
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
 }
@@ -593,34 +729,42 @@ __device__ __forceinline__ void um_ld8(uint32_t taddr, float* v) {
 #pragma unroll
     for (int i = 0; i < 8; i++) v[i] = __uint_as_float(r[i]);
 }
+// hi / lo halves of eight values into two 16-byte row vectors
+__device__ __forceinline__ void um_split8(const float* v, uint4& h, uint4& l) {
+    split_h2(v[0], v[1], h.x, l.x);
+    split_h2(v[2], v[3], h.y, l.y);
+    split_h2(v[4], v[5], h.z, l.z);
+    split_h2(v[6], v[7], h.w, l.w);
+}
 
-__global__ void __launch_bounds__(UM_THREADS + 64, 1) k_sfp_umma(const float* __restrict__ X,
-                                                                  const float* __restrict__ Y, int64_t n,
-                                                                  float inv_maxr, int maxm,
-                                                                  double* __restrict__ part, int NCP,
-                                                                  int32_t* __restrict__ errword) {
+__global__ void __launch_bounds__(UM_THREADS, 1) k_sfp_umma(const float* __restrict__ X,
+                                                            const float* __restrict__ Y, int64_t n,
+                                                            float inv_maxr, int maxm,
+                                                            double* __restrict__ raw,
+                                                            int32_t* __restrict__ errword) {
     extern __shared__ __align__(1024) unsigned char um_sm[];
-    __shared__ __align__(8) uint64_t full[UM_NBUF], empty[UM_NBUF];
+    __shared__ __align__(8) uint64_t full[UM_NBUF], empty[UM_NBUF], accfull[2], drained[2];
     __shared__ uint32_t tmem_slot;
-    unsigned char* buf0 = um_sm;
-    double* drain = reinterpret_cast<double*>(um_sm + UM_NBUF * UM_BUFBYTES);  // [64][UM_N]
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int NG = 2 * maxm;  // harmonic columns g_1 .. g_NG
-    const int nthr = UM_THREADS + 64;
-    const int MMAW = UM_THREADS / 32;  // warps MMAW (issue + lanes 0..31), MMAW + 1 (lanes 32..63)
+    constexpr int DW0 = UM_PROD / 32, ISW = DW0 + 2;  // drain warps DW0, DW0 + 1; issue warp
+    static_assert(DW0 % 4 == 0, "the drain warps read TMEM lanes 0..31 and 32..63");
     if (tid == 0) {
         for (int b = 0; b < UM_NBUF; b++) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(um_smem(&full[b])), "r"(UM_THREADS / 32)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(um_smem(&full[b])), "r"(UM_PROD / 32)
                          : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(um_smem(&empty[b])) : "memory");
         }
+        for (int a = 0; a < 2; a++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(um_smem(&accfull[a])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 2;" ::"r"(um_smem(&drained[a])) : "memory");
+        }
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    for (int i = tid; i < 64 * UM_N; i += nthr) drain[i] = 0.0;
-    // zero every buffer once (B rows past the harmonics, the padding rows)
-    for (int i = tid; i < UM_NBUF * UM_BUFBYTES / 4; i += nthr) reinterpret_cast<float*>(um_sm)[i] = 0.f;
+    // zero every stage once (B columns 33..47, the rows past the last K-block)
+    for (int i = tid; i < UM_NBUF * UM_BUFBYTES / 16; i += UM_THREADS)
+        reinterpret_cast<uint4*>(um_sm)[i] = make_uint4(0u, 0u, 0u, 0u);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (warp == MMAW) {
+    if (warp == ISW) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(um_smem(&tmem_slot)),
                      "r"(UM_TMEM_COLS)
                      : "memory");
@@ -632,10 +776,12 @@ __global__ void __launch_bounds__(UM_THREADS + 64, 1) k_sfp_umma(const float* __
     const uint32_t tmem = tmem_slot;
     const int64_t rounds_total = (n + UM_T - 1) / UM_T;
     const int64_t my_rounds = (blockIdx.x < rounds_total) ? (rounds_total - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    const int64_t ngroups = (my_rounds + UM_DRAIN - 1) / UM_DRAIN;
 
-    if (warp < MMAW) {
+    if (warp < DW0) {
         // ------------------------------------------------------------ producers
-        const int pt = tid & (UM_T - 1), role = tid / UM_T;  // particle of the round, rows written
+        const int pt = tid & (UM_T - 1), odd = tid / UM_T;  // particle of the round, its half
+        const int kb = pt >> 3, r = pt & 7;
         float nx = 0.f, ny = 0.f;
         bool nv = false;
         if (my_rounds > 0) {
@@ -648,8 +794,8 @@ __global__ void __launch_bounds__(UM_THREADS + 64, 1) k_sfp_umma(const float* __
         }
         for (int64_t li = 0; li < my_rounds; li++) {
             const int64_t rnd = blockIdx.x + li * gridDim.x;
-            const float cx = nx, cy = ny;
-            const bool cv = nv;
+            // a slot past the last particle sits outside the basis edge
+            const float px = nv ? nx * inv_maxr : 2.f, py = nv ? ny * inv_maxr : 0.f;
             {
                 const int64_t i = (rnd + gridDim.x) * UM_T + pt;
                 nv = false;
@@ -659,143 +805,155 @@ __global__ void __launch_bounds__(UM_THREADS + 64, 1) k_sfp_umma(const float* __
                     nv = true;
                 }
             }
-            const int b = (int)(li % UM_NBUF);
-            if (li >= UM_NBUF && !um_wait(&empty[b], (uint32_t)(((li / UM_NBUF) - 1) & 1))) {
-                atomicExch(errword, 5);
-                break;
-            }
-            unsigned char* A = buf0 + (size_t)b * UM_BUFBYTES;
-            unsigned char* B = A + UM_ABYTES;
-            // a slot past the last particle sits outside the basis edge
-            const float px = cv ? cx * inv_maxr : 2.f;
-            const float py = cv ? cy * inv_maxr : 0.f;
             const float p2 = px * px + py * py;
             const bool act = p2 <= 1.0f;
-            const float xc = 2.f * p2 - 1.f;
-            const int kb = pt >> 3, k = pt & 7;
-            if (role == 0) {
-                unsigned char* a = A + kb * UM_SA;
-                float tm2 = 1.f, tm1 = xc;
+            const float sw = act ? 1.f : 0.f;
+            const float xc = act ? 2.f * p2 - 1.f : 0.f, x2 = 2.f * xc;
+            const float y2 = 2.f * fmaf(x2, xc, -1.f);  // 2 T_2(x)
+            // |p| and the direction (x, y) / |p| from one reciprocal square root
+            const float rs = (act && p2 > 0.f) ? rsqrtf(p2) : 0.f;
+            const float pr = p2 * rs;
+            const bool dir = rs > 0.f;
+            const float cr = dir ? px * rs : 1.f, ci = dir ? py * rs : 0.f;
+            // T_{odd + 2j}, j = 0..15 (seeded with sw: zero outside the edge)
+            float t[16];
+            t[0] = odd ? sw * xc : sw;
+            t[1] = odd ? fmaf(x2, fmaf(x2, sw * xc, -sw), -sw * xc) : fmaf(x2, sw * xc, -sw);
 #pragma unroll
-                for (int d = 0; d < 32; d++) {
-                    float t;
-                    if (d == 0) t = 1.f;
-                    else if (d == 1) t = xc;
-                    else {
-                        t = 2.f * xc * tm1 - tm2;
-                        tm2 = tm1;
-                        tm1 = t;
-                    }
-                    t = act ? t : 0.f;
-                    const float hi = __uint_as_float(f2tf32(t));
-                    *reinterpret_cast<float*>(a + um_off(d, k)) = hi;
-                    *reinterpret_cast<float*>(a + um_off(d + 32, k)) = t - hi;
+            for (int j = 2; j < 16; j++) t[j] = fmaf(y2, t[j - 1], -t[j - 2]);
+            // g for m = 1..4 (even half) or 5..8 (odd half)
+            float g[8];
+            {
+                float zr = sw, zi = 0.f;
+                if (odd) {  // z^4
+                    const float ar = cr * cr - ci * ci, ai = 2.f * cr * ci;
+                    zr = sw * (ar * ar - ai * ai);
+                    zi = sw * (2.f * ar * ai);
                 }
-            } else {
-                unsigned char* bb = B + kb * UM_SB;
-                *reinterpret_cast<float*>(bb + um_off(0, k)) = act ? 1.f : 0.f;
-                const float pr = sqrtf(p2);
-                const float cr = pr > 0.f ? px / pr : 1.f, ci = pr > 0.f ? py / pr : 0.f;
-                float zr = 1.f, zi = 0.f;
 #pragma unroll
-                for (int u = 0; u < 16; u += 2) {
-                    const int m = u / 2 + 1;
-                    float gc = 0.f, gs = 0.f;
-                    if (u < NG) {
-                        const float nr = zr * cr - zi * ci;
-                        zi = zr * ci + zi * cr;
-                        zr = nr;
-                        const float f = (m & 1) ? pr : 1.f;
-                        gc = act ? zr * f : 0.f;
-                        gs = act ? zi * f : 0.f;
-                    }
-                    const float hc = __uint_as_float(f2tf32(gc)), hs = __uint_as_float(f2tf32(gs));
-                    *reinterpret_cast<float*>(bb + um_off(1 + u, k)) = hc;
-                    *reinterpret_cast<float*>(bb + um_off(2 + u, k)) = hs;
-                    *reinterpret_cast<float*>(bb + um_off(17 + u, k)) = gc - hc;
-                    *reinterpret_cast<float*>(bb + um_off(18 + u, k)) = gs - hs;
+                for (int k = 0; k < 4; k++) {
+                    const int m = 4 * odd + k + 1;
+                    const float nr = zr * cr - zi * ci;
+                    zi = zr * ci + zi * cr;
+                    zr = nr;
+                    const bool on = m <= maxm;
+                    const float f = (m & 1) ? pr : 1.f;
+                    g[2 * k] = on ? zr * f : 0.f;
+                    g[2 * k + 1] = on ? zi * f : 0.f;
                 }
             }
+            const int b = (int)(li % UM_NBUF);
+            // warp-uniform: a lane that timed out takes its whole warp out
+            if (li >= UM_NBUF &&
+                !__all_sync(0xffffffffu, um_wait(&empty[b], (uint32_t)(((li / UM_NBUF) - 1) & 1)))) {
+                if (lane == 0) atomicExch(errword, 5);
+                break;
+            }
+            unsigned char* A = um_sm + (size_t)b * UM_BUFBYTES + kb * UM_AKB + r * 16;
+            unsigned char* B = um_sm + (size_t)b * UM_BUFBYTES + UM_ABYTES + kb * UM_BKB + r * 16;
+            uint4 h, l;
+            um_split8(t, h, l);  // d = odd + 0, 2, .., 14: M block 2 odd (hi), 4 + 2 odd (lo)
+            *reinterpret_cast<uint4*>(A + (2 * odd) * 128) = h;
+            *reinterpret_cast<uint4*>(A + (4 + 2 * odd) * 128) = l;
+            um_split8(t + 8, h, l);  // d = odd + 16, .., 30
+            *reinterpret_cast<uint4*>(A + (2 * odd + 1) * 128) = h;
+            *reinterpret_cast<uint4*>(A + (5 + 2 * odd) * 128) = l;
+            um_split8(g, h, l);  // columns 8 odd .. + 7: N block odd (hi), 2 + odd (lo)
+            *reinterpret_cast<uint4*>(B + odd * 128) = h;
+            *reinterpret_cast<uint4*>(B + (2 + odd) * 128) = l;
+            if (odd) *reinterpret_cast<uint4*>(B + 4 * 128) = make_uint4(act ? 0x3C00u : 0u, 0u, 0u, 0u);
             // generic-proxy stores -> async proxy (the tensor core reads shared memory)
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             __syncwarp();
-            if (lane == 0)
-                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(um_smem(&full[b])) : "memory");
+            if (lane == 0) um_arrive(&full[b]);
         }
-    } else {
-        // ------------------------------------------------- MMA issue and drain
-        // both warps take every iteration and every named barrier; after a
-        // failed wait a warp only skips work (never the barrier)
-        const bool issuer = (warp == MMAW);
+    } else if (warp == ISW) {
+        // ------------------------------------------------------------ MMA issue
         bool ok = true;
-        int since = 0;
-        for (int64_t li = 0; li < my_rounds; li++) {
+        int64_t last = -1;  // last round whose MMAs were committed
+        for (int64_t li = 0; li < my_rounds && ok; li++) {
             const int b = (int)(li % UM_NBUF);
-            if (issuer && ok) {
-                if (!um_wait(&full[b], (uint32_t)((li / UM_NBUF) & 1))) {
-                    atomicExch(errword, 5);
-                    ok = false;
-                }
-                um_fence_after();
-                if (ok && lane == 0) {
-                    const uint32_t a0 = um_smem(buf0 + (size_t)b * UM_BUFBYTES), b0 = a0 + UM_ABYTES;
+            const int64_t grp = li / UM_DRAIN;
+            const int acc = (int)(grp & 1);
+            const bool first = (li % UM_DRAIN) == 0;
+            const bool lastr = (li % UM_DRAIN) == UM_DRAIN - 1 || li + 1 == my_rounds;
+            if (first && grp >= 2) ok = __all_sync(0xffffffffu, um_wait_idle(&drained[acc], (uint32_t)(((grp / 2) - 1) & 1)));
+            if (ok) ok = __all_sync(0xffffffffu, um_wait_idle(&full[b], (uint32_t)((li / UM_NBUF) & 1)));
+            if (!ok) {
+                if (lane == 0) atomicExch(errword, 5);
+                break;
+            }
+            um_fence_after();
+            if (lane == 0) {
+                const uint32_t a0 = um_smem(um_sm + (size_t)b * UM_BUFBYTES), b0 = a0 + UM_ABYTES;
+                const uint32_t td = tmem + (uint32_t)(64 * acc);
 #pragma unroll 1
-                    for (int kb = 0; kb < UM_KB; kb++)
-                        um_mma(tmem, um_desc(a0 + kb * UM_SA), um_desc(b0 + kb * UM_SB),
-                               (since == 0 && kb == 0) ? 0u : 1u);
-                    um_commit(&empty[b]);
-                }
-                __syncwarp();
+                for (int k = 0; k < UM_KB / 2; k++)
+                    um_mma(td, um_desc(a0 + k * 2 * UM_AKB, UM_AKB), um_desc(b0 + k * 2 * UM_BKB, UM_BKB),
+                           (first && k == 0) ? 0u : 1u);
+                um_commit(&empty[b]);
+                if (lastr) um_commit(&accfull[acc]);
             }
-            since++;
-            if (since == UM_DRAIN || li + 1 == my_rounds) {
-                // both drain warps meet once the issuer has committed this round
-                // (a parity wait must not start more than one phase early), then
-                // wait for its MMAs (and all before)
-                asm volatile("bar.sync 1, 64;" ::: "memory");
-                if (ok && !um_wait(&empty[b], (uint32_t)((li / UM_NBUF) & 1))) {
-                    atomicExch(errword, 5);
-                    ok = false;
-                }
-                um_fence_after();
-                if (ok) {
-                    float v[UM_N];
-                    const int q = warp - MMAW;  // TMEM lanes 32 q .. 32 q + 31
-#pragma unroll
-                    for (int c = 0; c < UM_N; c += 8) um_ld8(tmem + ((uint32_t)(32 * q) << 16) + c, v + c);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                    double* dr = drain + (32 * q + lane) * UM_N;
-#pragma unroll
-                    for (int c = 0; c < UM_N; c++) dr[c] += (double)v[c];
-                }
-                um_fence_before();
-                asm volatile("bar.sync 1, 64;" ::: "memory");  // the next MMA may overwrite
-                um_fence_after();
-                since = 0;
-            }
+            __syncwarp();
+            last = li;
         }
-        if (!ok && issuer && lane == 0 && my_rounds > 0) {
-            // wait (bounded) for whatever was committed before freeing TMEM
-            for (int bb = 0; bb < UM_NBUF; bb++) um_wait(&empty[bb], 0u);
+        if (last >= 0 && lane == 0)  // every issued MMA has completed (bounded)
+            um_wait(&empty[(int)(last % UM_NBUF)], (uint32_t)((last / UM_NBUF) & 1));
+        __syncwarp();
+    } else {
+        // ------------------------------------------------- drain (TMEM -> FP64)
+        const int q = warp - DW0;  // TMEM lanes 32 q .. 32 q + 31
+        double* row = raw + ((size_t)blockIdx.x * 64 + 32 * q + lane) * UM_N;
+        if (ngroups == 0)
+            for (int c = 0; c < UM_N; c++) row[c] = 0.0;
+        for (int64_t grp = 0; grp < ngroups; grp++) {
+            const int acc = (int)(grp & 1);
+            if (!__all_sync(0xffffffffu, um_wait_idle(&accfull[acc], (uint32_t)((grp / 2) & 1)))) {
+                if (lane == 0) atomicExch(errword, 5);
+                break;
+            }
+            um_fence_after();
+            float v[UM_N];
+#pragma unroll
+            for (int c = 0; c < UM_N; c += 8)
+                um_ld8(tmem + ((uint32_t)(32 * q) << 16) + (uint32_t)(64 * acc + c), v + c);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            um_fence_before();
+            __syncwarp();
+            if (lane == 0) um_arrive(&drained[acc]);
+#pragma unroll
+            for (int c = 0; c < UM_N; c += 2) {
+                double2 s = make_double2((double)v[c], (double)v[c + 1]);
+                if (grp > 0) {
+                    const double2 o = *reinterpret_cast<const double2*>(row + c);
+                    s.x += o.x;
+                    s.y += o.y;
+                }
+                *reinterpret_cast<double2*>(row + c) = s;
+            }
         }
     }
     um_fence_before();
     __syncthreads();
     um_fence_after();
-    if (warp == MMAW)
+    if (warp == ISW)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(UM_TMEM_COLS)
                      : "memory");
-    // combine the hi/lo quadrants: part[cta][d][c], c < NCP
-    double* dst = part + (size_t)blockIdx.x * 32 * NCP;
-    for (int i = tid; i < 32 * NCP; i += nthr) {
-        const int d = i / NCP, c = i - d * NCP;
-        double v = 0.0;
-        if (c == 0) v = drain[d * UM_N] + drain[(d + 32) * UM_N];
-        else if (c <= NG && c <= 16)
-            v = drain[d * UM_N + c] + drain[d * UM_N + c + 16] + drain[(d + 32) * UM_N + c] +
-                drain[(d + 32) * UM_N + c + 16];
-        dst[i] = v;
-    }
+}
+
+// mom = the FP64 sum of the nrow partial rows part[nrow][nmom]: slabs of
+// rows summed coalesced (at most 2 per SM), then the slab sums
+template <typename T>
+static int sfp_sum_rows(GxSfp* s, const T* part, int64_t nrow, int nmom) {
+    const int64_t nslab = std::min<int64_t>(nrow, 2 * (int64_t)s->nsm);
+    const int64_t rpb = (nrow + nslab - 1) / nslab;
+    const int nsl = (int)((nrow + rpb - 1) / rpb);
+    k_sfp_slab<T><<<nsl, 256, 0, s->stream>>>(part, nrow, nmom, rpb, s->slab);
+    SFP_CUDA(s, cudaGetLastError());
+    k_sfp_reduce<double><<<nmom, 256, 0, s->stream>>>(s->slab, nsl, nmom, s->mom);
+    SFP_CUDA(s, cudaGetLastError());
+    s->launches += 2;
+    return GX_OK;
 }
 
 // moments on the device (precision GX_PREC_MIXED: tensor cores; GX_PREC_FP64: CUDA cores)
@@ -809,43 +967,38 @@ static int sfp_moments(GxSfp* s, int precision) {
         k_sfp_moments64<<<(unsigned)nb, 256, sm, s->stream>>>(s->xy, s->xy + s->cap, n, 1.0 / s->maxr,
                                                               s->b.maxm, D, NCP, (double*)s->part);
         SFP_CUDA(s, cudaGetLastError());
-        k_sfp_reduce<double><<<nmom, 256, 0, s->stream>>>((double*)s->part, nb, nmom, s->mom);
-        SFP_CUDA(s, cudaGetLastError());
-        s->launches += 2;
-        return GX_OK;
+        s->launches += 1;
+        return sfp_sum_rows<double>(s, (const double*)s->part, nb, nmom);
     }
     const float inv = (float)(1.0 / s->maxr);
     if (precision == GX_PREC_MIXED_TC05) {
         if (D != 32 || s->NC > 17)
             return s->err = "the tcgen05 path takes at most 32 Chebyshev terms and maxm <= 8", GX_ERR_RANGE;
-        // tcgen05: one CTA per SM (at most), FP64 partial per CTA
+        // tcgen05: one CTA per SM (at most), FP64 partial rows [64][UM_N] per CTA
         const int64_t rounds = (n + UM_T - 1) / UM_T;
         const int grid = (int)std::min<int64_t>(rounds, s->nsm);
-        const size_t sm = (size_t)UM_NBUF * UM_BUFBYTES + sizeof(double) * 64 * UM_N;
+        // (+ 4 KB past the stages: no descriptor-addressed read can leave the allocation)
+        const size_t sm = (size_t)UM_NBUF * UM_BUFBYTES + 4096;
         SFP_CUDA(s, cudaFuncSetAttribute(k_sfp_umma, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_sfp_umma<<<grid, UM_THREADS + 64, sm, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->upart, NCP,
-                                                  s->errword);
+        k_sfp_umma<<<grid, UM_THREADS, sm, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, s->upart,
+                                                         s->errword);
         SFP_CUDA(s, cudaGetLastError());
-        k_sfp_reduce<double><<<32 * NCP, 256, 0, s->stream>>>(s->upart, grid, 32 * NCP, s->mom);
-        SFP_CUDA(s, cudaGetLastError());
-        s->launches += 2;
-        return GX_OK;
+        s->launches += 1;
+        return sfp_sum_rows<double>(s, s->upart, grid, UM_NRAW);
     }
     const int64_t nw = (n + SFP_CHUNK - 1) / SFP_CHUNK;
     const unsigned grid = (unsigned)((nw * 32 + 255) / 256);
     // feature columns 1 .. NC - 1 in blocks of 8
     const int NB = (s->NC - 1 + 7) / 8;
     if (NB > 3) return s->err = "more than 11 harmonics on the tensor-core path", GX_ERR_RANGE;
-    const size_t sm = sizeof(float) * 8 * 32 * ((size_t)(D + 8) + SFP_GSTR);
+    const size_t sm = sizeof(__half) * 8 * 2 * 32 * ((size_t)(D + 8) + (NB == 3 ? 40 : 24));
     auto k = (D == 32) ? ((NB <= 1) ? k_sfp_moments<2, 1> : (NB == 2) ? k_sfp_moments<2, 2> : k_sfp_moments<2, 3>)
                        : ((NB <= 1) ? k_sfp_moments<4, 1> : (NB == 2) ? k_sfp_moments<4, 2> : k_sfp_moments<4, 3>);
     SFP_CUDA(s, cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     k<<<grid, 256, sm, s->stream>>>(s->xy, s->xy + s->cap, n, inv, s->b.maxm, NCP, s->part);
     SFP_CUDA(s, cudaGetLastError());
-    k_sfp_reduce<float><<<nmom, 256, 0, s->stream>>>(s->part, nw, nmom, s->mom);
-    SFP_CUDA(s, cudaGetLastError());
-    s->launches += 2;
-    return GX_OK;
+    s->launches += 1;
+    return sfp_sum_rows<float>(s, s->part, nw, nmom);
 }
 
 // sfpsum + scaled: coeff[n * (2 maxm + 1) + m + maxm] (cosine +m, sine -m)
@@ -864,9 +1017,24 @@ extern "C" int gx_sfp_sum(GxSfp* s, int precision, double pmass, double* coeff) 
         if (rc) return rc;
     }
     SFP_CUDA(s, cudaEventRecord(s->e1, s->stream));
-    if (s->n > 0)
+    std::vector<double> raw;
+    if (s->n > 0 && precision == GX_PREC_MIXED_TC05) {
+        raw.resize(UM_NRAW);
+        SFP_CUDA(s, cudaMemcpyAsync(raw.data(), s->mom, sizeof(double) * UM_NRAW, cudaMemcpyDeviceToHost, s->stream));
+    } else if (s->n > 0)
         SFP_CUDA(s, cudaMemcpyAsync(mom.data(), s->mom, sizeof(double) * D * NCP, cudaMemcpyDeviceToHost, s->stream));
     SFP_CUDA(s, cudaStreamSynchronize(s->stream));
+    if (!raw.empty()) {
+        // the tcgen05 rows: T_d hi at row h (h = d / 2 for even d, 16 + d / 2
+        // for odd d), lo at h + 32; columns g hi 0..15, g lo 16..31, ones 32
+        for (int d = 0; d < D; d++) {
+            const double* rh = raw.data() + (size_t)((d & 1) ? 16 + d / 2 : d / 2) * UM_N;
+            const double* rl = rh + 32 * UM_N;
+            mom[(size_t)d * NCP] = rh[32] + rl[32];
+            for (int c = 1; c < NCP; c++)
+                mom[(size_t)d * NCP + c] = (c <= 16) ? rh[c - 1] + rh[c + 15] + rl[c - 1] + rl[c + 15] : 0.0;
+        }
+    }
     SFP_CUDA(s, cudaEventElapsedTime(&s->last_ms, s->e0, s->e1));
     {
         int32_t ew = 0;
