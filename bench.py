@@ -413,7 +413,7 @@ def run_sfp(n=20_000_000, reps=5):
                 "coeff_rel_err_vs_fp64": float(np.linalg.norm(c32 - c64) / np.linalg.norm(c64)),
                 "tcgen05_path": {"ms": round(float(np.median(t5)), 4),
                                  "coeff_rel_err_vs_fp64": float(np.linalg.norm(c5 - c64) / np.linalg.norm(c64)),
-                                 "what": "MMA M=128 N=40 K=8 per 8 particles, TMEM accumulator"},
+                                 "what": "tcgen05.mma M=128 N=48 K=16 per 16 particles, FP16 hi/lo operands MN-major in shared memory, TMEM accumulator"},
                 "hbm_GB_s": round(nbytes / (ms * 1e-3) / 1e9, 1),
                 "hbm_frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 4),
                 "useful_tflops": round(2 * n * 340 / (ms * 1e-3) / 1e12, 3)})
