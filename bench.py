@@ -405,6 +405,12 @@ def run_sfp(n=20_000_000, reps=5):
         for _ in range(reps):
             c5 = s.sum(1.0 / n, 2)
             t5.append(s.last_ms()[0])
+        # the SFP-driven time loop (sum + force + kick/drift per step, one
+        # host round trip per step for the coefficients), wall clock
+        s.step(2, 0.01, pmass=1.0 / n)
+        t0 = time.perf_counter()
+        s.step(10, 0.01, pmass=1.0 / n)
+        step_ms = (time.perf_counter() - t0) * 1e3 / 10
     ms = float(np.median(t))
     peak, src = peaks()
     nbytes = n * 8
@@ -414,6 +420,8 @@ def run_sfp(n=20_000_000, reps=5):
                 "tcgen05_path": {"ms": round(float(np.median(t5)), 4),
                                  "coeff_rel_err_vs_fp64": float(np.linalg.norm(c5 - c64) / np.linalg.norm(c64)),
                                  "what": "tcgen05.mma M=128 N=48 K=16 per 16 particles, FP16 hi/lo operands MN-major in shared memory, TMEM accumulator"},
+                "sfp_step": {"ms_per_step": round(step_ms, 4), "particle_steps_per_s": n / (step_ms * 1e-3),
+                             "what": "gx_sfp_step: coefficients (mma.sync path), force and leapfrog per step, wall clock"},
                 "hbm_GB_s": round(nbytes / (ms * 1e-3) / 1e9, 1),
                 "hbm_frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 4),
                 "useful_tflops": round(2 * n * 340 / (ms * 1e-3) / 1e12, 3)})

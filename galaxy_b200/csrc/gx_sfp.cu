@@ -49,6 +49,8 @@ struct GxSfp {
     double maxr = 1.0;
     int64_t n = 0, cap = 0;
     float* xy = nullptr;        // [2][cap]
+    float* vel = nullptr;       // [2][cap] velocities of the SFP-driven step
+    std::vector<double> qs_h;   // host staging of the force series
     float* part = nullptr;      // per-warp partial moments
     double* mom = nullptr;      // [D][NCP] FP64 moments
     double* qc = nullptr;       // device force series [2][maxm+1][D]
@@ -439,64 +441,87 @@ __global__ void k_sfp_moments64(const float* __restrict__ X, const float* __rest
     }
 }
 
-// sfpacc (sfpacc.f:41-112, 249-259) from the per-m Chebyshev series of the
-// scaled coefficients: qc[(0/1)][m][d] (cosine / sine), FP64
+// sfpacc (sfpacc.f:41-112, 249-259) at (x, y) from the per-m Chebyshev
+// series of the scaled coefficients: qc[(0/1)][m][d] (cosine / sine), FP64;
+// zero outside the basis edge r > maxr
+__device__ __forceinline__ void sfp_force(double x, double y, double maxr, int maxm, int D,
+                                          const double* __restrict__ qs, double& ax, double& ay, double& ph) {
+    const double rr = sqrt(x * x + y * y);
+    double ar = 0, at = 0;
+    ax = ay = ph = 0.0;
+    if (rr > maxr) return;
+    const double r = rr > 1e-5 ? rr : 1e-5;
+    const double c1 = x / r, s1 = y / r;
+    const double p = rr / maxr, xc = 2.0 * p * p - 1.0;
+    double cm = 1.0, sm = 0.0;  // cos m phi, sin m phi
+    for (int m = 0; m <= maxm; m++) {
+        if (m > 0) {
+            double nc = cm * c1 - sm * s1;
+            sm = sm * c1 + cm * s1;
+            cm = nc;
+        }
+        // Clenshaw for Q(x) and Q'(x) of both series
+        double val[2], der[2];
+        for (int h = 0; h < 2; h++) {
+            const double* a = qs + ((size_t)h * (maxm + 1) + m) * D;
+            double b1 = 0, b2 = 0, d1 = 0, d2 = 0;
+            for (int d = D - 1; d >= 1; d--) {
+                double bn = 2.0 * xc * b1 - b2 + a[d];
+                double dn = 2.0 * xc * d1 - d2 + 2.0 * b1;
+                b2 = b1;
+                b1 = bn;
+                d2 = d1;
+                d1 = dn;
+            }
+            val[h] = xc * b1 - b2 + a[0];
+            der[h] = xc * d1 - d2 + b1;
+        }
+        // f = p^e Q(x) (e = m mod 2), df/dp = e Q + p^e Q'(x) dx/dp, dx/dp = 4 p
+        const double pe = (m & 1) ? p : 1.0, e = (double)(m & 1);
+        const double fc = pe * val[0], fs = pe * val[1];
+        const double dc = e * val[0] + pe * der[0] * 4.0 * p;
+        const double ds = e * val[1] + pe * der[1] * 4.0 * p;
+        if (m == 0) {
+            ar += dc;
+            ph -= fc;
+        } else {
+            ar += dc * cm + ds * sm;
+            at += (double)m * (fs * cm - fc * sm);
+            ph -= fc * cm + fs * sm;
+        }
+    }
+    at = at * maxr / r;
+    ax = ar * c1 - at * s1;
+    ay = ar * s1 + at * c1;
+}
+
 __global__ void k_sfp_acc(const float* __restrict__ X, const float* __restrict__ Y, int64_t n,
                           double maxr, int maxm, int D, const double* __restrict__ qs,
                           float* __restrict__ acc, float* __restrict__ pot) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const double x = X[i], y = Y[i];
-    double rr = sqrt(x * x + y * y);
-    double ar = 0, at = 0, ph = 0;
-    if (rr <= maxr) {
-        const double r = rr > 1e-5 ? rr : 1e-5;
-        const double c1 = x / r, s1 = y / r;
-        const double p = rr / maxr, xc = 2.0 * p * p - 1.0;
-        double cm = 1.0, sm = 0.0;  // cos m phi, sin m phi
-        for (int m = 0; m <= maxm; m++) {
-            if (m > 0) {
-                double nc = cm * c1 - sm * s1;
-                sm = sm * c1 + cm * s1;
-                cm = nc;
-            }
-            // Clenshaw for Q(x) and Q'(x) of both series
-            double val[2], der[2];
-            for (int h = 0; h < 2; h++) {
-                const double* a = qs + ((size_t)h * (maxm + 1) + m) * D;
-                double b1 = 0, b2 = 0, d1 = 0, d2 = 0;
-                for (int d = D - 1; d >= 1; d--) {
-                    double bn = 2.0 * xc * b1 - b2 + a[d];
-                    double dn = 2.0 * xc * d1 - d2 + 2.0 * b1;
-                    b2 = b1;
-                    b1 = bn;
-                    d2 = d1;
-                    d1 = dn;
-                }
-                val[h] = xc * b1 - b2 + a[0];
-                der[h] = xc * d1 - d2 + b1;
-            }
-            // f = p^e Q(x) (e = m mod 2), df/dp = e Q + p^e Q'(x) dx/dp, dx/dp = 4 p
-            const double pe = (m & 1) ? p : 1.0, e = (double)(m & 1);
-            const double fc = pe * val[0], fs = pe * val[1];
-            const double dc = e * val[0] + pe * der[0] * 4.0 * p;
-            const double ds = e * val[1] + pe * der[1] * 4.0 * p;
-            if (m == 0) {
-                ar += dc;
-                ph -= fc;
-            } else {
-                ar += dc * cm + ds * sm;
-                at += (double)m * (fs * cm - fc * sm);
-                ph -= fc * cm + fs * sm;
-            }
-        }
-        at = at * maxr / r;
-        acc[2 * i] = (float)(ar * c1 - at * s1);
-        acc[2 * i + 1] = (float)(ar * s1 + at * c1);
-    } else {
-        acc[2 * i] = acc[2 * i + 1] = 0.f;
-    }
+    double ax, ay, ph;
+    sfp_force(X[i], Y[i], maxr, maxm, D, qs, ax, ay, ph);
+    acc[2 * i] = (float)ax;
+    acc[2 * i + 1] = (float)ay;
     if (pot) pot[i] = (float)ph;
+}
+
+// one leapfrog step in the SFP field (stpgrp.f:26-32 with the time step
+// made explicit): v += a(x) dt, x += v dt
+__global__ void k_sfp_kick(float* __restrict__ X, float* __restrict__ Y, float* __restrict__ VX,
+                           float* __restrict__ VY, int64_t n, double maxr, int maxm, int D,
+                           const double* __restrict__ qs, float dt) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float x = X[i], y = Y[i];
+    double ax, ay, ph;
+    sfp_force(x, y, maxr, maxm, D, qs, ax, ay, ph);
+    const float vx = VX[i] + (float)ax * dt, vy = VY[i] + (float)ay * dt;
+    VX[i] = vx;
+    VY[i] = vy;
+    X[i] = x + vx * dt;
+    Y[i] = y + vy * dt;
 }
 
 // ---------------------------------------------------------------------------
@@ -559,7 +584,7 @@ extern "C" void gx_sfp_destroy(GxSfp* s) {
     if (!s) return;
     cudaSetDevice(s->dev);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    void* p[] = {s->xy, s->part, s->mom, s->qc, s->upart, s->slab, s->errword};
+    void* p[] = {s->xy, s->vel, s->part, s->mom, s->qc, s->upart, s->slab, s->errword};
     for (void* q : p)
         if (q) cudaFree(q);
     if (s->e0) cudaEventDestroy(s->e0);
@@ -570,12 +595,24 @@ extern "C" void gx_sfp_destroy(GxSfp* s) {
 
 extern "C" const char* gx_sfp_last_error(const GxSfp* s) { return s ? s->err.c_str() : g_sfp_err.c_str(); }
 
+// records (x, y[, vx, vy], ...) -> SoA positions and velocities (zero when
+// the records carry none)
 __global__ void k_sfp_xy(const float* __restrict__ aos, int stride, int64_t n, int64_t cap,
-                         float* __restrict__ xy) {
+                         float* __restrict__ xy, float* __restrict__ vel) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     xy[i] = aos[i * stride];
     xy[cap + i] = aos[i * stride + 1];
+    vel[i] = stride >= 4 ? aos[i * stride + 2] : 0.f;
+    vel[cap + i] = stride >= 4 ? aos[i * stride + 3] : 0.f;
+}
+
+// SoA -> records (x, y, vx, vy)
+__global__ void k_sfp_unxy(const float* __restrict__ xy, const float* __restrict__ vel, int64_t n, int64_t cap,
+                           float4* __restrict__ aos) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    aos[i] = make_float4(xy[i], xy[cap + i], vel[i], vel[cap + i]);
 }
 
 extern "C" int gx_sfp_load(GxSfp* s, const float* coords, int64_t n, int stride) {
@@ -583,11 +620,14 @@ extern "C" int gx_sfp_load(GxSfp* s, const float* coords, int64_t n, int stride)
     cudaSetDevice(s->dev);
     if (n > s->cap) {
         if (s->xy) cudaFree(s->xy);
+        if (s->vel) cudaFree(s->vel);
         if (s->part) cudaFree(s->part);
         s->xy = nullptr;
+        s->vel = nullptr;
         s->part = nullptr;
         s->cap = std::max<int64_t>(n, 1);
         SFP_CUDA(s, cudaMalloc((void**)&s->xy, sizeof(float) * 2 * s->cap));
+        SFP_CUDA(s, cudaMalloc((void**)&s->vel, sizeof(float) * 2 * s->cap));
         const int64_t nw = (s->cap + SFP_CHUNK - 1) / SFP_CHUNK;
         const int64_t nb = (s->cap + 255) / 256;
         const size_t bytes = std::max(sizeof(float) * nw * 64 * 32, sizeof(double) * nb * 64 * 32);
@@ -598,7 +638,7 @@ extern "C" int gx_sfp_load(GxSfp* s, const float* coords, int64_t n, int stride)
     float* tmp = nullptr;
     SFP_CUDA(s, cudaMallocAsync((void**)&tmp, sizeof(float) * stride * n, s->stream));
     SFP_CUDA(s, cudaMemcpyAsync(tmp, coords, sizeof(float) * stride * n, cudaMemcpyHostToDevice, s->stream));
-    k_sfp_xy<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(tmp, stride, n, s->cap, s->xy);
+    k_sfp_xy<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(tmp, stride, n, s->cap, s->xy, s->vel);
     SFP_CUDA(s, cudaGetLastError());
     SFP_CUDA(s, cudaFreeAsync(tmp, s->stream));
     SFP_CUDA(s, cudaStreamSynchronize(s->stream));
@@ -1002,11 +1042,7 @@ static int sfp_moments(GxSfp* s, int precision) {
 }
 
 // sfpsum + scaled: coeff[n * (2 maxm + 1) + m + maxm] (cosine +m, sine -m)
-extern "C" int gx_sfp_sum(GxSfp* s, int precision, double pmass, double* coeff) {
-    if (!s || !coeff) return GX_ERR_ARG;
-    if (precision != GX_PREC_MIXED && precision != GX_PREC_FP64 && precision != GX_PREC_MIXED_TC05)
-        return GX_ERR_ARG;
-    cudaSetDevice(s->dev);
+static int sfp_coeff(GxSfp* s, int precision, double pmass, double* coeff) {
     const int D = s->D, NCP = (s->NC + 7) / 8 * 8;
     const int ngx = 2 * s->b.maxm + 1, maxm = s->b.maxm;
     std::vector<double> mom((size_t)D * NCP, 0.0);
@@ -1062,24 +1098,43 @@ extern "C" int gx_sfp_sum(GxSfp* s, int precision, double pmass, double* coeff) 
     return GX_OK;
 }
 
-// sfpacc for the loaded particles from scaled coefficients; acc [n][2], pot [n]
-extern "C" int gx_sfp_acc(GxSfp* s, const double* coeff, float* acc, float* pot) {
-    if (!s || !coeff || (!acc && s->n > 0)) return GX_ERR_ARG;
+extern "C" int gx_sfp_sum(GxSfp* s, int precision, double pmass, double* coeff) {
+    if (!s || !coeff) return GX_ERR_ARG;
+    if (precision != GX_PREC_MIXED && precision != GX_PREC_FP64 && precision != GX_PREC_MIXED_TC05)
+        return GX_ERR_ARG;
     cudaSetDevice(s->dev);
+    return sfp_coeff(s, precision, pmass, coeff);
+}
+
+// the per-m Chebyshev series of the force evaluation from scaled
+// coefficients, uploaded to s->qc (stream-ordered)
+static int sfp_series(GxSfp* s, const double* coeff) {
     const int D = s->D, maxm = s->b.maxm, ngx = 2 * maxm + 1;
-    std::vector<double> qs((size_t)2 * (maxm + 1) * D, 0.0);
+    // the previous upload from this buffer has completed (every caller syncs the stream)
+    s->qs_h.assign((size_t)2 * (maxm + 1) * D, 0.0);
     for (int f = 0; f < s->nfun; f++) {
         const int m = s->msel[f], n = s->nsel[f];
         const double* a = s->acheb.data() + (size_t)f * D;
         const int l = n * ngx + maxm;
         const double cr = coeff[l + m], ci = (m > 0) ? coeff[l - m] : 0.0;
         for (int d = 0; d < D; d++) {
-            qs[((size_t)0 * (maxm + 1) + m) * D + d] += cr * a[d];
-            qs[((size_t)1 * (maxm + 1) + m) * D + d] += ci * a[d];
+            s->qs_h[((size_t)0 * (maxm + 1) + m) * D + d] += cr * a[d];
+            s->qs_h[((size_t)1 * (maxm + 1) + m) * D + d] += ci * a[d];
         }
     }
     if (!s->qc) SFP_CUDA(s, cudaMalloc((void**)&s->qc, sizeof(double) * 2 * 12 * 64));
-    SFP_CUDA(s, cudaMemcpyAsync(s->qc, qs.data(), sizeof(double) * qs.size(), cudaMemcpyHostToDevice, s->stream));
+    SFP_CUDA(s, cudaMemcpyAsync(s->qc, s->qs_h.data(), sizeof(double) * s->qs_h.size(), cudaMemcpyHostToDevice,
+                                s->stream));
+    return GX_OK;
+}
+
+// sfpacc for the loaded particles from scaled coefficients; acc [n][2], pot [n]
+extern "C" int gx_sfp_acc(GxSfp* s, const double* coeff, float* acc, float* pot) {
+    if (!s || !coeff || (!acc && s->n > 0)) return GX_ERR_ARG;
+    cudaSetDevice(s->dev);
+    const int D = s->D, maxm = s->b.maxm;
+    int rc = sfp_series(s, coeff);
+    if (rc) return rc;
     const int64_t n = s->n;
     if (n > 0) {
         float *dacc = nullptr, *dpot = nullptr;
@@ -1093,6 +1148,56 @@ extern "C" int gx_sfp_acc(GxSfp* s, const double* coeff, float* acc, float* pot)
         SFP_CUDA(s, cudaFreeAsync(dacc, s->stream));
         SFP_CUDA(s, cudaFreeAsync(dpot, s->stream));
     }
+    SFP_CUDA(s, cudaStreamSynchronize(s->stream));
+    return GX_OK;
+}
+
+// The SFP-driven time loop (the sf2d code's step, step.f:135-290: getacc
+// -> sfpacc, stpgrp, massgn -> sfpadd, then sfpsum at step.f:250): per
+// step the coefficients of the current positions (gx_sfp_sum's arithmetic
+// at `precision`), then one kernel that evaluates the force at each
+// particle and moves it, v += a dt, x += v dt.  The particles stay on the
+// device; coeff_out (may be NULL) receives the coefficients of the final
+// positions.
+extern "C" int gx_sfp_step(GxSfp* s, int nsteps, double dt, int precision, double pmass, double* coeff_out) {
+    if (!s || nsteps < 0) return GX_ERR_ARG;
+    if (precision != GX_PREC_MIXED && precision != GX_PREC_FP64 && precision != GX_PREC_MIXED_TC05)
+        return GX_ERR_ARG;
+    cudaSetDevice(s->dev);
+    const int ngx = 2 * s->b.maxm + 1;
+    std::vector<double> coeff((size_t)(s->b.maxn + 1) * ngx);
+    const int64_t n = s->n;
+    for (int k = 0; k < nsteps; k++) {
+        int rc = sfp_coeff(s, precision, pmass, coeff.data());
+        if (rc) return rc;
+        rc = sfp_series(s, coeff.data());
+        if (rc) return rc;
+        if (n > 0) {
+            k_sfp_kick<<<(unsigned)((n + 127) / 128), 128, 0, s->stream>>>(
+                s->xy, s->xy + s->cap, s->vel, s->vel + s->cap, n, s->maxr, s->b.maxm, s->D, s->qc, (float)dt);
+            SFP_CUDA(s, cudaGetLastError());
+        }
+    }
+    if (coeff_out) {
+        int rc = sfp_coeff(s, precision, pmass, coeff_out);
+        if (rc) return rc;
+    }
+    SFP_CUDA(s, cudaStreamSynchronize(s->stream));
+    return GX_OK;
+}
+
+// the loaded particles back as records (x, y, vx, vy)
+extern "C" int gx_sfp_unload(GxSfp* s, float* coords) {
+    if (!s || (s->n > 0 && !coords)) return GX_ERR_ARG;
+    cudaSetDevice(s->dev);
+    const int64_t n = s->n;
+    if (n == 0) return GX_OK;
+    float4* tmp = nullptr;
+    SFP_CUDA(s, cudaMallocAsync((void**)&tmp, sizeof(float4) * n, s->stream));
+    k_sfp_unxy<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(s->xy, s->vel, n, s->cap, tmp);
+    SFP_CUDA(s, cudaGetLastError());
+    SFP_CUDA(s, cudaMemcpyAsync(coords, tmp, sizeof(float4) * n, cudaMemcpyDeviceToHost, s->stream));
+    SFP_CUDA(s, cudaFreeAsync(tmp, s->stream));
     SFP_CUDA(s, cudaStreamSynchronize(s->stream));
     return GX_OK;
 }

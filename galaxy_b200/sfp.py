@@ -61,6 +61,8 @@ class Sfp:
         L.gx_sfp_sum.argtypes = [P, C.c_int, C.c_double, P]
         L.gx_sfp_acc.argtypes = [P, P, P, P]
         L.gx_sfp_last_ms.argtypes = [P, C.POINTER(C.c_float), C.POINTER(C.c_int64)]
+        L.gx_sfp_step.argtypes = [P, C.c_int, C.c_double, C.c_int, C.c_double, P]
+        L.gx_sfp_unload.argtypes = [P, P]
         self._L = L
         self.basis = basis
         self._h = C.c_void_p()
@@ -101,6 +103,22 @@ class Sfp:
         pot = np.zeros(self.n, np.float32)
         self._chk(self._L.gx_sfp_acc(self._h, coeff.ctypes.data, acc.ctypes.data, pot.ctypes.data))
         return acc, pot
+
+    def step(self, nsteps, dt, pmass=1.0, precision=0):
+        """nsteps leapfrog steps in the particles' own SFP field (positions
+        and velocities from `load`); returns the coefficients of the final
+        positions."""
+        b = self.basis
+        out = np.zeros((b.maxn + 1) * (2 * b.maxm + 1), np.float64)
+        self._chk(self._L.gx_sfp_step(self._h, int(nsteps), float(dt), precision, float(pmass),
+                                      out.ctypes.data))
+        return out.reshape(b.maxn + 1, 2 * b.maxm + 1)
+
+    def unload(self):
+        """The particles as (n, 4) records: x, y, vx, vy."""
+        out = np.zeros((self.n, 4), np.float32)
+        self._chk(self._L.gx_sfp_unload(self._h, out.ctypes.data))
+        return out
 
     def last_ms(self):
         ms = self._C.c_float()

@@ -363,19 +363,21 @@ int gx_sfp_init(const GxSfpBasis* basis, double maxr, int device, GxSfp** out);
 void gx_sfp_destroy(GxSfp* sfp);
 const char* gx_sfp_last_error(const GxSfp* sfp);
 
-/* Copy n particle records (stride floats each; x, y first) to the device. */
+/* Copy n particle records (stride floats each; x, y first, then vx, vy
+ * when stride >= 4, else zero velocities) to the device. */
 int gx_sfp_load(GxSfp* sfp, const float* coords, int64_t n, int stride);
 
 /* sfpsum/sfpadd + scaled: coefficients of the loaded particles with
  * r <= maxr, x pmass / maxr^2, into coeff[n * (2 maxm + 1) + m + maxm]
  * (cosine terms at +m, sine terms at -m).  precision GX_PREC_MIXED runs the
- * moment contraction on the tensor cores with warp-level mma.sync TF32
- * (operands split hi/lo, 3 products, FP32 accumulate per 1024-particle
- * chunk, FP64 across chunks); GX_PREC_MIXED_TC05 on the tcgen05 tensor cores
- * (all four hi/lo products in one MMA of M = 128, N = 40, K = 8 per 8
- * particles, accumulator in TMEM drained to FP64 every 1024 particles per
- * CTA; at most 32 Chebyshev terms and maxm <= 8); GX_PREC_FP64 on the CUDA
- * cores in FP64.  SRC/lib15/sfpsum.f:26-47, sfpadd.f:37-93, scaled.f:53-72. */
+ * moment contraction on the tensor cores with warp-level mma.sync m16n8k16
+ * FP16 (operands split into FP16 hi and lo parts, 3 products, FP32
+ * accumulate per 1024-particle chunk, FP64 across chunks);
+ * GX_PREC_MIXED_TC05 on the tcgen05 tensor cores (all four hi/lo products
+ * in one MMA of M = 128, N = 48, K = 16 per 16 particles, accumulator in
+ * TMEM drained to FP64 every 1024 particles per CTA; at most 32 Chebyshev
+ * terms and maxm <= 8); GX_PREC_FP64 on the CUDA cores in FP64.
+ * SRC/lib15/sfpsum.f:26-47, sfpadd.f:37-93, scaled.f:53-72. */
 int gx_sfp_sum(GxSfp* sfp, int precision, double pmass, double* coeff);
 
 /* sfpacc: Cartesian accelerations [n][2] and potentials [n] (pot may be
@@ -385,6 +387,20 @@ int gx_sfp_acc(GxSfp* sfp, const double* coeff, float* acc, float* pot);
 
 /* Device ms and kernel launches of the last gx_sfp_sum. */
 int gx_sfp_last_ms(const GxSfp* sfp, float* ms, int64_t* launches);
+
+/* The SFP-driven time loop of the sf2d code (SRC/lib15/step.f:135-290:
+ * getacc -> sfpacc, stpgrp, massgn -> sfpadd, sfpsum at step.f:250): nsteps
+ * leapfrog steps of the loaded particles in the field of their own
+ * coefficients.  Per step: the coefficients of the current positions
+ * (gx_sfp_sum's arithmetic at `precision`, scaled by pmass), then
+ * v += a(x) dt, x += v dt (stpgrp.f:26-32 with the time step explicit:
+ * positions, velocities and dt in the caller's units, G = 1).  The
+ * particles stay on the device; coeff_out (may be NULL) receives the
+ * coefficients of the final positions. */
+int gx_sfp_step(GxSfp* sfp, int nsteps, double dt, int precision, double pmass, double* coeff_out);
+
+/* The loaded particles as n records of 4 floats (x, y, vx, vy). */
+int gx_sfp_unload(GxSfp* sfp, float* coords);
 
 /* Adjoint of nsteps mixed-path steps (2D, one sector) of the loaded
  * particles for the objective J = |A2(t_final)|, A2 = (1/n) sum_p

@@ -4,8 +4,10 @@ CPU: the oracle's restatement of ajfun/ajder/sfptab/sfpval (table of nrtab
 radii + 5-point Lagrange interpolation, the reference's algorithm) agrees
 with direct evaluation of the basis functions, and its coefficient sum
 agrees with the direct-evaluation sum.
-GPU: gx_sfp_sum (tensor-core moments, 3xTF32) and its FP64 path against the
-oracle's FP64 sum; gx_sfp_acc against the oracle's sfpacc.
+GPU: gx_sfp_sum (tensor-core moments: mma.sync and tcgen05, FP16 hi/lo
+operands) and its FP64 path against the oracle's FP64 sum; gx_sfp_acc
+against the oracle's sfpacc; the SFP-driven time loop gx_sfp_step against
+the oracle's FP64 loop (sfpadd + sfpacc + stpgrp).
 Basis data: tests/golden/aj07.json (tests/golden/make_aj_fixture.py).
 """
 import os
@@ -88,3 +90,45 @@ def test_sfp_forces_match_oracle(basis):
         acc, pot = s.acc(coeff)
     assert np.linalg.norm(acc - acc_ref) / np.linalg.norm(acc_ref) < 1e-5
     assert np.linalg.norm(pot - pot_ref) / np.linalg.norm(pot_ref) < 1e-5
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [0, 2])
+def test_sfp_step_tracks_oracle(basis, precision):
+    """gx_sfp_step against the same loop on the oracle in FP64 (step.f:
+    sfpadd over the current positions, sfpacc, then v += a dt, x += v dt),
+    10 steps of 20k particles of the exponential disc set rotating in their
+    own initial field.  The loop on the device keeps FP32 positions and
+    velocities and evaluates the basis exactly (Chebyshev series) where the
+    oracle interpolates the reference's table."""
+    from galaxy_b200.sfp import Sfp
+    n, nsteps, dt, maxr = 20000, 10, 0.05, 6.0
+    pm = 1.0 / n
+    pos = exp_disk(n, seed=21).astype(np.float64)
+    c0 = ox.sfp_coeffs(basis, pos, maxr, pmass=pm)
+    a0, _ = ox.sfp_acc(basis, c0, pos, maxr)
+    r = np.hypot(pos[:, 0], pos[:, 1])
+    ar = -(a0[:, 0] * pos[:, 0] + a0[:, 1] * pos[:, 1]) / np.maximum(r, 1e-12)
+    vc = np.sqrt(np.maximum(r * ar, 0.0))
+    vel = np.stack([-vc * pos[:, 1], vc * pos[:, 0]], axis=1) / np.maximum(r, 1e-12)[:, None]
+    rec = np.concatenate([pos, vel], axis=1).astype(np.float32)
+    x = rec[:, :2].astype(np.float64)
+    v = rec[:, 2:].astype(np.float64)
+    for _ in range(nsteps):
+        c = ox.sfp_coeffs(basis, x, maxr, pmass=pm)
+        a, _ = ox.sfp_acc(basis, c, x, maxr)
+        v = v + a * dt
+        x = x + v * dt
+    c_ref = ox.sfp_coeffs(basis, x, maxr, pmass=pm)
+    with Sfp(basis, maxr) as s:
+        s.load(rec)
+        c_gpu = s.step(nsteps, dt, pmass=pm, precision=precision)
+        out = s.unload()
+    assert out.shape == (n, 4)
+    dx = np.abs(out[:, :2] - x).max() / np.abs(x).max()
+    dv = np.abs(out[:, 2:] - v).max() / np.abs(v).max()
+    ec = np.linalg.norm(c_gpu - c_ref) / np.linalg.norm(c_ref)
+    assert dx < 1e-5 and dv < 1e-4, (dx, dv)
+    assert ec < 1e-5, ec
+    # the particles did move: 10 steps of a rotating disc
+    assert np.abs(out[:, :2] - rec[:, :2]).max() > 0.1
