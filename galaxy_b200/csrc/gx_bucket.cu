@@ -348,7 +348,10 @@ __global__ void __launch_bounds__(BK_THREADS, BK_MINB) k_push_bkt(
                     rmin_l = min(rmin_l, cn.ju);
                     rmax_l = max(rmax_l, cn.ju);
                     if (d3) {
-                        zmin_l = min(zmin_l, cn.iz);
+                        // a cell in the top plane (a spoke coordinate that
+                        // rounded up to na moved it there) has its upper
+                        // corners in plane 0 of the next ring
+                        zmin_l = min(zmin_l, (cn.iz + 1 == ngz) ? 0 : cn.iz);
                         zmax_l = max(zmax_l, cn.iz);
                     }
                 }
