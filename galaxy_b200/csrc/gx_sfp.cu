@@ -541,7 +541,10 @@ extern "C" int gx_sfp_init(const GxSfpBasis* b, double maxr, int device, GxSfp**
         b->k < 0 || !b->xcoeff || (b->maxn > 0 && !b->roots))
         return g_sfp_err = "invalid basis selection", GX_ERR_ARG;
     if (b->maxm > 11) return g_sfp_err = "maxm > 11 not supported", GX_ERR_RANGE;
-    if (b->maxn + b->k + 1 > 64) return g_sfp_err = "maxn + k + 1 > 64 not supported", GX_ERR_RANGE;
+    // U_nm / p^(m mod 2) has degree n + k + (m - m mod 2) / 2 in x = 2 p^2 - 1:
+    // that many Chebyshev terms plus one, 32 or 64
+    const int deg = b->maxn + b->k + b->maxm / 2;
+    if (deg + 1 > 64) return g_sfp_err = "maxn + k + maxm / 2 + 1 > 64 not supported", GX_ERR_RANGE;
     GxSfp* s = new GxSfp();
     s->b = *b;
     s->roots.assign(b->roots ? b->roots : b->xcoeff,
@@ -557,7 +560,7 @@ extern "C" int gx_sfp_init(const GxSfpBasis* b, double maxr, int device, GxSfp**
             s->nsel.push_back(n);
         }
     s->nfun = (int)s->msel.size();
-    s->D = (b->maxn + b->k + 1 <= 32) ? 32 : 64;
+    s->D = (deg + 1 <= 32) ? 32 : 64;
     s->NC = 2 * b->maxm + 1;
     cheb_coeffs(s);
     s->dev = device;

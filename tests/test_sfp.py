@@ -132,3 +132,35 @@ def test_sfp_step_tracks_oracle(basis, precision):
     assert ec < 1e-5, ec
     # the particles did move: 10 steps of a rotating disc
     assert np.abs(out[:, :2] - rec[:, :2]).max() > 0.1
+
+
+@pytest.mark.gpu
+def test_sfp_sum_64_chebyshev_terms(basis):
+    """A basis whose functions need 64 Chebyshev terms: the aj07 roots with
+    the polynomial in 1 - r^2 extended to k = 16 (degree up to maxn + k +
+    maxm / 2 = 39 in x), so the sum runs the 4-tile mma.sync kernels.  Both
+    device paths against the oracle's table sum; the tcgen05 path, which
+    takes 32 terms at most, refuses the basis."""
+    from galaxy_b200 import GxError
+    from galaxy_b200.sfp import Basis, Sfp
+    rng = np.random.default_rng(5)
+    k = 16
+    roots, xc = {}, {}
+    for m in range(basis.maxm + 1):
+        for n in range(basis.maxn + 1):
+            roots[(m, n)] = list(basis.roots[m, n, :n])
+            base = list(basis.xcoeff[m, n, :])
+            xc[(m, n)] = base + list(0.05 * abs(base[0]) * rng.standard_normal(k + 1 - len(base)))
+    b16 = Basis(k, roots, xc, maxm=basis.maxm, maxn=basis.maxn)
+    pos = exp_disk(300_000, seed=13)
+    ref = ox.sfp_coeffs(b16, pos.astype(np.float64), 6.0, pmass=2.5e-6)
+    with Sfp(b16, 6.0) as s:
+        s.load(pos)
+        c32 = s.sum(pmass=2.5e-6, precision=0)
+        c64 = s.sum(pmass=2.5e-6, precision=1)
+        with pytest.raises(GxError):
+            s.sum(pmass=2.5e-6, precision=2)
+    e32 = np.linalg.norm(c32 - ref) / np.linalg.norm(ref)
+    e64 = np.linalg.norm(c64 - ref) / np.linalg.norm(ref)
+    assert e64 < 1e-7, e64
+    assert e32 < 1e-6, e32
