@@ -508,6 +508,15 @@ int gx_unload(GxCtx* c, float* coords) {
     if (!c || (!coords && c->n > 0)) return GX_ERR_ARG;
     if (c->n == 0) return GX_OK;
     cudaSetDevice(c->dev);
+    if (c->bucketed && !c->fp64 && c->nzones <= 1) {
+        // the step's bucketed store straight into the records, in load order
+        int rc = gx_bucket_unload(c, c->stagebuf);
+        if (rc) return rc;
+        GX_CUDA(c, cudaMemcpyAsync(coords, c->stagebuf, sizeof(float) * 2 * c->g.ndim * c->n,
+                                   cudaMemcpyDeviceToHost, c->stream));
+        GX_CUDA(c, cudaStreamSynchronize(c->stream));
+        return GX_OK;
+    }
     int rc = gx_dense(c);
     if (rc) return rc;
     const int nw = 2 * c->g.ndim;
@@ -531,6 +540,14 @@ int gx_unload(GxCtx* c, float* coords) {
 int gx_masset(GxCtx* c) {
     if (!c) return GX_ERR_ARG;
     cudaSetDevice(c->dev);
+    if (gx_fast_ok(c)) {
+        int rc = gx_fast_masset(c);
+        if (rc) return rc;
+        GX_CUDA(c, cudaStreamSynchronize(c->stream));
+        c->have_mass = true;
+        c->have_field = false;
+        return GX_OK;
+    }
     int rc = gx_dense(c);
     if (rc) return rc;
     c->zr_valid = false;

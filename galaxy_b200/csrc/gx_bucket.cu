@@ -281,7 +281,10 @@ __device__ __forceinline__ void rec_store(float4* __restrict__ Q, int64_t bcap, 
 // items.  Window of an item of row (ir, iz): rings ir - 1 .. ir + 2 and, in
 // 3D, planes iz - 1 .. iz + 2 (bin row 4 a + b for ring ir - 1 + a, plane
 // iz - 1 + b); 2D: rows ir - 1 .. ir + 2.
-template <int ND, bool COMP>
+// DEP: the deposit alone (masset on the bucketed store): the cell of each
+// particle's current position, its weights into the bins and the mesh, the
+// ring and plane range; no field, no move, the store is not rewritten
+template <int ND, bool COMP, bool DEP = false>
 __global__ void __launch_bounds__(BK_THREADS, BK_MINB) k_push_bkt(
     DevGeo g, const float4* __restrict__ Qin, float4* __restrict__ Qout, int64_t bcap,
     const float4* __restrict__ F,
@@ -324,24 +327,26 @@ __global__ void __launch_bounds__(BK_THREADS, BK_MINB) k_push_bkt(
                 rec_load<NP>(Qin, bcap, s, P, o);
                 float &x = P[0], &y = P[1];
                 float z = d3 ? P[2] : 0.f;
-                const CellW cw = gx_cell_t<false, ND>(g, x, y, z, true);
-                float ax, ay, az, ph;
-                gx_accel_cell_t<false, ND>(g, F, cw, x, y, z, ax, ay, az, ph);
-                float& vx = P[ND];
-                float& vy = P[ND + 1];
-                vx += ax;
-                vy += ay;
-                if (d3) P[ND + 2] += az;
-                if (COMP) {
-                    gx_comp_add(x, P[NW], vx);
-                    gx_comp_add(y, P[NW + 1], vy);
-                    if (d3) gx_comp_add(P[2], P[NW + 2], P[ND + 2]);
-                } else {
-                    x += vx;
-                    y += vy;
-                    if (d3) P[2] += P[ND + 2];
+                if (!DEP) {
+                    const CellW cw = gx_cell_t<false, ND>(g, x, y, z, true);
+                    float ax, ay, az, ph;
+                    gx_accel_cell_t<false, ND>(g, F, cw, x, y, z, ax, ay, az, ph);
+                    float& vx = P[ND];
+                    float& vy = P[ND + 1];
+                    vx += ax;
+                    vy += ay;
+                    if (d3) P[ND + 2] += az;
+                    if (COMP) {
+                        gx_comp_add(x, P[NW], vx);
+                        gx_comp_add(y, P[NW + 1], vy);
+                        if (d3) gx_comp_add(P[2], P[NW + 2], P[ND + 2]);
+                    } else {
+                        x += vx;
+                        y += vy;
+                        if (d3) P[2] += P[ND + 2];
+                    }
+                    z = d3 ? P[2] : 0.f;
                 }
-                z = d3 ? P[2] : 0.f;
                 cn = gx_cell_t<true, ND>(g, x, y, z, false);
                 rk = (cn.key >= 0) ? (uint32_t)cn.row : (uint32_t)nrow;
                 if (cn.key >= 0) {
@@ -359,14 +364,17 @@ __global__ void __launch_bounds__(BK_THREADS, BK_MINB) k_push_bkt(
             // the row's slot: warp-aggregated atomic on its fill counter,
             // issued before the deposit so that its latency overlaps it
             const unsigned lane = threadIdx.x & 31;
-            const uint32_t am = __ballot_sync(0xffffffffu, act);
-            const uint32_t peers = __match_any_sync(0xffffffffu, act ? rk : 0xffffffffu) & am;
-            const int leader = __ffs(peers) - 1;
-            int bslot = 0, capr = 0, baser = 0;
-            if (act && (int)lane == leader) bslot = atomicAdd(fill_o + rk, __popc(peers));
-            if (act) {
-                capr = __ldg(cap_o + rk);
-                baser = __ldg(base_o + rk);
+            uint32_t peers = 0;
+            int leader = -1, bslot = 0, capr = 0, baser = 0;
+            if (!DEP) {
+                const uint32_t am = __ballot_sync(0xffffffffu, act);
+                peers = __match_any_sync(0xffffffffu, act ? rk : 0xffffffffu) & am;
+                leader = __ffs(peers) - 1;
+                if (act && (int)lane == leader) bslot = atomicAdd(fill_o + rk, __popc(peers));
+                if (act) {
+                    capr = __ldg(cap_o + rk);
+                    baser = __ldg(base_o + rk);
+                }
             }
             // the common case: every corner inside the window (the new cell
             // in its inner 3 x 3 rows, or 3 rows in 2D, no plane wrap, inside
@@ -442,19 +450,21 @@ __global__ void __launch_bounds__(BK_THREADS, BK_MINB) k_push_bkt(
                     else if (v1) red_add_s64(ar + jt1, v1);
                 }
             }
-            bslot = __shfl_sync(0xffffffffu, bslot, leader < 0 ? 0 : leader);
-            const int slot = bslot + __popc(peers & lanemask_lt());
-            int64_t dst = (int64_t)baser + slot;
-            const bool ovf = act && slot >= capr;
-            const uint32_t om = __ballot_sync(0xffffffffu, ovf);
-            if (om) {
-                const int ol = __ffs(om) - 1;
-                int ob = 0;
-                if ((int)lane == ol) ob = atomicAdd(ovf_o, __popc(om));
-                ob = __shfl_sync(0xffffffffu, ob, ol);
-                if (ovf) dst = ovf_base + ob + __popc(om & lanemask_lt());
+            if (!DEP) {
+                bslot = __shfl_sync(0xffffffffu, bslot, leader < 0 ? 0 : leader);
+                const int slot = bslot + __popc(peers & lanemask_lt());
+                int64_t dst = (int64_t)baser + slot;
+                const bool ovf = act && slot >= capr;
+                const uint32_t om = __ballot_sync(0xffffffffu, ovf);
+                if (om) {
+                    const int ol = __ffs(om) - 1;
+                    int ob = 0;
+                    if ((int)lane == ol) ob = atomicAdd(ovf_o, __popc(om));
+                    ob = __shfl_sync(0xffffffffu, ob, ol);
+                    if (ovf) dst = ovf_base + ob + __popc(om & lanemask_lt());
+                }
+                if (act) rec_store<NP>(Qout, bcap, dst, P, o);
             }
-            if (act) rec_store<NP>(Qout, bcap, dst, P, o);
         }
         if (win) {
             __syncthreads();
@@ -592,6 +602,32 @@ bool gx_fast_ok(const GxCtx* c) {
 
 static inline int bk_nplanes(const GxCtx* c) { return 2 * c->g.ndim + (c->g.comp ? c->g.ndim : 0); }
 
+// bucketed store -> the host records (x, y[, z], vx, vy[, vz]) in load
+// order, straight from the records (unload without the dense store): each
+// record is read once, coalesced, and written as one 16 / 24-byte record
+template <int NP, int NW>
+__global__ void k_bk_unload(const float4* __restrict__ Qin, int64_t bcap, float* __restrict__ aos,
+                            const int4* __restrict__ items, const int32_t* __restrict__ ctl) {
+    static_assert(NW == 4 || NW == 6, "2D or 3D records");
+    const int nit = ctl[0];
+    for (int it = blockIdx.x; it < nit; it += gridDim.x) {
+        const int4 I = items[it];
+        for (int s = I.y + threadIdx.x; s < I.z; s += blockDim.x) {
+            float w[NP];
+            int32_t o;
+            rec_load<NP>(Qin, bcap, s, w, o);
+            if (NW == 4) {
+                reinterpret_cast<float4*>(aos)[o] = make_float4(w[0], w[1], w[2], w[3]);
+            } else {
+                float2* d = reinterpret_cast<float2*>(aos + (size_t)o * 6);
+                d[0] = make_float2(w[0], w[1]);
+                d[1] = make_float2(w[2], w[3]);
+                d[2] = make_float2(w[4], w[5]);
+            }
+        }
+    }
+}
+
 // float4 words of one record of the bucketed store
 int gx_bucket_words(const GxCtx* c) { return (bk_nplanes(c) + 1 + 3) / 4; }
 
@@ -727,15 +763,34 @@ int gx_dense(GxCtx* c) {
     return GX_OK;
 }
 
-template <int ND, bool COMP>
+// gx_unload's records from the bucketed store (the store stays as it is)
+int gx_bucket_unload(GxCtx* c, float* aos) {
+    const unsigned grid = 148 * 8;
+    const float4* Q = c->bq[c->bcur];
+    const int4* it = c->bk_items;
+    const int32_t* ctl = c->bk_ctl + 8;
+    // record planes: the phase space (2D: 4, 3D: 6) and the compensated
+    // update's low parts of the positions
+    if (c->g.ndim == 3) {
+        if (c->g.comp) k_bk_unload<9, 6><<<grid, 256, 0, c->stream>>>(Q, c->bcap, aos, it, ctl);
+        else k_bk_unload<6, 6><<<grid, 256, 0, c->stream>>>(Q, c->bcap, aos, it, ctl);
+    } else {
+        if (c->g.comp) k_bk_unload<6, 4><<<grid, 256, 0, c->stream>>>(Q, c->bcap, aos, it, ctl);
+        else k_bk_unload<4, 4><<<grid, 256, 0, c->stream>>>(Q, c->bcap, aos, it, ctl);
+    }
+    GX_LAUNCHED(c);
+    return GX_OK;
+}
+
+template <int ND, bool COMP, bool DEP = false>
 static int bk_launch_push(GxCtx* c, int cur, int nxt) {
     const DevGeo& g = c->g;
     const size_t sm = sizeof(uint32_t) * (ND == 3 ? 16 : 4) * g.na;
-    auto kp = k_push_bkt<ND, COMP>;
+    auto kp = k_push_bkt<ND, COMP, DEP>;
     GX_CUDA(c, cudaFuncSetAttribute(kp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     if (!c->bk_grid) {
         int per = 0, sms = 148;
-        GX_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kp, BK_THREADS, sm));
+        GX_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_push_bkt<ND, COMP>, BK_THREADS, sm));
         GX_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
         c->bk_grid = std::max(1, per) * sms;
     }
@@ -751,6 +806,30 @@ static int bk_join(GxCtx* c) {
     if (!c->bk_pending) return GX_OK;
     GX_CUDA(c, cudaStreamWaitEvent(c->stream, c->bk_ev[1], 0));
     c->bk_pending = false;
+    return GX_OK;
+}
+
+// masset on the fused path: the deposit-only pass over the bucketed store
+// (bucketized first when the particles are dense), then the conversion.
+// The mass is the same integers, converted the same way, as the sorted
+// deposit's (massgn.f:140-172), and the ring and plane ranges of the mass
+// are known to the next solve.
+int gx_fast_masset(GxCtx* c) {
+    const DevGeo& g = c->g;
+    int rc = c->bucketed ? bk_join(c) : gx_bucketize(c);
+    if (rc) return rc;
+    const int cur = c->bcur, nxt = cur ^ 1;
+    if (g.ndim == 3)
+        rc = g.comp ? bk_launch_push<3, true, true>(c, cur, nxt) : bk_launch_push<3, false, true>(c, cur, nxt);
+    else
+        rc = g.comp ? bk_launch_push<2, true, true>(c, cur, nxt) : bk_launch_push<2, false, true>(c, cur, nxt);
+    if (rc) return rc;
+    // the pass took the items through the work counter: the next pass starts it afresh
+    GX_CUDA(c, cudaMemsetAsync(c->bk_ctl + 9, 0, sizeof(int32_t), c->stream));
+    k_mass_convert<<<(unsigned)((g.mesh / 2 + 255) / 256), 256, 0, c->stream>>>(
+        c->macc, c->mass, g.mesh, g.pmass, c->bk_ctl + 13, c->jrk_d, g.nr, c->bk_ctl + 10, c->zr_d, g.ngz);
+    GX_LAUNCHED(c);
+    c->zr_valid = true;
     return GX_OK;
 }
 

@@ -701,6 +701,8 @@ int gx_comm_reduce_range(GxCtx* c);
 bool gx_fast_ok(const GxCtx* c);  // single zone, linear scheme, mixed, not GX_FLAG_SORTED_DEPOSIT
 int gx_fast_step(GxCtx* c, int nsteps, int phys);
 int gx_dense(GxCtx* c);  // bucketed store -> dense store (no-op when dense)
+int gx_bucket_unload(GxCtx* c, float* aos);  // unload from the bucketed store
+int gx_fast_masset(GxCtx* c);  // masset by the deposit-only fused pass
 int gx_bucket_alloc(GxCtx* c);
 int gx_bucket_words(const GxCtx* c);  // float4 words per record of the bucketed store
 int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk = nullptr,
