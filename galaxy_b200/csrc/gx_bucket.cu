@@ -41,8 +41,10 @@
 // gx_deposit.cu: the fused path is bitwise identical to it, whatever order
 // the atomics resolve in.  A particle's record carries its load index;
 // gx_dense() writes the store back to the n contiguous SoA particles of
-// pbuf[cur] for the entry points that walk them that way (unload, getacc,
-// tmcent, icheck, the adjoint, masset).
+// pbuf[cur] for the entry points that walk them that way (getacc, tmcent,
+// icheck, the adjoint); unload writes the records straight from the store
+// in load order, and masset deposits from the store with the same kernel
+// run without the field and the move.
 #include <algorithm>
 
 #include "gx_common.cuh"
