@@ -50,6 +50,7 @@ struct GxSfp {
     int64_t n = 0, cap = 0;
     float* xy = nullptr;        // [2][cap]
     float* vel = nullptr;       // [2][cap] velocities of the SFP-driven step
+    float4* ftab = nullptr;     // [maxm + 1][SFP_NT] force table of the SFP-driven step
     std::vector<double> qs_h;   // host staging of the force series
     float* part = nullptr;      // per-warp partial moments
     double* mom = nullptr;      // [D][NCP] FP64 moments
@@ -507,17 +508,84 @@ __global__ void k_sfp_acc(const float* __restrict__ X, const float* __restrict__
     if (pot) pot[i] = (float)ph;
 }
 
+// The time loop's force table, as the reference tabulates its basis
+// (sfptab.f:43-78) and interpolates it (sfpval.f:24-52): per m the radial
+// factors f_c, f_s = p^e Q(x) of the cosine and sine series and their
+// p-derivatives, at SFP_NT radii p_i = i / (SFP_NT - 1), evaluated in FP64
+// from the force series (Clenshaw, as sfp_force) and stored as FP32.
+#define SFP_NT 1025
+__global__ void k_sfp_ftab(int maxm, int D, const double* __restrict__ qs, float4* __restrict__ tab) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= (maxm + 1) * SFP_NT) return;
+    const int m = i / SFP_NT, j = i - m * SFP_NT;
+    const double p = (double)j / (double)(SFP_NT - 1), xc = 2.0 * p * p - 1.0;
+    double val[2], der[2];
+    for (int h = 0; h < 2; h++) {
+        const double* a = qs + ((size_t)h * (maxm + 1) + m) * D;
+        double b1 = 0, b2 = 0, d1 = 0, d2 = 0;
+        for (int d = D - 1; d >= 1; d--) {
+            const double bn = 2.0 * xc * b1 - b2 + a[d];
+            const double dn = 2.0 * xc * d1 - d2 + 2.0 * b1;
+            b2 = b1;
+            b1 = bn;
+            d2 = d1;
+            d1 = dn;
+        }
+        val[h] = xc * b1 - b2 + a[0];
+        der[h] = xc * d1 - d2 + b1;
+    }
+    const double pe = (m & 1) ? p : 1.0, e = (double)(m & 1);
+    tab[i] = make_float4((float)(pe * val[0]), (float)(pe * val[1]), (float)(e * val[0] + pe * der[0] * 4.0 * p),
+                         (float)(e * val[1] + pe * der[1] * 4.0 * p));
+}
+
 // one leapfrog step in the SFP field (stpgrp.f:26-32 with the time step
-// made explicit): v += a(x) dt, x += v dt
+// made explicit): v += a(x) dt, x += v dt, the force from the table by
+// 4-point Lagrange interpolation in p (FP32; the interpolation error of the
+// degree <= 63 series on 1025 radii is ~1e-7 of the force)
 __global__ void k_sfp_kick(float* __restrict__ X, float* __restrict__ Y, float* __restrict__ VX,
-                           float* __restrict__ VY, int64_t n, double maxr, int maxm, int D,
-                           const double* __restrict__ qs, float dt) {
+                           float* __restrict__ VY, int64_t n, float maxr, int maxm,
+                           const float4* __restrict__ tab, float dt) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float x = X[i], y = Y[i];
-    double ax, ay, ph;
-    sfp_force(x, y, maxr, maxm, D, qs, ax, ay, ph);
-    const float vx = VX[i] + (float)ax * dt, vy = VY[i] + (float)ay * dt;
+    float ax = 0.f, ay = 0.f;
+    const float rr = sqrtf(x * x + y * y);
+    if (rr <= maxr) {
+        const float r = fmaxf(rr, 1e-5f);
+        const float c1 = x / r, s1 = y / r;
+        const float u = rr / maxr * (float)(SFP_NT - 1);
+        const int i0 = min(max((int)u - 1, 0), SFP_NT - 4);
+        const float t = u - (float)i0;  // in [0, 3]: nodes i0 .. i0 + 3
+        const float w0 = -(t - 1.f) * (t - 2.f) * (t - 3.f) * (1.f / 6.f);
+        const float w1 = t * (t - 2.f) * (t - 3.f) * 0.5f;
+        const float w2 = -t * (t - 1.f) * (t - 3.f) * 0.5f;
+        const float w3 = t * (t - 1.f) * (t - 2.f) * (1.f / 6.f);
+        float ar = 0.f, at = 0.f, cm = 1.f, sm = 0.f;
+        for (int m = 0; m <= maxm; m++) {
+            if (m > 0) {
+                const float nc = cm * c1 - sm * s1;
+                sm = sm * c1 + cm * s1;
+                cm = nc;
+            }
+            const float4* q = tab + (size_t)m * SFP_NT + i0;
+            const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+            const float fc = w0 * a.x + w1 * b.x + w2 * c.x + w3 * d.x;
+            const float fs = w0 * a.y + w1 * b.y + w2 * c.y + w3 * d.y;
+            const float dc = w0 * a.z + w1 * b.z + w2 * c.z + w3 * d.z;
+            const float ds = w0 * a.w + w1 * b.w + w2 * c.w + w3 * d.w;
+            if (m == 0) {
+                ar += dc;
+            } else {
+                ar += dc * cm + ds * sm;
+                at += (float)m * (fs * cm - fc * sm);
+            }
+        }
+        at = at * maxr / r;
+        ax = ar * c1 - at * s1;
+        ay = ar * s1 + at * c1;
+    }
+    const float vx = VX[i] + ax * dt, vy = VY[i] + ay * dt;
     VX[i] = vx;
     VY[i] = vy;
     X[i] = x + vx * dt;
@@ -587,7 +655,7 @@ extern "C" void gx_sfp_destroy(GxSfp* s) {
     if (!s) return;
     cudaSetDevice(s->dev);
     if (s->stream) cudaStreamSynchronize(s->stream);
-    void* p[] = {s->xy, s->vel, s->part, s->mom, s->qc, s->upart, s->slab, s->errword};
+    void* p[] = {s->xy, s->vel, s->ftab, s->part, s->mom, s->qc, s->upart, s->slab, s->errword};
     for (void* q : p)
         if (q) cudaFree(q);
     if (s->e0) cudaEventDestroy(s->e0);
@@ -1170,14 +1238,18 @@ extern "C" int gx_sfp_step(GxSfp* s, int nsteps, double dt, int precision, doubl
     const int ngx = 2 * s->b.maxm + 1;
     std::vector<double> coeff((size_t)(s->b.maxn + 1) * ngx);
     const int64_t n = s->n;
+    if (!s->ftab) SFP_CUDA(s, cudaMalloc((void**)&s->ftab, sizeof(float4) * 12 * SFP_NT));
     for (int k = 0; k < nsteps; k++) {
         int rc = sfp_coeff(s, precision, pmass, coeff.data());
         if (rc) return rc;
         rc = sfp_series(s, coeff.data());
         if (rc) return rc;
         if (n > 0) {
-            k_sfp_kick<<<(unsigned)((n + 127) / 128), 128, 0, s->stream>>>(
-                s->xy, s->xy + s->cap, s->vel, s->vel + s->cap, n, s->maxr, s->b.maxm, s->D, s->qc, (float)dt);
+            const int nt = (s->b.maxm + 1) * SFP_NT;
+            k_sfp_ftab<<<(unsigned)((nt + 127) / 128), 128, 0, s->stream>>>(s->b.maxm, s->D, s->qc, s->ftab);
+            SFP_CUDA(s, cudaGetLastError());
+            k_sfp_kick<<<(unsigned)((n + 255) / 256), 256, 0, s->stream>>>(
+                s->xy, s->xy + s->cap, s->vel, s->vel + s->cap, n, (float)s->maxr, s->b.maxm, s->ftab, (float)dt);
             SFP_CUDA(s, cudaGetLastError());
         }
     }
