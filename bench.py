@@ -14,7 +14,7 @@ table 411 MB per step), so no flush is needed between steps.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 --impl reference times the CPU restatement of the same step (the oracle
-port; the Fortran reference cannot be built in this image) on the host
+port; the Fortran reference cannot be built without a Fortran compiler) on the host
 cores, on a bounded sample of the same workload.
 Under torchrun (N > 1) each rank owns its own particles (weak scaling) and
 the ranks sum their mass grids every step (the reference's MPI design).

@@ -1,7 +1,7 @@
 /*
  * gx_oracle.c -- CPU restatement of the GALAXY v15 polar-grid PM step.
- * TEST INFRASTRUCTURE ONLY (see gx_oracle.h): the checker for the CUDA
- * library, never part of the product path.
+ * TEST INFRASTRUCTURE ONLY (see gx_oracle.h): what the CUDA library's
+ * results are checked against, never part of the product path.
  */
 #include "gx_oracle.h"
 

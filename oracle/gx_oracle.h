@@ -1,12 +1,12 @@
 /*
  * gx_oracle.h -- CPU restatement of the GALAXY v15 polar-grid PM step.
  *
- * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path:
+ * TEST INFRASTRUCTURE ONLY.  The CUDA path's results are checked against it:
  * only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may
  * load it.  The product path (galaxy_b200/libgalaxy_gpu.so) never links or
  * calls it.
  *
- * The reference (Fortran 77, SRC/lib15) cannot be compiled in this image (no
+ * The reference (Fortran 77, SRC/lib15) cannot be compiled here (no
  * Fortran compiler), so each routine below restates the reference routine it
  * names, in the reference's loop order, in two flavours built from one
  * template (gx_oracle_tmpl.h):

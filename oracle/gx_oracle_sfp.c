@@ -1,8 +1,8 @@
 /*
  * gx_oracle_sfp.c -- CPU restatement of the SFP (smooth-field-particle)
  * Abel-Jacobi coefficient sum and force evaluation, FP64.
- * TEST INFRASTRUCTURE ONLY (see gx_oracle.h): the checker for the CUDA
- * library's gx_sfp_* entry points.
+ * TEST INFRASTRUCTURE ONLY (see gx_oracle.h): what the CUDA library's
+ * gx_sfp_* entry points are checked against.
  *
  * Follows: ajfun.f:33-47 (basis function), ajder.f:38-101 (its radial
  * derivative), sfptab.f:43-78 (table at nrtab radii), sfpval.f:24-52 (5-point

@@ -1,7 +1,7 @@
 """ctypes driver of the CPU oracle (oracle/liboracle.so).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
-bench.py's CPU-baseline leg, as the checker.  The product path
+bench.py's CPU-baseline leg, to check results against.  The product path
 (galaxy_b200) never imports this module.
 
 Every function wraps one restated reference routine; see gx_oracle.h for
