@@ -238,15 +238,27 @@ __device__ __forceinline__ int64_t bk_slot(bool act, uint32_t rk, const int32_t*
     return dst;
 }
 
-// A particle of the bucketed store is one record of R float4 words, planes
-// of bcap records each (word plane q of record s at Q[q * bcap + s]): its NP
-// floats (x, y[, z], vx, vy[, vz][, the compensated low parts]) then its load
-// index as float bits, zero-padded: two 16-byte accesses per particle in 3D
-// instead of seven 4-byte ones, each with its own 64-bit address.
+// A particle of the bucketed store is one record of R float4 words (R even:
+// 32 or 64 bytes), record s at Q[R s]: its NP floats (x, y[, z], vx, vy[,
+// vz][, the compensated low parts]) then its load index as float bits,
+// zero-padded.  A record moves with one or two 32-byte accesses
+// (ld/st .v8.f32): a warp's loads of consecutive records are contiguous,
+// and each store writes whole 32-byte sectors.
 template <int NP>
 struct Rec {
-    static constexpr int R = (NP + 1 + 3) / 4;
+    static constexpr int R = ((NP + 1 + 7) / 8) * 2;
 };
+
+__device__ __forceinline__ void ld8f(const float4* p, float* w) {
+    asm volatile("ld.global.nc.v8.f32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=f"(w[0]), "=f"(w[1]), "=f"(w[2]), "=f"(w[3]), "=f"(w[4]), "=f"(w[5]), "=f"(w[6]), "=f"(w[7])
+                 : "l"(p));
+}
+__device__ __forceinline__ void st8f(float4* p, const float* w) {
+    asm volatile("st.global.v8.f32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"l"(p), "f"(w[0]), "f"(w[1]), "f"(w[2]),
+                 "f"(w[3]), "f"(w[4]), "f"(w[5]), "f"(w[6]), "f"(w[7])
+                 : "memory");
+}
 
 template <int NP>
 __device__ __forceinline__ void rec_load(const float4* __restrict__ Q, int64_t bcap, int64_t s, float* P,
@@ -254,13 +266,7 @@ __device__ __forceinline__ void rec_load(const float4* __restrict__ Q, int64_t b
     constexpr int R = Rec<NP>::R;
     float w[4 * R];
 #pragma unroll
-    for (int q = 0; q < R; q++) {
-        const float4 v = __ldg(Q + q * bcap + s);
-        w[4 * q] = v.x;
-        w[4 * q + 1] = v.y;
-        w[4 * q + 2] = v.z;
-        w[4 * q + 3] = v.w;
-    }
+    for (int q = 0; q < R; q += 2) ld8f(Q + R * s + q, w + 4 * q);
 #pragma unroll
     for (int k = 0; k < NP; k++) P[k] = w[k];
     o = __float_as_int(w[NP]);
@@ -275,7 +281,7 @@ __device__ __forceinline__ void rec_store(float4* __restrict__ Q, int64_t bcap, 
     for (int k = 0; k < 4 * R; k++) w[k] = (k < NP) ? P[k] : 0.f;
     w[NP] = __int_as_float(o);
 #pragma unroll
-    for (int q = 0; q < R; q++) Q[q * bcap + s] = make_float4(w[4 * q], w[4 * q + 1], w[4 * q + 2], w[4 * q + 3]);
+    for (int q = 0; q < R; q += 2) st8f(Q + R * s + q, w + 4 * q);
 }
 
 // The fused particle pass of one step.  Persistent CTAs take work items from
@@ -631,7 +637,7 @@ __global__ void k_bk_unload(const float4* __restrict__ Qin, int64_t bcap, float*
 }
 
 // float4 words of one record of the bucketed store
-int gx_bucket_words(const GxCtx* c) { return (bk_nplanes(c) + 1 + 3) / 4; }
+int gx_bucket_words(const GxCtx* c) { return (bk_nplanes(c) + 1 + 7) / 8 * 2; }
 
 static inline size_t bk_npad(const GxCtx* c);
 static int bk_plan(GxCtx* c, int out, bool with_items, cudaStream_t st);
