@@ -394,6 +394,7 @@ static int adj_solve(GxCtx* c, const float* S, int64_t n) {
     GX_CUDA(c, cudaMemcpyAsync(c->pbuf[c->cur], S, sizeof(float) * n, cudaMemcpyDeviceToDevice, c->stream));
     GX_CUDA(c, cudaMemcpyAsync(c->pbuf[c->cur] + c->cap, S + n, sizeof(float) * n, cudaMemcpyDeviceToDevice,
                                c->stream));
+    c->zr_valid = false;  // the mass array is no longer a fused pass's
     int rc = gx_mixed_masset(c);
     if (rc) return rc;
     return gx_mixed_findf(c, 0, true);
@@ -525,6 +526,7 @@ extern "C" int gx_adjoint(GxCtx* c, int nsteps, int ckpt_every, double* J_out, f
     if (g.comp)  // the low parts of compensated positions start at zero, as after gx_loadup
         GX_CUDA(c, cudaMemsetAsync(c->pbuf[c->cur] + (size_t)4 * c->cap, 0, sizeof(float) * 2 * c->cap, st));
     c->have_keys = false;
+    c->zr_valid = false;
     int rc = gx_mixed_masset(c);
     if (rc) return rc;
     GX_CUDA(c, cudaStreamSynchronize(st));
