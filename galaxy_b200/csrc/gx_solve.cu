@@ -55,20 +55,6 @@ __device__ __forceinline__ void sgemm44(int M, int N, int K, const float* A, int
 }
 
 // forward azimuthal twiddles T[j][2a] = cos(2 pi m_a j / na), T[j][2a+1] = -sin(...)
-__device__ void build_taz(float* T, const int* __restrict__ act, int na, int nact, int ncp) {
-    for (int i = threadIdx.x; i < na * ncp; i += blockDim.x) {
-        int j = i / ncp, c = i - j * ncp;
-        float v = 0.f;
-        if (c < 2 * nact) {
-            int m = act[c >> 1];
-            int idx = (int)(((int64_t)m * j) % na);
-            float s, co;
-            sincospif(2.0f * (float)idx / (float)na, &s, &co);
-            v = (c & 1) ? -s : co;
-        }
-        T[i] = v;
-    }
-}
 
 // C[M][N] = A[M][K] * B[K][N] in shared memory, 4x4 register tiles with the
 // K sum split over KS adjacent lanes (lane ks takes k = ks, ks + KS, ...) and
@@ -313,41 +299,49 @@ __global__ void __launch_bounds__(288) k_fwd_z(DevGeo g, int nact, int ncp,
 }
 
 // 2D forward transform, RB rings per CTA.
-#define RB2 16
-__global__ void k_fwd2(DevGeo g, int nact, int ncp, const float* __restrict__ mass,
-                       float4* __restrict__ S) {
+#define RB2 4
+// 2D forward (p2manl.f:32-45): RB2 rings per CTA, one warp per ring; lane c
+// sums column c of the active-harmonic DFT (the twiddle table of the
+// context, k_fwdtab) over the ring's na spokes in spoke order, the m = 0
+// column in FP64 over the warp.  S[a nr + ir] = (a_m, 0, b_m, 0).
+__global__ void __launch_bounds__(32 * RB2) k_fwd2(DevGeo g, int nact, int ncp, const float* __restrict__ mass,
+                                                   const float* __restrict__ Taz, float4* __restrict__ S) {
     extern __shared__ __align__(16) float sm[];
     const int na = g.na, nr = g.nr;
     const int ldx = na + 1;
-    const int jr1 = nr - 1;
     const int ir0 = blockIdx.x * RB2;
     float* X = sm;                   // [RB2][na + 1]
     float* T = X + RB2 * ldx;        // [na][ncp]
     for (int i = threadIdx.x; i < RB2 * na; i += blockDim.x) {
-        int r = i / na, j = i - r * na;
-        int ir = ir0 + r;
-        X[r * ldx + j] = (ir <= jr1) ? mass[(size_t)ir * na + j] : 0.f;
+        const int r = i / na, j = i - r * na, ir = ir0 + r;
+        X[r * ldx + j] = (ir < nr) ? __ldg(mass + (size_t)ir * na + j) : 0.f;
     }
-    build_taz(T, g.act, na, nact, ncp);
+    for (int i = threadIdx.x; i < na * ncp; i += blockDim.x) T[i] = __ldg(Taz + i);
     __syncthreads();
-    sgemm44(RB2, ncp, na, X, ldx, T, ncp, [&](int r0, int c0, float (&acc)[4][4]) {
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            int ir = ir0 + r0 + i;
-            if (ir > jr1) continue;
-            double s0 = 0.0;
-            bool m0 = (c0 == 0) && (g.act[0] == 0);
-            if (m0)
-                for (int j = 0; j < na; j++) s0 += (double)X[(r0 + i) * ldx + j];
-#pragma unroll
-            for (int da = 0; da < 2; da++) {
-                int a = (c0 >> 1) + da;
-                if (a >= nact) continue;
-                float av = (m0 && da == 0) ? (float)s0 : acc[i][2 * da];
-                S[(size_t)a * nr + ir] = make_float4(av, 0.f, acc[i][2 * da + 1], 0.f);
+    const int r = threadIdx.x >> 5, lane = threadIdx.x & 31, ir = ir0 + r;
+    if (ir >= nr) return;
+    const float* x = X + r * ldx;
+    for (int c0 = 0; c0 < 2 * nact; c0 += 64) {
+        // two columns per lane per pass: cosine and sine of one harmonic
+        const int a = (c0 >> 1) + lane;
+        float sc = 0.f, ss = 0.f;
+        if (a < nact) {
+            for (int j = 0; j < na; j++) {
+                const float xv = x[j];
+                const float2 t = *reinterpret_cast<const float2*>(T + (size_t)j * ncp + 2 * a);
+                sc += xv * t.x;
+                ss += xv * t.y;
             }
         }
-    });
+        if (a < nact && !(a == 0 && g.act[0] == 0)) S[(size_t)a * nr + ir] = make_float4(sc, 0.f, ss, 0.f);
+    }
+    if (g.act[0] == 0) {
+        double s0 = 0.0;
+        for (int j = lane; j < na; j += 32) s0 += (double)x[j];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+        if (lane == 0) S[ir] = make_float4((float)s0, 0.f, 0.f, 0.f);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -370,8 +364,10 @@ __global__ void __launch_bounds__(256) k_conv(DevGeo g, int nact, int tmask,
     for (int i = threadIdx.x; i < nr; i += blockDim.x)
         Sin[i] = (i >= js && i <= ks) ? S[((size_t)a * nkz + k) * nr + i] : make_float4(0, 0, 0, 0);
     __syncthreads();
-    for (int t = 0; t < 4; t++) {
-        if (!((tmask >> t) & 1)) continue;
+    {
+        // one field type per CTA (blockIdx.z)
+        const int t = blockIdx.z;
+        if (!((tmask >> t) & 1)) return;
         bool valid = true;
         if (t == 1) valid = (m >= 1) && (m <= min(ng, mmax - 1) - 1);
         if (t == 2) valid = (g.ndim == 3) && (k >= 1) && (k <= ngz - 1);
@@ -380,7 +376,7 @@ __global__ void __launch_bounds__(256) k_conv(DevGeo g, int nact, int tmask,
         float4* out = O + ((size_t)t * nr * nkz + k) * nact + a;
         if (!valid) {
             for (int i = threadIdx.x; i < nr; i += blockDim.x) out[i * ost] = make_float4(0, 0, 0, 0);
-            continue;
+            return;
         }
         const float* Gt = G + ((((size_t)t * ng + m) * nkz + k) * nr) * (size_t)nr;
         for (int ib = 0; ib < nr; ib += 128) {
@@ -483,10 +479,16 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* fr
                                             c->specS);
         GX_LAUNCHED(c);
     } else {
-        size_t sm = sizeof(float) * ((size_t)RB2 * (g.na + 1) + (size_t)g.na * ncp);
+        const size_t ntaz = (size_t)g.na * ncp;
+        if (!c->fwdtab) {
+            GX_CUDA(c, cudaMalloc((void**)&c->fwdtab, sizeof(float) * ntaz));
+            k_fwdtab<<<(unsigned)((ntaz + 255) / 256), 256, 0, c->stream>>>(g, nact, ncp, c->fwdtab, nullptr);
+            GX_LAUNCHED(c);
+        }
+        size_t sm = sizeof(float) * ((size_t)RB2 * (g.na + 1) + ntaz);
         GX_CUDA(c, cudaFuncSetAttribute(k_fwd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         int nb = (g.nr + RB2 - 1) / RB2;
-        k_fwd2<<<nb, 256, sm, c->stream>>>(g, nact, ncp, c->mass, c->specS);
+        k_fwd2<<<nb, 32 * RB2, sm, c->stream>>>(g, nact, ncp, c->mass, c->fwdtab, c->specS);
         GX_LAUNCHED(c);
     }
     rc = gx_comm_reduce_spectrum(c);
@@ -502,7 +504,7 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* fr
         }
     } else {
         size_t sm = sizeof(float4) * (size_t)g.nr * 9;
-        dim3 grid(nact, g.nkz);
+        dim3 grid(nact, g.nkz, 4);
         bool vec = (g.nr % 4) == 0;
         if (vec) {
             GX_CUDA(c, cudaFuncSetAttribute(k_conv<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
