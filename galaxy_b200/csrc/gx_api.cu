@@ -449,9 +449,17 @@ static int alloc_particles(GxCtx* c, int64_t n) {
     DALLOC(c, c->items, (size_t)3 * c->maxitems);
     int nq = c->g.quad ? 9 : (c->g.ndim == 3) ? 4 : 2;
     DALLOC(c, c->stage, (size_t)c->maxitems * nq * c->g.na);
-    // fused-pass work items: every row's segment in chunks of BK_ITEM, and
-    // the overflow area's
-    c->bk_maxitems = (int64_t)c->g.nrow + 1 + 2 * (n / BK_ITEM + 2);
+    // fused-pass work items: every row's segment in chunks of bk_item
+    // particles, and the overflow area's.  bk_item: at most BK_ITEM, at
+    // least half a deposit window of particles (the bins each item
+    // flushes), and otherwise small enough that a B200's resident CTAs
+    // (148 SMs x 5) get two items each when the particles are few
+    {
+        const int64_t wrows = (c->g.ndim == 3) ? 16 : 4;
+        const int64_t wmin = std::min<int64_t>(BK_ITEM, std::max<int64_t>(256, wrows * c->g.na / 2));
+        c->bk_item = (int)std::min<int64_t>(BK_ITEM, std::max<int64_t>(wmin, n / (2 * 148 * 5)));
+    }
+    c->bk_maxitems = (int64_t)c->g.nrow + 1 + 2 * (n / c->bk_item + 2);
     DALLOC(c, c->bk_items, (size_t)c->bk_maxitems);
     // the bucketed store: row segments with 1/8 + 16 slots of slack per row,
     // then an overflow area that can take every particle

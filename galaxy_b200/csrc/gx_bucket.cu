@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_bk_plan(
     const int32_t* __restrict__ base_o, const int32_t* __restrict__ ovf_o, int64_t ovf_base,
     int4* __restrict__ items, int32_t* __restrict__ ctl,
     const int32_t* __restrict__ want, int32_t* __restrict__ cap_n, int32_t* __restrict__ base_n,
-    int32_t* __restrict__ fill_n, int32_t* __restrict__ ovf_n) {
+    int32_t* __restrict__ fill_n, int32_t* __restrict__ ovf_n, int item) {
     int carry_cap = 0, carry_it = 0;
     for (int c0 = 0; c0 < nrow1; c0 += PLAN_THREADS * PLAN_ROWS) {
         const int r0 = c0 + threadIdx.x * PLAN_ROWS;
@@ -164,7 +164,7 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_bk_plan(
             val[k] = nit[k] = 0;
             if (fill_o) {
                 val[k] = min(fv[k], cv[k]);
-                nit[k] = (val[k] + BK_ITEM - 1) / BK_ITEM;
+                nit[k] = (val[k] + item - 1) / item;
             }
             scap += capv[k];
             snit += nit[k];
@@ -187,8 +187,7 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_bk_plan(
             for (int k = 0; k < PLAN_ROWS; k++) {
                 const int ring = (r0 + k) / ngz;
                 for (int q = 0; q < nit[k]; q++)
-                    items[eit + q] = make_int4(r0 + k, bv[k] + q * BK_ITEM,
-                                               bv[k] + min((q + 1) * BK_ITEM, val[k]), ring);
+                    items[eit + q] = make_int4(r0 + k, bv[k] + q * item, bv[k] + min((q + 1) * item, val[k]), ring);
                 eit += nit[k];
             }
         }
@@ -198,8 +197,8 @@ __global__ void __launch_bounds__(PLAN_THREADS) k_bk_plan(
     if (fill_o && threadIdx.x == 0) {
         const int ov = *ovf_o;
         int it = carry_it;
-        for (int q = 0; q * BK_ITEM < ov; q++, it++)
-            items[it] = make_int4(-1, (int)ovf_base + q * BK_ITEM, (int)ovf_base + min((q + 1) * BK_ITEM, ov), 0);
+        for (int q = 0; q * item < ov; q++, it++)
+            items[it] = make_int4(-1, (int)ovf_base + q * item, (int)ovf_base + min((q + 1) * item, ov), 0);
         ctl[0] = it;
         ctl[1] = 0;
     }
@@ -691,7 +690,7 @@ static int bk_plan(GxCtx* c, int out, bool with_items, cudaStream_t st) {
         g.nrow + 1, g.ngz, with_items ? c->bk_fill[out] : nullptr, c->bk_cap[out], c->bk_base[out],
         c->bk_ctl + 4 * out, c->bk_main, c->bk_items, c->bk_ctl + 8,
         with_items ? c->bk_fill[out] : c->bk_cnt, c->bk_cap[nxt], c->bk_base[nxt], c->bk_fill[nxt],
-        c->bk_ctl + 4 * nxt);
+        c->bk_ctl + 4 * nxt, c->bk_item);
     GX_LAUNCHED(c);
     return GX_OK;
 }

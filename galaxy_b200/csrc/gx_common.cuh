@@ -179,6 +179,7 @@ struct GxCtx {
                                              // [13..14] ring range (of the pass's new cells)
     int4* bk_items = nullptr;                // work items of pbuf[cur]: row (-1: overflow), first, end slot
     int64_t bk_maxitems = 0;
+    int bk_item = BK_ITEM;                   // particles per work item of the fused pass
     int32_t* bk_cnt = nullptr;               // [nrow + 1] row counts of the dense store (bucketing)
     unsigned long long* macc = nullptr;      // [mesh] fixed-point mass (2^-20 of a particle), zero between steps
     int32_t* zr_d = nullptr;                 // [2] first, last plane holding the fused pass's mass
