@@ -840,8 +840,75 @@ int gx_fast_masset(GxCtx* c) {
     return GX_OK;
 }
 
-int gx_fast_step(GxCtx* c, int nsteps, int phys) {
+// one fused step: the solve of the current mass (only the planes that hold
+// it once they are known), the pass, its plan on the side stream, the mass
+static int fast_one_step(GxCtx* c, bool lpot) {
     const DevGeo& g = c->g;
+    // once the mass is a fused pass's, the solve knows the planes that
+    // hold it, and the field is needed only where the particles are
+    int rc = gx_mixed_findf(c, lpot ? 1 : 0, true, nullptr, (c->zr_valid && g.ndim == 3) ? c->zr_d : nullptr);
+    if (rc) return rc;
+    const int cur = c->bcur, nxt = cur ^ 1;
+    rc = bk_join(c);
+    if (rc) return rc;
+    rc = gx_phase_mark(c, PH_PUSH);
+    if (rc) return rc;
+    if (g.ndim == 3) rc = g.comp ? bk_launch_push<3, true>(c, cur, nxt) : bk_launch_push<3, false>(c, cur, nxt);
+    else rc = g.comp ? bk_launch_push<2, true>(c, cur, nxt) : bk_launch_push<2, false>(c, cur, nxt);
+    if (rc) return rc;
+    if (c->prof) {
+        // profile mode: the plan in line, so that it has a phase time
+        rc = gx_phase_mark(c, PH_SORT);
+        if (rc) return rc;
+        rc = bk_plan(c, nxt, true, c->stream);
+        if (rc) return rc;
+    } else {
+        // the plan needs only the push: it runs on the side stream while
+        // the next field solve runs, and the next push waits for it
+        GX_CUDA(c, cudaEventRecord(c->bk_ev[0], c->stream));
+        GX_CUDA(c, cudaStreamWaitEvent(c->bk_side, c->bk_ev[0], 0));
+        rc = bk_plan(c, nxt, true, c->bk_side);
+        if (rc) return rc;
+        GX_CUDA(c, cudaEventRecord(c->bk_ev[1], c->bk_side));
+        c->bk_pending = true;
+    }
+    rc = gx_phase_mark(c, PH_COMBINE);
+    if (rc) return rc;
+    k_mass_convert<<<(unsigned)((g.mesh / 2 + 255) / 256), 256, 0, c->stream>>>(
+        c->macc, c->mass, g.mesh, g.pmass, c->bk_ctl + 13, c->jrk_d, g.nr, c->bk_ctl + 10, c->zr_d, g.ngz);
+    GX_LAUNCHED(c);
+    c->zr_valid = true;
+    c->bcur = nxt;
+    return GX_OK;
+}
+
+// two fused steps from the current store captured into a CUDA graph (the
+// plans forked to the side stream and joined inside it): the graph, and the
+// kernels of one replay in *per; null when the capture is refused, and the
+// steps then run as plain launches.  Capturing runs nothing: the host state
+// the two steps would change is put back.
+static cudaGraphExec_t fast_capture(GxCtx* c, int64_t* per) {
+    const int b = c->bcur;
+    if (bk_join(c) != GX_OK) return nullptr;
+    const int64_t l0 = c->launches;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool ok = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+    if (ok) ok = fast_one_step(c, false) == GX_OK && fast_one_step(c, false) == GX_OK && bk_join(c) == GX_OK;
+    const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
+    ok = ok && ec == cudaSuccess && graph;
+    if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    *per = c->launches - l0;
+    c->bcur = b;
+    c->bk_pending = false;
+    c->launches = l0;
+    c->err.clear();
+    return ok ? exec : nullptr;
+}
+
+int gx_fast_step(GxCtx* c, int nsteps, int phys) {
     int rc;
     if (!c->bk_side) {
         int lo = 0, hi = 0;
@@ -854,45 +921,39 @@ int gx_fast_step(GxCtx* c, int nsteps, int phys) {
         rc = gx_bucketize(c);
         if (rc) return rc;
     }
-    for (int s = 0; s < nsteps; s++) {
+    // 2D contexts (small grids: their steps take tens of microseconds, so the
+    // gaps between launches count) replay pairs of steps from a CUDA graph,
+    // captured in this call once the state is steady (the mass a fused
+    // pass's, every buffer allocated) and released at its end
+    const bool graphs = c->g.ndim == 2 && !c->prof && c->nranks <= 1;
+    cudaGraphExec_t exec = nullptr;
+    int64_t per = 0;
+    bool tried = false;
+    int s = 0;
+    while (s < nsteps) {
         const bool last = (s == nsteps - 1);
-        // once the mass is a fused pass's, the solve knows the planes that
-        // hold it, and the field is needed only where the particles are
-        rc = gx_mixed_findf(c, phys && last, true, nullptr, (c->zr_valid && g.ndim == 3) ? c->zr_d : nullptr);
-        if (rc) return rc;
-        const int cur = c->bcur, nxt = cur ^ 1;
-        rc = bk_join(c);
-        if (rc) return rc;
-        rc = gx_phase_mark(c, PH_PUSH);
-        if (rc) return rc;
-        if (g.ndim == 3) rc = g.comp ? bk_launch_push<3, true>(c, cur, nxt) : bk_launch_push<3, false>(c, cur, nxt);
-        else rc = g.comp ? bk_launch_push<2, true>(c, cur, nxt) : bk_launch_push<2, false>(c, cur, nxt);
-        if (rc) return rc;
-        if (c->prof) {
-            // profile mode: the plan in line, so that it has a phase time
-            rc = gx_phase_mark(c, PH_SORT);
-            if (rc) return rc;
-            rc = bk_plan(c, nxt, true, c->stream);
-            if (rc) return rc;
-        } else {
-            // the plan needs only the push: it runs on the side stream while
-            // the next field solve runs, and the next push waits for it
-            GX_CUDA(c, cudaEventRecord(c->bk_ev[0], c->stream));
-            GX_CUDA(c, cudaStreamWaitEvent(c->bk_side, c->bk_ev[0], 0));
-            rc = bk_plan(c, nxt, true, c->bk_side);
-            if (rc) return rc;
-            GX_CUDA(c, cudaEventRecord(c->bk_ev[1], c->bk_side));
-            c->bk_pending = true;
+        const int pairs = (nsteps - s - 1) / 2;  // the last step runs as plain launches (phys)
+        if (graphs && c->zr_valid && pairs >= 4 && !tried) {
+            tried = true;
+            exec = fast_capture(c, &per);
         }
-        rc = gx_phase_mark(c, PH_COMBINE);
-        if (rc) return rc;
-        k_mass_convert<<<(unsigned)((g.mesh / 2 + 255) / 256), 256, 0, c->stream>>>(
-            c->macc, c->mass, g.mesh, g.pmass, c->bk_ctl + 13, c->jrk_d, g.nr, c->bk_ctl + 10, c->zr_d,
-            g.ngz);
-        GX_LAUNCHED(c);
-        c->zr_valid = true;
-        c->bcur = nxt;
+        if (exec && pairs > 0) {
+            rc = bk_join(c);
+            if (rc) break;
+            for (int p = 0; p < pairs && !rc; p++) {
+                if (cudaGraphLaunch(exec, c->stream) != cudaSuccess) rc = (c->err = "cudaGraphLaunch failed", GX_ERR_CUDA);
+                c->launches += per;
+            }
+            if (rc) break;
+            s += 2 * pairs;
+            continue;
+        }
+        rc = fast_one_step(c, phys && last);
+        if (rc) break;
+        s++;
     }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (rc) return rc;
     rc = bk_join(c);
     if (rc) return rc;
     rc = gx_phase_end(c);

@@ -502,7 +502,8 @@ __global__ void __launch_bounds__(SYNAZ_THREADS) k_synaz(DevGeo g, int nact, int
                                               const float* __restrict__ R, SynTab tb,
                                               float4* __restrict__ F, float* __restrict__ polar,
                                               const int32_t* __restrict__ frk,
-                                              const int32_t* __restrict__ zr) {
+                                              const int32_t* __restrict__ zr,
+                                              const float4* __restrict__ O2) {
     extern __shared__ __align__(16) float sm[];
     const int ir = blockIdx.x, zb = blockIdx.y * SYN_ZB;
     if (frk && (ir + 1 < frk[0] || ir + 1 > frk[1])) return;  // rings no moving particle reads
@@ -548,8 +549,19 @@ __global__ void __launch_bounds__(SYNAZ_THREADS) k_synaz(DevGeo g, int nact, int
             const int t = i / (SYN_ZB * ncp), rem = i - t * SYN_ZB * ncp;
             const int z = rem / ncp, c = rem - z * ncp;
             v[u] = 0.f;
-            if (i < 4 * SYN_ZB * ncp && ((tmask >> t) & 1) && z < nz)
-                v[u] = __ldg(R + (((size_t)t * nr + ir) * ngz + zb0 + z) * ncp + c);
+            if (i < 4 * SYN_ZB * ncp && ((tmask >> t) & 1) && z < nz) {
+                if (O2) {
+                    // 2D: the ring's contracted spectrum itself (no vertical
+                    // part): column 2a the cosine term, 2a + 1 the sine term
+                    const int a = c >> 1;
+                    if (a < nact) {
+                        const float4 o = __ldg(O2 + ((size_t)t * nr + ir) * nact + a);
+                        v[u] = (c & 1) ? o.z : o.x;
+                    }
+                } else {
+                    v[u] = __ldg(R + (((size_t)t * nr + ir) * ngz + zb0 + z) * ncp + c);
+                }
+            }
         }
 #pragma unroll
         for (int u = 0; u < 8; u++) {
@@ -638,7 +650,7 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk, const in
     const float* b = c->syntab;
     SynTab tb{b, b + nWe, b + 2 * nWe, b + 2 * nWe + nWo, b + 2 * nWe + 2 * nWo,
               b + 2 * nWe + 2 * nWo + nT, b + 2 * nWe + 2 * nWo + 2 * nT, Z0, KE, KO, njp};
-    {
+    if (g.ndim == 3) {
         // the tables, three bank pads of at most 31 floats, the spectrum
         if (gx_synz_tc_ok(g, nact, ncp)) {
             int sms = 148;
@@ -659,8 +671,10 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk, const in
         const size_t sm = sizeof(float) * (2 * nT + 2 * (size_t)njp + (size_t)4 * SYN_ZB * ncp);
         GX_CUDA(c, cudaFuncSetAttribute(k_synaz, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
         dim3 grid(g.nr, (g.ngz + SYN_ZB - 1) / SYN_ZB);
+        // 2D has no vertical part: the azimuthal synthesis reads the contracted spectrum
         k_synaz<<<grid, SYNAZ_THREADS, sm, c->stream>>>(g, nact, ncp, tmask, c->synR, tb, c->field, polar, frk,
-                                                        g.ndim == 3 ? zr : nullptr);
+                                                        g.ndim == 3 ? zr : nullptr,
+                                                        g.ndim == 3 ? nullptr : c->specO);
         GX_LAUNCHED(c);
     }
     return GX_OK;

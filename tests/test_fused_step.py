@@ -107,3 +107,24 @@ def test_fused_step_empty_context():
         gal.step(2)
         assert gal.unload().shape == (0, 6)
         assert not gal.grid(GX_GRID_MASS).any()
+
+
+def test_fused_2d_graph_replay_is_bitwise_the_sorted_deposit():
+    """A 2D run long enough that the fused path replays pairs of steps from
+    a CUDA graph (captured once the mass is a fused pass's): the same
+    particles and mass, bit for bit, as the sorted deposit's plain
+    launches, over two calls."""
+    cfg, rec, pm, _ = case("2d")
+    out = []
+    for flags in (0, GX_FLAG_SORTED_DEPOSIT):
+        cfg.pmass = pm
+        cfg.flags = flags
+        with Galaxy(cfg) as gal:
+            gal.greenm()
+            gal.loadup(rec)
+            gal.masset()
+            gal.step(21)
+            gal.step(14, phys=True)
+            out.append((gal.unload(), gal.grid(GX_GRID_MASS)))
+    for x, y in zip(out[0], out[1]):
+        assert (x.view(np.uint32) == y.view(np.uint32)).all()
