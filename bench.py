@@ -382,6 +382,28 @@ def run_e2e(args, w, rec, pm, cfg_dev):
             "pinned": pinned, "finite": ok, "what": "gx_loadup + gx_masset + gx_step(K) + gx_unload, wall clock, best of 2"}
 
 
+def run_small2d(steps=200):
+    """The 2D CPU-runnable configuration (64 x 128 log rings x spokes, m =
+    0..8, 100k particles, dt = 0.025) stepped on the GPU: the size of the
+    reference's own p2d examples, where a step takes tens of microseconds."""
+    from galaxy_b200 import Galaxy, GX_PREC_MIXED
+    w = WORKLOADS["polar2d-64x128-100k"]
+    rec, pm = make_ic(w, w["n"], seed=12345)
+    cfg = make_cfg(w, GX_PREC_MIXED)
+    cfg.pmass = pm
+    with Galaxy(cfg) as gal:
+        gal.greenm()
+        gal.loadup(rec)
+        gal.masset()
+        gal.findf(True)
+        gal.tmcent(True)
+        gal.step(10)
+        gal.step(steps)
+        ms = gal.last_step_ms() / steps
+    return {"workload": "polar2d-64x128-100k", "steps": steps, "ms_per_step": round(ms, 4),
+            "particle_steps_per_s": w["n"] / (ms * 1e-3)}
+
+
 def run_sfp(n=20_000_000, reps=5):
     """The SFP coefficient sum of the 2D Abel-Jacobi configuration: 20M
     particles of an exponential disc (scale 1, truncated at r = 6), k = 7,
@@ -660,6 +682,7 @@ def main():
         comm.barrier()
     if rank == 0:
         e2e = run_e2e(args, w, rec, pm, cfg.device) if world == 1 else None
+        small2d = run_small2d() if world == 1 else None
         sfp = run_sfp() if (world == 1 and not args.no_sfp) else None
         ens = run_ensemble() if (world == 1 and not args.no_ens) else None
         adj = run_adjoint() if (world == 1 and not args.no_adj) else None
@@ -680,7 +703,7 @@ def main():
                 "pot_rel_err": out.get("pot_rel_err"),
                 "accuracy_vs_oracle": out.get("vs_oracle"),
                 "compensated_step": out.get("compensated_step"),
-                "step_roofline": out["step_roofline"], "phases": out["phases"], "sfp": sfp,
+                "step_roofline": out["step_roofline"], "phases": out["phases"], "small2d": small2d, "sfp": sfp,
                 "ensemble": ens, "adjoint": adj}
         print(json.dumps(line))
     if comm is not None:
