@@ -237,15 +237,17 @@ __device__ __forceinline__ int64_t bk_slot(bool act, uint32_t rk, const int32_t*
     return dst;
 }
 
-// A particle of the bucketed store is one record of R float4 words (R even:
-// 32 or 64 bytes), record s at Q[R s]: its NP floats (x, y[, z], vx, vy[,
-// vz][, the compensated low parts]) then its load index as float bits,
-// zero-padded.  A record moves with one or two 32-byte accesses
-// (ld/st .v8.f32): a warp's loads of consecutive records are contiguous,
-// and each store writes whole 32-byte sectors.
+// A particle of the bucketed store is one record: its NP floats (x, y[, z],
+// vx, vy[, vz][, the compensated low parts]) then its load index as float
+// bits, zero-padded to R float4 words.  The first two words of record s
+// are bytes 32 s .. 32 s + 31 (moved with one 32-byte ld/st.v8 access, so a
+// warp's loads of consecutive records are contiguous and each store writes
+// a whole sector); a third word (the compensated 3D records, R = 3) sits in
+// a plane of its own after them, at word 2 bcap + s.
 template <int NP>
 struct Rec {
-    static constexpr int R = ((NP + 1 + 7) / 8) * 2;
+    static constexpr int R = (NP + 1 + 3) / 4;
+    static_assert(R >= 2 && R <= 3, "records of 5 to 12 floats");
 };
 
 __device__ __forceinline__ void ld8f(const float4* p, float* w) {
@@ -264,8 +266,14 @@ __device__ __forceinline__ void rec_load(const float4* __restrict__ Q, int64_t b
                                          int32_t& o) {
     constexpr int R = Rec<NP>::R;
     float w[4 * R];
-#pragma unroll
-    for (int q = 0; q < R; q += 2) ld8f(Q + R * s + q, w + 4 * q);
+    ld8f(Q + 2 * s, w);
+    if (R == 3) {
+        const float4 v = __ldg(Q + 2 * bcap + s);
+        w[8] = v.x;
+        w[9] = v.y;
+        w[10] = v.z;
+        w[11] = v.w;
+    }
 #pragma unroll
     for (int k = 0; k < NP; k++) P[k] = w[k];
     o = __float_as_int(w[NP]);
@@ -279,8 +287,8 @@ __device__ __forceinline__ void rec_store(float4* __restrict__ Q, int64_t bcap, 
 #pragma unroll
     for (int k = 0; k < 4 * R; k++) w[k] = (k < NP) ? P[k] : 0.f;
     w[NP] = __int_as_float(o);
-#pragma unroll
-    for (int q = 0; q < R; q += 2) st8f(Q + R * s + q, w + 4 * q);
+    st8f(Q + 2 * s, w);
+    if (R == 3) Q[2 * bcap + s] = make_float4(w[8], w[9], w[10], w[11]);
 }
 
 // The fused particle pass of one step.  Persistent CTAs take work items from
@@ -636,7 +644,7 @@ __global__ void k_bk_unload(const float4* __restrict__ Qin, int64_t bcap, float*
 }
 
 // float4 words of one record of the bucketed store
-int gx_bucket_words(const GxCtx* c) { return (bk_nplanes(c) + 1 + 7) / 8 * 2; }
+int gx_bucket_words(const GxCtx* c) { return (bk_nplanes(c) + 1 + 3) / 4; }
 
 static inline size_t bk_npad(const GxCtx* c);
 static int bk_plan(GxCtx* c, int out, bool with_items, cudaStream_t st);
