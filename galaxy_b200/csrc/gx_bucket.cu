@@ -901,8 +901,17 @@ static cudaGraphExec_t fast_capture(GxCtx* c, int64_t* per) {
     const int64_t l0 = c->launches;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    bool ok = cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
-    if (ok) ok = fast_one_step(c, false) == GX_OK && fast_one_step(c, false) == GX_OK && bk_join(c) == GX_OK;
+    // a stream the caller is capturing already is left alone
+    cudaStreamCaptureStatus st = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(c->stream, &st) != cudaSuccess || st != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    bool ok = fast_one_step(c, false) == GX_OK && fast_one_step(c, false) == GX_OK && bk_join(c) == GX_OK;
     const cudaError_t ec = cudaStreamEndCapture(c->stream, &graph);
     ok = ok && ec == cudaSuccess && graph;
     if (ok) ok = cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
