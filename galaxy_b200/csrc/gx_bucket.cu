@@ -568,6 +568,64 @@ __global__ void k_bk_rows(DevGeo g, const float* __restrict__ P, int64_t cap, in
     if (act && (peers & lanemask_lt()) == 0) atomicAdd(cnt + rk, (int)__popc(peers));
 }
 
+// The same two steps with the counts gathered per CTA first (grids whose row
+// table fits in shared memory): a CTA takes a run of BK_RUN particles, counts
+// their rows in shared memory, and touches each global counter once per
+// nonzero row instead of once per warp group -- a disc's central rows get
+// tens of thousands of particles, whose single-address atomics otherwise
+// serialise.  The scatter reserves each row's slots for the CTA with one
+// atomic on the row's fill counter and hands them out from shared memory.
+#define BK_RUN 32768
+template <int ND>
+__global__ void __launch_bounds__(256) k_bk_rows_cta(DevGeo g, const float* __restrict__ P, int64_t cap,
+                                                     int64_t n, int32_t* __restrict__ rows,
+                                                     int32_t* __restrict__ cnt) {
+    extern __shared__ int32_t hist[];  // [nrow + 1]
+    const int nr1 = g.nrow + 1;
+    for (int r = threadIdx.x; r < nr1; r += blockDim.x) hist[r] = 0;
+    __syncthreads();
+    const int64_t i0 = (int64_t)blockIdx.x * BK_RUN, i1 = min(n, i0 + BK_RUN);
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const CellW c = gx_cell_t<true, ND>(g, P[i], P[cap + i], ND == 3 ? P[2 * cap + i] : 0.f, false);
+        const int rk = (c.key >= 0) ? c.row : g.nrow;
+        rows[i] = rk;
+        atomicAdd(hist + rk, 1);
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < nr1; r += blockDim.x)
+        if (hist[r]) atomicAdd(cnt + r, hist[r]);
+}
+
+template <int NP>
+__global__ void __launch_bounds__(256) k_bk_scatter_cta(const float* __restrict__ P, int64_t cap, int64_t n,
+                                                        const int32_t* __restrict__ oin, float4* __restrict__ Qout,
+                                                        int64_t bcap, const int32_t* __restrict__ rows, int nr1,
+                                                        const int32_t* __restrict__ cap_o,
+                                                        const int32_t* __restrict__ base_o,
+                                                        int32_t* __restrict__ fill_o, int32_t* __restrict__ ovf_o,
+                                                        int64_t ovf_base) {
+    extern __shared__ int32_t slot[];  // [nrow + 1]: this CTA's count, then its next slot
+    for (int r = threadIdx.x; r < nr1; r += blockDim.x) slot[r] = 0;
+    __syncthreads();
+    const int64_t i0 = (int64_t)blockIdx.x * BK_RUN, i1 = min(n, i0 + BK_RUN);
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) atomicAdd(slot + rows[i], 1);
+    __syncthreads();
+    for (int r = threadIdx.x; r < nr1; r += blockDim.x)
+        if (slot[r]) slot[r] = atomicAdd(fill_o + r, slot[r]);
+    __syncthreads();
+    for (int64_t i = i0 + threadIdx.x; i < i1; i += blockDim.x) {
+        const int rk = rows[i];
+        const int sl = atomicAdd(slot + rk, 1);
+        int64_t dst;
+        if (sl < __ldg(cap_o + rk)) dst = (int64_t)__ldg(base_o + rk) + sl;
+        else dst = ovf_base + atomicAdd(ovf_o, 1);  // past the segment (rare): the overflow area
+        float w[NP];
+#pragma unroll
+        for (int k = 0; k < NP; k++) w[k] = P[(size_t)k * cap + i];
+        rec_store<NP>(Qout, bcap, dst, w, oin[i]);
+    }
+}
+
 template <int NP>
 __global__ void k_bk_scatter(const float* __restrict__ P, int64_t cap, int64_t n, const int32_t* __restrict__ oin,
                              float4* __restrict__ Qout, int64_t bcap, const int32_t* __restrict__ rows,
@@ -704,6 +762,17 @@ static int bk_plan(GxCtx* c, int out, bool with_items, cudaStream_t st) {
 }
 
 template <int NP>
+static void bk_scatter_cta_launch(GxCtx* c, int b) {
+    const int nr1 = c->g.nrow + 1;
+    const unsigned nruns = (unsigned)((c->n + BK_RUN - 1) / BK_RUN);
+    cudaFuncSetAttribute(k_bk_scatter_cta<NP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)(sizeof(int32_t) * nr1));
+    k_bk_scatter_cta<NP><<<nruns, 256, sizeof(int32_t) * nr1, c->stream>>>(
+        c->pbuf[c->cur], c->cap, c->n, c->origin, c->bq[b], c->bcap, c->pkey[0], nr1, c->bk_cap[b], c->bk_base[b],
+        c->bk_fill[b], c->bk_ctl + 4 * b, c->bk_main);
+}
+
+template <int NP>
 static void bk_scatter_launch(GxCtx* c, unsigned nb, int b) {
     k_bk_scatter<NP><<<nb, 256, 0, c->stream>>>(c->pbuf[c->cur], c->cap, c->n, c->origin, c->bq[b], c->bcap,
                                                 c->pkey[0], c->bk_cap[b], c->bk_base[b], c->bk_fill[b],
@@ -725,9 +794,19 @@ static int gx_bucketize(GxCtx* c) {
     const int b = c->bcur ^ 1;
     const unsigned nb = (unsigned)((std::max<int64_t>(n, 1) + 255) / 256);
     GX_CUDA(c, cudaMemsetAsync(c->bk_cnt, 0, sizeof(int32_t) * bk_npad(c), c->stream));
+    // the row table in shared memory when it fits in 96 KB (two CTAs per SM)
+    const size_t hbytes = sizeof(int32_t) * ((size_t)g.nrow + 1);
+    const bool cta = hbytes <= 96 * 1024;
     if (n > 0) {
-        auto kr = (g.ndim == 3) ? k_bk_rows<3> : k_bk_rows<2>;
-        kr<<<nb, 256, 0, c->stream>>>(g, c->pbuf[c->cur], c->cap, n, c->pkey[0], c->bk_cnt);
+        if (cta) {
+            auto kr = (g.ndim == 3) ? k_bk_rows_cta<3> : k_bk_rows_cta<2>;
+            cudaFuncSetAttribute(kr, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)hbytes);
+            kr<<<(unsigned)((n + BK_RUN - 1) / BK_RUN), 256, hbytes, c->stream>>>(g, c->pbuf[c->cur], c->cap, n,
+                                                                                c->pkey[0], c->bk_cnt);
+        } else {
+            auto kr = (g.ndim == 3) ? k_bk_rows<3> : k_bk_rows<2>;
+            kr<<<nb, 256, 0, c->stream>>>(g, c->pbuf[c->cur], c->cap, n, c->pkey[0], c->bk_cnt);
+        }
         GX_LAUNCHED(c);
     }
     // segments of bq[b] from the exact counts (with_items = false plans the
@@ -736,9 +815,9 @@ static int gx_bucketize(GxCtx* c) {
     if (rc) return rc;
     if (n > 0) {
         switch (bk_nplanes(c)) {
-            case 4: bk_scatter_launch<4>(c, nb, b); break;
-            case 6: bk_scatter_launch<6>(c, nb, b); break;
-            default: bk_scatter_launch<9>(c, nb, b); break;
+            case 4: cta ? bk_scatter_cta_launch<4>(c, b) : bk_scatter_launch<4>(c, nb, b); break;
+            case 6: cta ? bk_scatter_cta_launch<6>(c, b) : bk_scatter_launch<6>(c, nb, b); break;
+            default: cta ? bk_scatter_cta_launch<9>(c, b) : bk_scatter_launch<9>(c, nb, b); break;
         }
         GX_LAUNCHED(c);
     }
