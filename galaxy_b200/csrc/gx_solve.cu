@@ -18,6 +18,7 @@
 // b_m = -sum x sin; backward x_j = a_0 + (-1)^j a_N + 2 sum (a cos - b sin).
 #include <algorithm>
 
+#include "gx_bulk.cuh"
 #include "gx_common.cuh"
 
 
@@ -99,10 +100,54 @@ __device__ __forceinline__ void sgemm44_sk(int M, int N, int K, const float* A, 
     }
 }
 
+// sgemm44_sk with A stored transposed: A(r, k) = At[k * ldat + r] (ldat % 4
+// == 0, rows up to ru4(M) addressable), so each k takes one float4 of A.
+// The products and their order are those of sgemm44_sk on the same matrix.
+template <int KS, class Epi>
+__device__ __forceinline__ void sgemm44_skT(int M, int N, int K, const float* At, int ldat,
+                                            const float* B, int ldb, Epi epi) {
+    const int tilesN = (N + 3) >> 2, tilesM = (M + 3) >> 2, nt = tilesM * tilesN;
+    const int per = blockDim.x / KS, ks = threadIdx.x % KS;
+    for (int t0 = 0; t0 < nt; t0 += per) {
+        const int t = t0 + threadIdx.x / KS;
+        const bool act = t < nt;
+        const int tm = act ? t / tilesN : 0, tn = act ? t - tm * tilesN : 0;
+        const int r0 = tm * 4, c0 = tn * 4;
+        float acc[4][4];
+#pragma unroll
+        for (int i = 0; i < 4; i++)
+#pragma unroll
+            for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
+        if (act) {
+            const float* ap = At + r0;
+            const float* bp = B + c0;
+#pragma unroll 4
+            for (int k = ks; k < K; k += KS) {
+                const float4 b = *reinterpret_cast<const float4*>(bp + (size_t)k * ldb);
+                const float4 a = *reinterpret_cast<const float4*>(ap + (size_t)k * ldat);
+                acc[0][0] += a.x * b.x; acc[0][1] += a.x * b.y; acc[0][2] += a.x * b.z; acc[0][3] += a.x * b.w;
+                acc[1][0] += a.y * b.x; acc[1][1] += a.y * b.y; acc[1][2] += a.y * b.z; acc[1][3] += a.y * b.w;
+                acc[2][0] += a.z * b.x; acc[2][1] += a.z * b.y; acc[2][2] += a.z * b.z; acc[2][3] += a.z * b.w;
+                acc[3][0] += a.w * b.x; acc[3][1] += a.w * b.y; acc[3][2] += a.w * b.z; acc[3][3] += a.w * b.w;
+            }
+        }
+#pragma unroll
+        for (int o = 1; o < KS; o <<= 1)
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) acc[i][j] += __shfl_xor_sync(0xffffffffu, acc[i][j], o);
+        if (act && ks == 0) epi(r0, c0, acc);
+    }
+}
+
 // forward twiddle tables, built once per context:
 //   Taz[j][2a] = cos(2 pi m_a j / na), Taz[j][2a+1] = -sin(...)   [na][ncp]
 //   Tz[2k][z] = cos(pi k z / ngz), Tz[2k+1][z] = -sin(...)       [ru4(2 nkz)][ngz]
-__global__ void k_fwdtab(DevGeo g, int nact, int ncp, float* __restrict__ Taz, float* __restrict__ Tz) {
+//   TzT[z][r] = Tz[r][z]                                         [ngz][ru4(2 nkz)]
+//   Tf[j][c] = Taz[j][c + cb], c < 2 nact - cb, else 0           [na][ncpf]
+__global__ void k_fwdtab(DevGeo g, int nact, int ncp, float* __restrict__ Taz, float* __restrict__ Tz,
+                         float* __restrict__ TzT, float* __restrict__ Tf, int cb, int ncpf) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int na = g.na, ngz = g.ngz, nkz = g.nkz;
     if (i < na * ncp) {
@@ -116,6 +161,7 @@ __global__ void k_fwdtab(DevGeo g, int nact, int ncp, float* __restrict__ Taz, f
             v = (c & 1) ? -sn : co;
         }
         Taz[i] = v;
+        if (Tf && c >= cb && c - cb < ncpf) Tf[(size_t)j * ncpf + (c - cb)] = v;
     }
     if (g.ndim == 3 && i < ru4(2 * nkz) * ngz) {
         const int r = i / ngz, z = i - r * ngz, k = r >> 1;
@@ -127,6 +173,7 @@ __global__ void k_fwdtab(DevGeo g, int nact, int ncp, float* __restrict__ Taz, f
             v = (r & 1) ? -sn : co;
         }
         Tz[i] = v;
+        TzT[(size_t)z * ru4(2 * nkz) + r] = v;
     }
 }
 
@@ -298,6 +345,255 @@ __global__ void __launch_bounds__(288) k_fwd_z(DevGeo g, int nact, int ncp,
     });
 }
 
+// 3D forward transform of one ring per CTA (p3manl.f:62-109): the
+// azimuthal and vertical DFTs of k_fwd_az and k_fwd_z in one launch, with
+// the ring's planes, the twiddle tables and the intermediate spectra in
+// shared memory.  One thread issues bulk copies of the azimuthal table and
+// of the ring's plane rows (only the planes summed: those holding mass, the
+// first rounded down to a multiple of 4) on one mbarrier; the azimuthal DFT
+// of up to FWR_XR rows at a time goes into C1 [plane][ncpf] in shared
+// memory; then the block of the transposed vertical table for those planes
+// replaces the first two and the vertical DFT writes S.
+//
+// Both DFTs are FP32 GEMMs on 4 x 4 register tiles whose operands are
+// float4 loads from shared memory.  A warp takes 4 row groups x 8 column
+// quads, so that each operand load is 4 or 8 distinct 16-byte words (one
+// shared-memory wavefront).  Thread rows are interleaved (rows tm + RG i) so
+// that the 4 row groups of a warp fall on different banks.  The azimuthal
+// sum over spokes is split over warps in contiguous ranges and the partial
+// tiles are added in warp order; the vertical sum runs over the planes in
+// order, so a sum over the planes holding mass equals the sum over all
+// planes bit for bit (the others add exact zeros).  The m = 0 column is not
+// in the GEMMs: its azimuthal sum is formed in FP64 (8 lanes per row), its
+// vertical DFT by 4 lanes per kz (planes by residue mod 4), and its sine
+// part is zero.
+#define FWR_THREADS 512
+#define FWR_WARPS (FWR_THREADS / 32)
+#define FWR_XR 48
+__global__ void __launch_bounds__(FWR_THREADS) k_fwd_ring(DevGeo g, int nact, int ncpf, int cb,
+                                                          const int32_t* __restrict__ jrk,
+                                                          const int32_t* __restrict__ zr,
+                                                          const float* __restrict__ mass,
+                                                          const float* __restrict__ Tf,
+                                                          const float* __restrict__ TzT, float4* __restrict__ S,
+                                                          int32_t* __restrict__ errword) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ uint64_t bar;
+    const int na = g.na, ngz = g.ngz, nkz = g.nkz, nr = g.nr;
+    const int ir = blockIdx.x;
+    if (ir < jrk[0] - 1 || ir > min(jrk[1], nr) - 1) {
+        // a ring without mass: zero spectrum (p3fndf.f:44-57)
+        for (int i = threadIdx.x; i < nact * nkz; i += blockDim.x)
+            S[(size_t)i * nr + ir] = make_float4(0.f, 0.f, 0.f, 0.f);
+        return;
+    }
+    const int zs = zr ? (zr[0] & ~3) : 0;
+    const int nzs = zr ? max(zr[1] - zs + 1, 0) : ngz;
+    const int ldx = na + 4, ldt = ru4(2 * nkz), tnN = ncpf >> 2;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, tml = lane >> 3, tnl = lane & 7;
+    float* C1 = sm;                            // [ru4(ngz)][ncpf]   harmonics m > 0 (or all)
+    float* C0 = C1 + (size_t)ru4(ngz) * ncpf;  // [ru4(ngz)]         m = 0 (FP64 sums)
+    float* P = C0 + ru4(ngz);                  // [FWR_WARPS][16][32] partial tiles
+    float* T = P + FWR_WARPS * 16 * 32;        // [na][ncpf]         (azimuthal part)
+    float* X = T + (size_t)na * ncpf;          // [FWR_XR][na + 4]   (azimuthal part)
+    float* Tt = T;                             // [nzs][ldt]         (vertical part)
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    uint32_t ph = 0;
+    for (int c0 = 0; c0 < nzs; c0 += FWR_XR) {
+        const int nx = min(FWR_XR, nzs - c0);
+        if (threadIdx.x == 0) {
+            const uint32_t rowb = (uint32_t)na * 4u, tabb = c0 == 0 ? (uint32_t)(na * ncpf) * 4u : 0u;
+            mbar_expect_tx(&bar, tabb + (uint32_t)nx * rowb);
+            if (tabb) bulk_g2s(T, Tf, tabb, &bar);
+            const float* src = mass + ((size_t)ir * ngz + zs + c0) * na;
+            for (int r = 0; r < nx; r++) bulk_g2s(X + (size_t)r * ldx, src + (size_t)r * na, rowb, &bar);
+        }
+        if (!__syncthreads_and(mbar_wait(&bar, ph))) {
+            if (threadIdx.x == 0) {
+                atomicExch(errword, 5);
+                mbar_wait(&bar, ph);  // the copies in flight land before the CTA leaves
+            }
+            return;
+        }
+        ph ^= 1;
+        if (cb) {
+            // m = 0: FP64 sum of each row, 8 lanes per row, na / 8 points each
+            const int r = threadIdx.x >> 3, q = threadIdx.x & 7;
+            double s = 0.0;
+            if (r < nx)
+                for (int j = q; j < na; j += 8) s += (double)X[r * ldx + j];
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+            if (r < nx && q == 0) C0[c0 + r] = (float)s;
+        }
+        // C1[c0 + r][c] = sum_j X[r][j] Tf[j][c]; thread rows tm + RG i
+        // the split of the spoke sum depends on the columns alone (not on the
+        // chunk's rows), so that every row's sum is formed the same way
+        // whichever planes are transformed
+        const int RG = (nx + 3) >> 2;
+        const int WTN = (tnN + 7) >> 3, WT = ((RG + 3) >> 2) * WTN;
+        const int KG = max(1, FWR_WARPS / (((FWR_XR / 4 + 3) >> 2) * WTN));
+        const int kc = (na + 4 * KG - 1) / (4 * KG) * 4;
+        for (int wi = warp; wi < WT * KG; wi += FWR_WARPS) {
+            const int wt = wi % WT, kg = wi / WT;
+            const int tm = (wt / WTN) * 4 + tml, tn = (wt % WTN) * 8 + tnl;
+            const int tmc = min(tm, RG - 1), tnc = min(tn, tnN - 1);
+            float acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[i][c] = 0.f;
+            const int j1 = min(na, (kg + 1) * kc);
+            const float* xa = X + (size_t)tmc * ldx;
+            const float* tb = T + 4 * tnc;
+#pragma unroll 1
+            for (int j = kg * kc; j < j1; j += 4) {
+                float4 a[4], b[4];
+#pragma unroll
+                for (int i = 0; i < 4; i++) a[i] = *reinterpret_cast<const float4*>(xa + (size_t)i * RG * ldx + j);
+#pragma unroll
+                for (int q = 0; q < 4; q++) b[q] = *reinterpret_cast<const float4*>(tb + (size_t)(j + q) * ncpf);
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const float av[4] = {a[i].x, a[i].y, a[i].z, a[i].w};
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        acc[i][0] += av[q] * b[q].x;
+                        acc[i][1] += av[q] * b[q].y;
+                        acc[i][2] += av[q] * b[q].z;
+                        acc[i][3] += av[q] * b[q].w;
+                    }
+                }
+            }
+            if (KG == 1) {
+                if (tm < RG && tn < tnN) {
+#pragma unroll
+                    for (int i = 0; i < 4; i++) {
+                        const int r = tm + RG * i;
+                        if (r < nx)
+                            *reinterpret_cast<float4*>(C1 + (size_t)(c0 + r) * ncpf + 4 * tn) =
+                                make_float4(acc[i][0], acc[i][1], acc[i][2], acc[i][3]);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int e = 0; e < 16; e++) P[(warp * 16 + e) * 32 + lane] = acc[e >> 2][e & 3];
+            }
+        }
+        if (KG > 1) {
+            __syncthreads();
+            // add the KG partial tiles of each warp tile in warp order
+            for (int idx = threadIdx.x; idx < WT * 16 * 32; idx += blockDim.x) {
+                const int ln = idx & 31, e = (idx >> 5) & 15, wt = idx >> 9;
+                const int tm = (wt / WTN) * 4 + (ln >> 3), tn = (wt % WTN) * 8 + (ln & 7);
+                const int r = tm + RG * (e >> 2);
+                if (tm >= RG || tn >= tnN || r >= nx) continue;
+                float v = P[((0 * WT + wt) * 16 + e) * 32 + ln];
+                for (int kg = 1; kg < KG; kg++) v += P[((kg * WT + wt) * 16 + e) * 32 + ln];
+                C1[(size_t)(c0 + r) * ncpf + 4 * tn + (e & 3)] = v;
+            }
+        }
+        __syncthreads();  // X, T and P are free again
+    }
+    if (nzs > 0) {
+        if (threadIdx.x == 0) {
+            const uint32_t b = (uint32_t)nzs * (uint32_t)ldt * 4u;
+            mbar_expect_tx(&bar, b);
+            bulk_g2s(Tt, TzT + (size_t)zs * ldt, b, &bar);
+        }
+        if (!__syncthreads_and(mbar_wait(&bar, ph))) {
+            if (threadIdx.x == 0) {
+                atomicExch(errword, 5);
+                mbar_wait(&bar, ph);
+            }
+            return;
+        }
+    }
+    // S[a][k][ir] from rows 2k, 2k+1 (cos, -sin kz) x columns 2a, 2a+1 (a_m, b_m)
+    {
+        const int tmN = ldt >> 2, WTN = (tnN + 7) >> 3, WT = ((tmN + 3) >> 2) * WTN;
+        for (int wt = warp; wt < WT; wt += FWR_WARPS) {
+            const int tm = (wt / WTN) * 4 + tml, tn = (wt % WTN) * 8 + tnl;
+            const int tmc = min(tm, tmN - 1), tnc = min(tn, tnN - 1);
+            float acc[4][4];
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int c = 0; c < 4; c++) acc[i][c] = 0.f;
+            const float* ta = Tt + 4 * tmc;
+            const float* cbp = C1 + 4 * tnc;
+#pragma unroll 4
+            for (int z = 0; z < nzs; z++) {
+                const float4 a = *reinterpret_cast<const float4*>(ta + (size_t)z * ldt);
+                const float4 b = *reinterpret_cast<const float4*>(cbp + (size_t)z * ncpf);
+                const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    acc[i][0] += av[i] * b.x;
+                    acc[i][1] += av[i] * b.y;
+                    acc[i][2] += av[i] * b.z;
+                    acc[i][3] += av[i] * b.w;
+                }
+            }
+            if (tm < tmN && tn < tnN) {
+#pragma unroll
+                for (int dk = 0; dk < 2; dk++) {
+                    const int k = 2 * tm + dk;
+                    if (k >= nkz) continue;
+#pragma unroll
+                    for (int da = 0; da < 2; da++) {
+                        const int a = (4 * tn + cb) / 2 + da;
+                        if (a >= nact) continue;
+                        S[((size_t)a * nkz + k) * nr + ir] =
+                            make_float4(acc[2 * dk][2 * da], acc[2 * dk + 1][2 * da], acc[2 * dk][2 * da + 1],
+                                        acc[2 * dk + 1][2 * da + 1]);
+                    }
+                }
+            }
+        }
+        if (cb) {
+            // m = 0: 4 lanes per kz, lane q sums the planes z = zs + q (mod 4)
+            const int q = threadIdx.x & 3;
+            for (int kb = 0; kb < nkz; kb += FWR_THREADS / 4) {
+                const int k = kb + (threadIdx.x >> 2);
+                float ac = 0.f, bc = 0.f;
+                if (k < nkz)
+                    for (int z = q; z < nzs; z += 4) {
+                        const float2 t = *reinterpret_cast<const float2*>(Tt + (size_t)z * ldt + 2 * k);
+                        ac += t.x * C0[z];
+                        bc += t.y * C0[z];
+                    }
+#pragma unroll
+                for (int o = 1; o < 4; o <<= 1) {
+                    ac += __shfl_xor_sync(0xffffffffu, ac, o);
+                    bc += __shfl_xor_sync(0xffffffffu, bc, o);
+                }
+                if (k < nkz && q == 0) S[(size_t)k * nr + ir] = make_float4(ac, bc, 0.f, 0.f);
+            }
+        }
+    }
+}
+
+// the column layout of k_fwd_ring's azimuthal table: with m = 0 active its
+// two columns are left out (cb = 2)
+static inline int fwd_ring_cb(const Spec& sp) { return (sp.nact > 0 && sp.m[0] == 0) ? 2 : 0; }
+static inline int fwd_ring_ncpf(const Spec& sp) { return ru4(2 * sp.nact - fwd_ring_cb(sp)); }
+
+// shared memory of k_fwd_ring, bytes; 0 when the geometry does not fit
+static size_t fwd_ring_smem(const DevGeo& g, const Spec& sp) {
+    if (g.na % 4) return 0;
+    const int ncpf = fwd_ring_ncpf(sp);
+    if (ncpf == 0) return 0;
+    const size_t az = (size_t)g.na * ncpf + (size_t)FWR_XR * (g.na + 4);
+    const size_t vz = (size_t)g.ngz * ru4(2 * g.nkz);
+    const size_t b = sizeof(float) * ((size_t)ru4(g.ngz) * (ncpf + 1) + FWR_WARPS * 16 * 32 + std::max(az, vz));
+    return b <= 200 * 1024 ? b : 0;
+}
+
 // 2D forward transform, RB rings per CTA.
 #define RB2 4
 // 2D forward (p2manl.f:32-45): RB2 rings per CTA, one warp per ring; lane c
@@ -459,30 +755,45 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* fr
     }
     if (g.ndim == 3) {
         const size_t ntaz = (size_t)g.na * ncp, ntz = (size_t)ru4(2 * g.nkz) * g.ngz;
+        const int cb = fwd_ring_cb(c->spec), ncpf = fwd_ring_ncpf(c->spec);
+        float* TzT = c->fwdtab ? c->fwdtab + ntaz + ntz : nullptr;
+        float* Tf = c->fwdtab ? TzT + ntz : nullptr;
         if (!c->fwdtab) {
-            GX_CUDA(c, cudaMalloc((void**)&c->fwdtab, sizeof(float) * (ntaz + ntz)));
+            // [Taz][Tz][TzT][Tf]
+            GX_CUDA(c, cudaMalloc((void**)&c->fwdtab, sizeof(float) * (2 * ntaz + 2 * ntz)));
+            TzT = c->fwdtab + ntaz + ntz;
+            Tf = TzT + ntz;
             const size_t mx = std::max(ntaz, ntz);
             k_fwdtab<<<(unsigned)((mx + 255) / 256), 256, 0, c->stream>>>(g, nact, ncp, c->fwdtab,
-                                                                          c->fwdtab + ntaz);
+                                                                          c->fwdtab + ntaz, TzT, Tf, cb, ncpf);
             GX_LAUNCHED(c);
         }
-        if (!c->fwdC1) GX_CUDA(c, cudaMalloc((void**)&c->fwdC1, sizeof(float) * (size_t)g.nrow * ncp));
-        size_t sm = sizeof(float) * ((size_t)FWD_RB * (g.na + 1) + ntaz);
-        GX_CUDA(c, cudaFuncSetAttribute(k_fwd_az, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_fwd_az<<<(g.nrow + FWD_RB - 1) / FWD_RB, 288, sm, c->stream>>>(g, ncp, c->jrk_d, zr, c->mass,
-                                                                         c->fwdtab, c->fwdC1);
-        GX_LAUNCHED(c);
-        sm = sizeof(float) * ((size_t)g.ngz * ncp + (size_t)FWD_KR * g.ngz);
-        GX_CUDA(c, cudaFuncSetAttribute(k_fwd_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        dim3 gz(g.nr, (2 * g.nkz + FWD_KR - 1) / FWD_KR);
-        k_fwd_z<<<gz, 288, sm, c->stream>>>(g, nact, ncp, c->jrk_d, zr, c->fwdC1, c->fwdtab + ntaz,
-                                            c->specS);
-        GX_LAUNCHED(c);
+        const size_t smr = fwd_ring_smem(g, c->spec);
+        if (smr) {
+            GX_CUDA(c, cudaFuncSetAttribute(k_fwd_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr));
+            k_fwd_ring<<<g.nr, FWR_THREADS, smr, c->stream>>>(g, nact, ncpf, cb, c->jrk_d, zr, c->mass, Tf, TzT,
+                                                              c->specS, c->errword);
+            GX_LAUNCHED(c);
+        } else {
+            if (!c->fwdC1) GX_CUDA(c, cudaMalloc((void**)&c->fwdC1, sizeof(float) * (size_t)g.nrow * ncp));
+            size_t sm = sizeof(float) * ((size_t)FWD_RB * (g.na + 1) + ntaz);
+            GX_CUDA(c, cudaFuncSetAttribute(k_fwd_az, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            k_fwd_az<<<(g.nrow + FWD_RB - 1) / FWD_RB, 288, sm, c->stream>>>(g, ncp, c->jrk_d, zr, c->mass,
+                                                                             c->fwdtab, c->fwdC1);
+            GX_LAUNCHED(c);
+            sm = sizeof(float) * ((size_t)g.ngz * ncp + (size_t)FWD_KR * g.ngz);
+            GX_CUDA(c, cudaFuncSetAttribute(k_fwd_z, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+            dim3 gz(g.nr, (2 * g.nkz + FWD_KR - 1) / FWD_KR);
+            k_fwd_z<<<gz, 288, sm, c->stream>>>(g, nact, ncp, c->jrk_d, zr, c->fwdC1, c->fwdtab + ntaz,
+                                                c->specS);
+            GX_LAUNCHED(c);
+        }
     } else {
         const size_t ntaz = (size_t)g.na * ncp;
         if (!c->fwdtab) {
             GX_CUDA(c, cudaMalloc((void**)&c->fwdtab, sizeof(float) * ntaz));
-            k_fwdtab<<<(unsigned)((ntaz + 255) / 256), 256, 0, c->stream>>>(g, nact, ncp, c->fwdtab, nullptr);
+            k_fwdtab<<<(unsigned)((ntaz + 255) / 256), 256, 0, c->stream>>>(g, nact, ncp, c->fwdtab, nullptr,
+                                                                            nullptr, nullptr, 0, 0);
             GX_LAUNCHED(c);
         }
         size_t sm = sizeof(float) * ((size_t)RB2 * (g.na + 1) + ntaz);
