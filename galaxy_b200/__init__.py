@@ -20,7 +20,7 @@ from ._abi import (GxConfig, GxDiag, GxGeometry, make_config, GX_OK, GX_PREC_FP6
                    GX_GRID_POT, GX_GRID_FX, GX_GRID_FY, GX_GREEN_FR, GX_GREEN_FT,
                    GX_GREEN_FZ, GX_GREEN_POT, GX_FLAG_COMPENSATED,
                    GX_FLAG_QUADRATIC, GX_FLAG_WHOLE_GRID, GX_FLAG_SORTED_DEPOSIT,
-                   GX_FLAG_PLANE_SPLIT)
+                   GX_FLAG_PLANE_SPLIT, GX_FLAG_ROWBLOCK_TRANSFORMS)
 
 __all__ = ["Galaxy", "GxError", "GxConfig", "GxDiag", "GxGeometry", "make_config", "lib",
            "LIB_PATH"]

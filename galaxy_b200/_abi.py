@@ -26,6 +26,7 @@ GX_FLAG_QUADRATIC = 2
 GX_FLAG_WHOLE_GRID = 4
 GX_FLAG_SORTED_DEPOSIT = 8
 GX_FLAG_PLANE_SPLIT = 16
+GX_FLAG_ROWBLOCK_TRANSFORMS = 32
 GX_OP_SUM, GX_OP_MIN, GX_OP_MAX = 0, 1, 2
 GX_DT_INT32, GX_DT_FLOAT32 = 0, 1
 

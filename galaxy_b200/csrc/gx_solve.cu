@@ -768,7 +768,7 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* fr
                                                                           c->fwdtab + ntaz, TzT, Tf, cb, ncpf);
             GX_LAUNCHED(c);
         }
-        const size_t smr = fwd_ring_smem(g, c->spec);
+        const size_t smr = (c->cfg.flags & GX_FLAG_ROWBLOCK_TRANSFORMS) ? 0 : fwd_ring_smem(g, c->spec);
         if (smr) {
             GX_CUDA(c, cudaFuncSetAttribute(k_fwd_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr));
             k_fwd_ring<<<g.nr, FWR_THREADS, smr, c->stream>>>(g, nact, ncpf, cb, c->jrk_d, zr, c->mass, Tf, TzT,

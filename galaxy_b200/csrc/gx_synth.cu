@@ -14,6 +14,7 @@
 //            (fx, fy) and one float4 (fx, fy, fz, phi) store per node.
 #include <algorithm>
 
+#include "gx_bulk.cuh"
 #include "gx_common.cuh"
 
 struct ActList {
@@ -28,10 +29,17 @@ struct SynTab {
     const float* TC;   // [nact][njp]    cosine row weights (scaled)
     const float* TS;   // [nact][njp]    sine row weights (scaled)
     const float* CS;   // [2][njp]       cos, sin of the spoke angles 2 pi j / na (polcat)
+    const float* TP;   // [nkz][szr_stride(Z0)] k even: wA(k, z), odd: wB(k, z)  (the P sum)
+    const float* TQ;   // [nkz][szr_stride(Z0)] k even: wB(k, z), odd: wA(k, z)  (the Q sum)
     int Z0, KE, KO, njp;
 };
 
 __host__ __device__ static inline int ru4s(int x) { return (x + 3) & ~3; }
+// row stride of TP / TQ: whole 16-plane blocks, and 8 (mod 32) floats so
+// that the 16-byte table loads of a quarter warp in k_synz_ring (4
+// consecutive wavenumbers x 2 four-plane groups) fall on 8 different groups
+// of 4 banks
+__host__ __device__ static inline int szr_stride(int Z0) { return (((Z0 + 15) & ~15) + 23) / 32 * 32 + 8; }
 
 static void syn_dims(const DevGeo& g, int& Z0, int& KE, int& KO, int& njp) {
     Z0 = g.ngz / 2 + 1;
@@ -53,10 +61,17 @@ __device__ __forceinline__ float wB(int k, int z, int ngz) {
 }
 
 __global__ void k_syntab(DevGeo g, ActList act, int nact, float scale, float* WAe, float* WBe,
-                         float* WAo, float* WBo, float* TC, float* TS, float* CS, int Z0, int KE,
-                         int KO, int njp) {
+                         float* WAo, float* WBo, float* TC, float* TS, float* CS, float* TP, float* TQ,
+                         int Z0, int KE, int KO, int njp) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     const int nz = ru4s(Z0);
+    const int nzt = szr_stride(Z0);
+    if (TP && tid < nzt * g.nkz) {
+        const int k = tid / nzt, z = tid - k * nzt;
+        const float a = (z < Z0) ? wA(k, z, g.ngz) : 0.f, b = (z < Z0) ? wB(k, z, g.ngz) : 0.f;
+        TP[tid] = (k & 1) ? b : a;
+        TQ[tid] = (k & 1) ? a : b;
+    }
     if (tid < nz * KE) {
         int i = tid / nz, z = tid - i * nz;
         WAe[tid] = (z < Z0) ? wA(2 * i, z, g.ngz) : 0.f;
@@ -493,6 +508,308 @@ __global__ void __launch_bounds__(SYNZ_THREADS, 1) k_synz_tc(DevGeo g, int nact,
     }
 }
 
+// ---------------------------------------------------------------------------
+// The vertical synthesis of one ring per CTA, all four field types, in FP32:
+// the ring's spectra O[t][ir][k][a] (four bulk copies) and the tables TP, TQ
+// (two) come into shared memory on one mbarrier.  For the rows y of the
+// needed 16-row blocks (as k_synz_tc: a block is summed when its planes or
+// their mirrors ngz - y are wanted) P[y][c] = sum_k TP[k][y] s_P(k, c) and
+// Q[y][c] = sum_k TQ[k][y] s_Q(k, c), where s_P is the cosine part A of the
+// spectrum at even k and the sine part B at odd k, s_Q the other; plane y is
+// P + Q and plane ngz - y is P - Q.  A thread owns 4 rows x 2 (type,
+// harmonic) pairs (both columns 2a, 2a + 1 of each, P and Q: 32 sums); the
+// wavenumber sum is split over 4 adjacent lanes by k mod 4 (so each lane's
+// k have one parity and its spectrum parts are fixed) and added by
+// shuffles.  A warp takes 4 row groups x 2 pairs: its table loads are 4 x 4
+// distinct 16-byte words, its spectrum loads 2 x 4.  With m = 0 active its
+// column is summed apart (2 warps), its sine column is zero.
+#define SZR_THREADS 512
+#define SZR_WARPS (SZR_THREADS / 32)
+#define SZR_MAXBLK 64  // 16-row blocks at most (Z0 <= 1024)
+// the field type of the n-th set bit of tmask
+__device__ __forceinline__ int nth_type(int tmask, int n) {
+    int t = 0;
+#pragma unroll
+    for (int b = 0; b < 4; b++)
+        if ((tmask >> b) & 1) {
+            if (n == 0) t = b;
+            n--;
+        }
+    return t;
+}
+__global__ void __launch_bounds__(SZR_THREADS, 1) k_syn_ring(DevGeo g, int nact, int a0, int ncp, int tmask,
+                                                             const float4* __restrict__ O, SynTab tb,
+                                                             float* __restrict__ R, float4* __restrict__ F,
+                                                             float* __restrict__ polar,
+                                                             const int32_t* __restrict__ frk,
+                                                             const int32_t* __restrict__ zr,
+                                                             int32_t* __restrict__ errword) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ uint64_t bar;
+    __shared__ int s_blk[SZR_MAXBLK], s_nblk;
+    const int ir = blockIdx.x;
+    if (frk && (ir + 1 < frk[0] || ir + 1 > frk[1])) return;  // rings no moving particle reads
+    const int nr = g.nr, nkz = g.nkz, ngz = g.ngz, Z0 = tb.Z0, nz4 = szr_stride(Z0);
+    float4* OS = reinterpret_cast<float4*>(sm);            // [4][nkz][nact]
+    float* TP = sm + (size_t)16 * nkz * nact;              // [nkz][nz4]
+    float* TQ = TP + (size_t)nkz * nz4;
+    const int zlo = zr ? max(zr[0] - 1, 0) : 0, zhi = zr ? min(zr[1] + 1, ngz - 1) : ngz - 1;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t ob = (uint32_t)(nkz * nact) * 16u, tb4 = (uint32_t)(nkz * nz4) * 4u;
+        uint32_t tot = 2 * tb4;
+        for (int t = 0; t < 4; t++)
+            if ((tmask >> t) & 1) tot += ob;
+        mbar_expect_tx(&bar, tot);
+        bulk_g2s(TP, tb.TP, tb4, &bar);
+        bulk_g2s(TQ, tb.TQ, tb4, &bar);
+        for (int t = 0; t < 4; t++)
+            if ((tmask >> t) & 1)
+                bulk_g2s(OS + (size_t)t * nkz * nact, O + ((size_t)t * nr + ir) * nkz * nact, ob, &bar);
+    }
+    if (!__syncthreads_and(mbar_wait(&bar, 0))) {
+        if (threadIdx.x == 0) {
+            atomicExch(errword, 6);
+            mbar_wait(&bar, 0);  // the copies in flight land before the CTA leaves
+        }
+        return;
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, ks = lane & 3, tl = lane >> 2;
+    const int yg = tl & 3, pl = tl >> 2, par = ks & 1;
+    // the field types wanted (tmask) and the 16-row blocks summed
+    const int nty = __popc(tmask & 15);
+    if (threadIdx.x == 0) {
+        int n = 0;
+        for (int yb = 0; yb < Z0; yb += 16) {
+            const int y1 = min(yb + 15, Z0 - 1);
+            if ((yb <= zhi && y1 >= zlo) || (ngz - y1 <= zhi && ngz - yb >= zlo)) s_blk[n++] = yb;
+        }
+        s_nblk = n;
+    }
+    __syncthreads();
+    const int nblk = s_nblk;
+    const int nh = nact - a0, nu = nty * nh, npair = (nu + 1) >> 1, npg = (npair + 1) >> 1;
+    // units: (block, 2 pairs) for the harmonics a >= a0, then (block, 2 types)
+    // for m = 0; dealt to the warps in turn
+    const int nmain = nblk * npg, nunit = nmain + (a0 ? nblk * 2 : 0);
+    for (int un = warp; un < nunit; un += SZR_WARPS) {
+        if (un < nmain) {
+            const int y = s_blk[un / npg] + 4 * yg;
+            const int p = (un % npg) * 2 + pl;
+            int tu[2], au[2];
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                const int uu = min(2 * p + u, nu - 1);
+                const int ti = uu / nh;
+                tu[u] = nth_type(tmask, ti);
+                au[u] = a0 + (uu - ti * nh);
+            }
+            float P[2][4][2], Q[2][4][2];
+#pragma unroll
+            for (int u = 0; u < 2; u++)
+#pragma unroll
+                for (int i = 0; i < 4; i++) P[u][i][0] = P[u][i][1] = Q[u][i][0] = Q[u][i][1] = 0.f;
+            const float4* o0 = OS + (size_t)tu[0] * nkz * nact + au[0];
+            const float4* o1 = OS + (size_t)tu[1] * nkz * nact + au[1];
+            // P takes the cosine part (x, z) at even k, the sine part (y, w) at
+            // odd k, Q the other; a lane's k have one parity, so it sums the
+            // cosine part against tx and the sine part against ty (TP and TQ
+            // in its parity's roles) into P and Q, swapped at odd parity below
+            const float* tx = par ? TQ : TP;
+            const float* ty = par ? TP : TQ;
+#pragma unroll 2
+            for (int k = ks; k < nkz; k += 4) {
+                const float4 ta = *reinterpret_cast<const float4*>(tx + (size_t)k * nz4 + y);
+                const float4 tb4 = *reinterpret_cast<const float4*>(ty + (size_t)k * nz4 + y);
+                const float4 s0 = o0[(size_t)k * nact], s1 = o1[(size_t)k * nact];
+                const float tav[4] = {ta.x, ta.y, ta.z, ta.w}, tbv[4] = {tb4.x, tb4.y, tb4.z, tb4.w};
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    P[0][i][0] += tav[i] * s0.x; P[0][i][1] += tav[i] * s0.z;
+                    Q[0][i][0] += tbv[i] * s0.y; Q[0][i][1] += tbv[i] * s0.w;
+                    P[1][i][0] += tav[i] * s1.x; P[1][i][1] += tav[i] * s1.z;
+                    Q[1][i][0] += tbv[i] * s1.y; Q[1][i][1] += tbv[i] * s1.w;
+                }
+            }
+            if (par) {
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int c = 0; c < 2; c++) {
+                            const float t = P[u][i][c];
+                            P[u][i][c] = Q[u][i][c];
+                            Q[u][i][c] = t;
+                        }
+            }
+#pragma unroll
+            for (int o = 1; o < 4; o <<= 1)
+#pragma unroll
+                for (int u = 0; u < 2; u++)
+#pragma unroll
+                    for (int i = 0; i < 4; i++)
+#pragma unroll
+                        for (int c = 0; c < 2; c++) {
+                            P[u][i][c] += __shfl_xor_sync(0xffffffffu, P[u][i][c], o);
+                            Q[u][i][c] += __shfl_xor_sync(0xffffffffu, Q[u][i][c], o);
+                        }
+            if (ks != 0 || p >= npair) continue;
+#pragma unroll
+            for (int u = 0; u < 2; u++) {
+                if (2 * p + u >= nu) continue;
+                float* Rt = R + (((size_t)tu[u] * nr + ir) * ngz) * ncp + 2 * au[u];
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int z = y + i;
+                    if (z >= Z0) continue;
+                    *reinterpret_cast<float2*>(Rt + (size_t)z * ncp) =
+                        make_float2(P[u][i][0] + Q[u][i][0], P[u][i][1] + Q[u][i][1]);
+                    const int zm = ngz - z;
+                    if (z >= 1 && zm != z && zm < ngz)
+                        *reinterpret_cast<float2*>(Rt + (size_t)zm * ncp) =
+                            make_float2(P[u][i][0] - Q[u][i][0], P[u][i][1] - Q[u][i][1]);
+                }
+            }
+        } else {
+            // m = 0: 4 row groups x 2 types per unit, the cosine column only
+            const int um = un - nmain;
+            const int y = s_blk[um >> 1] + 4 * yg;
+            const int tt = (um & 1) * 2 + pl;  // 0..3
+            const float4* os = OS + (size_t)tt * nkz * nact;
+            float Pc[4] = {0.f, 0.f, 0.f, 0.f}, Qc[4] = {0.f, 0.f, 0.f, 0.f};
+            const float* tx = par ? TQ : TP;
+            const float* ty = par ? TP : TQ;
+            for (int k = ks; k < nkz; k += 4) {
+                const float4 ta = *reinterpret_cast<const float4*>(tx + (size_t)k * nz4 + y);
+                const float4 tb4 = *reinterpret_cast<const float4*>(ty + (size_t)k * nz4 + y);
+                const float4 sv = os[(size_t)k * nact];
+                Pc[0] += ta.x * sv.x; Pc[1] += ta.y * sv.x; Pc[2] += ta.z * sv.x; Pc[3] += ta.w * sv.x;
+                Qc[0] += tb4.x * sv.y; Qc[1] += tb4.y * sv.y; Qc[2] += tb4.z * sv.y; Qc[3] += tb4.w * sv.y;
+            }
+            if (par) {
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const float t = Pc[i];
+                    Pc[i] = Qc[i];
+                    Qc[i] = t;
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < 4; o <<= 1)
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    Pc[i] += __shfl_xor_sync(0xffffffffu, Pc[i], o);
+                    Qc[i] += __shfl_xor_sync(0xffffffffu, Qc[i], o);
+                }
+            if (ks == 0 && ((tmask >> tt) & 1)) {
+                float* Rt = R + (((size_t)tt * nr + ir) * ngz) * ncp;
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const int z = y + i;
+                    if (z >= Z0) continue;
+                    *reinterpret_cast<float2*>(Rt + (size_t)z * ncp) = make_float2(Pc[i] + Qc[i], 0.f);
+                    const int zm = ngz - z;
+                    if (z >= 1 && zm != z && zm < ngz)
+                        *reinterpret_cast<float2*>(Rt + (size_t)zm * ncp) = make_float2(Pc[i] - Qc[i], 0.f);
+                }
+            }
+        }
+    }
+    // ---- azimuthal synthesis and polcat of the ring (as k_synaz) ----
+    // R of the planes [zlo, zhi] comes back from L2 (written above by this
+    // CTA: visible after the barrier; loads that bypass L1), the tables TC,
+    // TS, CS with it; both into the space the spectra and TP / TQ held
+    __syncthreads();
+    const int nzw = zhi - zlo + 1;
+    if (nzw <= 0) return;
+    const int njp = tb.njp, na = g.na, nq = njp >> 2, half = na / 2;
+    float* TCs = sm;                         // [nact][njp]
+    float* TSs = TCs + (size_t)nact * njp;   // [nact][njp]
+    float* CSs = TSs + (size_t)nact * njp;   // [2][njp]
+    float* Rs = CSs + 2 * njp;               // [4][nzw][ncp]
+    {
+        const float4* src = reinterpret_cast<const float4*>(tb.TC);
+        float4* dst = reinterpret_cast<float4*>(TCs);
+        const int n4 = (2 * (nact + 1) * njp) >> 2;
+        for (int i = threadIdx.x; i < n4; i += blockDim.x) dst[i] = __ldg(src + i);
+        const int nrow4 = (nzw * ncp) >> 2;
+        for (int t = 0; t < 4; t++) {
+            float4* d = reinterpret_cast<float4*>(Rs + (size_t)t * nzw * ncp);
+            if ((tmask >> t) & 1) {
+                const float4* s4 = reinterpret_cast<const float4*>(R + (((size_t)t * nr + ir) * ngz + zlo) * ncp);
+                for (int i = threadIdx.x; i < nrow4; i += blockDim.x) d[i] = __ldcg(s4 + i);
+            } else {
+                for (int i = threadIdx.x; i < nrow4; i += blockDim.x) d[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        }
+    }
+    __syncthreads();
+    const size_t mesh = g.mesh;
+    for (int it = threadIdx.x; it < nzw * nq; it += blockDim.x) {
+        const int z = it / nq, j0 = (it - z * nq) * 4;
+        float C[4][4], S[4][4];
+#pragma unroll
+        for (int t = 0; t < 4; t++)
+#pragma unroll
+            for (int q = 0; q < 4; q++) C[t][q] = S[t][q] = 0.f;
+        for (int a = 0; a < nact; a++) {
+            const float4 tc = *reinterpret_cast<const float4*>(TCs + a * njp + j0);
+            const float4 ts = *reinterpret_cast<const float4*>(TSs + a * njp + j0);
+#pragma unroll
+            for (int t = 0; t < 4; t++) {
+                const float2 r = *reinterpret_cast<const float2*>(Rs + ((size_t)t * nzw + z) * ncp + 2 * a);
+                C[t][0] += r.x * tc.x; C[t][1] += r.x * tc.y; C[t][2] += r.x * tc.z; C[t][3] += r.x * tc.w;
+                S[t][0] += r.y * ts.x; S[t][1] += r.y * ts.y; S[t][2] += r.y * ts.z; S[t][3] += r.y * ts.w;
+            }
+        }
+        const size_t rowb = ((size_t)ir * ngz + zlo + z) * na;
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int j = j0 + q;
+            if (j > half) continue;
+            const float cs = CSs[j], sn = CSs[njp + j];
+            {
+                const float fr = C[0][q] + S[0][q], ft = C[1][q] + S[1][q];
+                const float fz = C[2][q] + S[2][q], ph = C[3][q] + S[3][q];
+                F[rowb + j] = make_float4(fr * cs - ft * sn, fr * sn + ft * cs, fz, ph);
+                if (polar) {
+                    polar[rowb + j] = fr;
+                    polar[mesh + rowb + j] = ft;
+                    polar[2 * mesh + rowb + j] = fz;
+                    polar[3 * mesh + rowb + j] = ph;
+                }
+            }
+            if (j > 0 && j < half) {
+                const int jm = na - j;  // angle -theta_j: cos same, sin negated
+                const float fr = C[0][q] - S[0][q], ft = C[1][q] - S[1][q];
+                const float fz = C[2][q] - S[2][q], ph = C[3][q] - S[3][q];
+                F[rowb + jm] = make_float4(fr * cs + ft * sn, -fr * sn + ft * cs, fz, ph);
+                if (polar) {
+                    polar[rowb + jm] = fr;
+                    polar[mesh + rowb + jm] = ft;
+                    polar[2 * mesh + rowb + jm] = fz;
+                    polar[3 * mesh + rowb + jm] = ph;
+                }
+            }
+        }
+    }
+}
+
+// shared memory of k_syn_ring, bytes; 0 when the ring's data do not fit
+static size_t syn_ring_smem(const DevGeo& g, int nact, int Z0, int njp, int ncp) {
+    // vertical part: the four types' spectra (float4 per wavenumber and
+    // harmonic), TP and TQ; azimuthal part: TC, TS, CS and R of every plane
+    const size_t v = (size_t)4 * sizeof(float4) * g.nkz * nact + (size_t)2 * sizeof(float) * g.nkz * szr_stride(Z0);
+    const size_t a = sizeof(float) * ((size_t)2 * (nact + 1) * njp + (size_t)4 * g.ngz * ncp);
+    const size_t b = std::max(v, a);
+    return (g.ndim == 3 && (Z0 + 15) / 16 <= SZR_MAXBLK && b <= 220 * 1024) ? b : 0;
+}
+
 #define SYN_ZB 16
 // 288 threads: the SYN_ZB x njp / 4 (plane, 4-spoke) items of a CTA (528 at
 // 256 spokes) take two passes instead of two and a sliver
@@ -632,27 +949,42 @@ int gx_synthesis(GxCtx* c, int tmask, float* polar, const int32_t* frk, const in
     syn_dims(g, Z0, KE, KO, njp);
     const int nz4 = ru4s(Z0);
     const size_t nWe = (size_t)nz4 * KE, nWo = (size_t)nz4 * KO, nT = (size_t)nact * njp;
+    const size_t nTk = g.ndim == 3 ? (size_t)szr_stride(Z0) * g.nkz : 0;  // TP, TQ
     if (!c->syntab) {
         if (nact > 64) return c->err = "more than 64 active harmonics", GX_ERR_RANGE;
-        const size_t tot = 2 * nWe + 2 * nWo + 2 * nT + 2 * (size_t)njp;
+        const size_t tot = 2 * nWe + 2 * nWo + 2 * nT + 2 * (size_t)njp + 2 * nTk;
         GX_CUDA(c, cudaMalloc((void**)&c->syntab, sizeof(float) * tot));
         ActList act;
         for (int a = 0; a < 64; a++) act.m[a] = a < nact ? c->spec.m[a] : 0;
         const float scale = (g.ndim == 3) ? 1.0f / (float)(2 * g.ngz * g.na) : 1.0f / (float)g.na;
         float* b = c->syntab;
-        const size_t mx = std::max(std::max(nWe, nWo), std::max(nT, (size_t)njp));
+        const size_t mx = std::max(std::max(std::max(nWe, nWo), std::max(nT, (size_t)njp)), nTk);
+        float* tk = b + 2 * nWe + 2 * nWo + 2 * nT + 2 * njp;
         k_syntab<<<(unsigned)((mx + 255) / 256), 256, 0, c->stream>>>(
             g, act, nact, scale, b, b + nWe, b + 2 * nWe, b + 2 * nWe + nWo, b + 2 * nWe + 2 * nWo,
-            b + 2 * nWe + 2 * nWo + nT, b + 2 * nWe + 2 * nWo + 2 * nT, Z0, KE, KO, njp);
+            b + 2 * nWe + 2 * nWo + nT, b + 2 * nWe + 2 * nWo + 2 * nT, nTk ? tk : nullptr, nTk ? tk + nTk : nullptr,
+            Z0, KE, KO, njp);
         GX_LAUNCHED(c);
     }
     if (!c->synR) GX_CUDA(c, cudaMalloc((void**)&c->synR, sizeof(float) * 4 * g.nr * g.ngz * ncp));
     const float* b = c->syntab;
+    const float* tk = b + 2 * nWe + 2 * nWo + 2 * nT + 2 * njp;
     SynTab tb{b, b + nWe, b + 2 * nWe, b + 2 * nWe + nWo, b + 2 * nWe + 2 * nWo,
-              b + 2 * nWe + 2 * nWo + nT, b + 2 * nWe + 2 * nWo + 2 * nT, Z0, KE, KO, njp};
+              b + 2 * nWe + 2 * nWo + nT, b + 2 * nWe + 2 * nWo + 2 * nT, tk, tk + nTk, Z0, KE, KO, njp};
     if (g.ndim == 3) {
-        // the tables, three bank pads of at most 31 floats, the spectrum
+        const size_t smr =
+            (c->cfg.flags & GX_FLAG_ROWBLOCK_TRANSFORMS) ? 0 : syn_ring_smem(g, nact, Z0, njp, ncp);
+        if (smr) {
+            // vertical and azimuthal synthesis and polcat of one ring per CTA
+            const int a0 = c->spec.m[0] == 0 ? 1 : 0;
+            GX_CUDA(c, cudaFuncSetAttribute(k_syn_ring, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smr));
+            k_syn_ring<<<g.nr, SZR_THREADS, smr, c->stream>>>(g, nact, a0, ncp, tmask, c->specO, tb, c->synR,
+                                                               c->field, polar, frk, zr, c->errword);
+            GX_LAUNCHED(c);
+            return GX_OK;
+        }
         if (gx_synz_tc_ok(g, nact, ncp)) {
+            // the tables, three bank pads of at most 31 floats, the spectrum
             int sms = 148;
             GX_CUDA(c, cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->dev));
             const size_t sm = sizeof(float) * (8 * SZT_K * 64 + 4 * SZT_K * SZT_SS);

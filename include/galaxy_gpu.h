@@ -74,6 +74,12 @@ extern "C" {
                                    fixed-point items, combine) instead of the
                                    fused pass over the bucketed particle store;
                                    the two give bitwise identical results */
+#define GX_FLAG_ROWBLOCK_TRANSFORMS 32 /* 3D mixed path: the field solve's transforms
+                                   with the kernels that take any grid (per block of
+                                   ring-plane rows or per ring and field type),
+                                   instead of the per-ring kernels that hold a ring's
+                                   planes, spectra and tables in shared memory; the
+                                   results agree to FP32 rounding */
 #define GX_MAX_WEIGHTS     27   /* weights per particle of gx_weight          */
 
 /* grid arrays for gx_get_grid / gx_set_mass */

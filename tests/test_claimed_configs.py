@@ -21,7 +21,8 @@ import numpy as np
 import pytest
 
 from galaxy_b200 import (Galaxy, make_config, GX_PREC_FP64, GX_PREC_MIXED, GX_RMAP_LOG,
-                         GX_GRID_MASS, GX_GRID_FR, GX_GRID_FT, GX_GRID_FZ, GX_GRID_POT)
+                         GX_GRID_MASS, GX_GRID_FR, GX_GRID_FT, GX_GRID_FZ, GX_GRID_POT,
+                         GX_FLAG_ROWBLOCK_TRANSFORMS)
 from galaxy_b200.disk import kt_disk
 from oracle import oracle as ox
 
@@ -195,20 +196,27 @@ def test_bench2_200_steps_track_oracle_fp64(precision, tol):
     assert abs(a - b) < 1e-4 * abs(b), (a, b)
 
 
-# grids the tensor-core vertical synthesis does not take: 68 even
-# wavenumbers (ngz = 135), and 81 spectral columns (m = 0..40)
+# Transform kernels by grid.  By default the per-ring kernels take every
+# grid below; with GX_FLAG_ROWBLOCK_TRANSFORMS the general kernels run:
+# the forward k_fwd_az + k_fwd_z, and for the vertical synthesis the
+# tensor-core k_synz_tc ("std") or, where it does not take the grid, the FP32
+# k_synz (68 even wavenumbers at ngz = 135, 81 spectral columns at
+# m = 0..40), then k_synaz.
 FALLBACK = {
     "ngz135": dict(nr=32, na=32, ngz=135, dzg=0.02, ng=5),
     "m0..40": dict(nr=32, na=128, ngz=15, dzg=0.1, ng=41),
+    "std": dict(nr=32, na=64, ngz=45, dzg=0.05, ng=9),
 }
 
 
+@pytest.mark.parametrize("rowblock", [False, True], ids=["ring", "rowblock"])
 @pytest.mark.parametrize("case", sorted(FALLBACK))
-def test_fp32_vertical_synthesis_grids_vs_oracle(case):
+def test_fp32_vertical_synthesis_grids_vs_oracle(case, rowblock):
     p = FALLBACK[case]
     nr = p["nr"]
     cfg = make_config(3, nr, p["na"], ngz=p["ngz"], dzg=p["dzg"], ng=p["ng"], rmap=GX_RMAP_LOG,
-                      rmap_a=float(np.log(100.0) / (nr - 1)), rmap_r0=0.05, softl=0.2, tsoft=1)
+                      rmap_a=float(np.log(100.0) / (nr - 1)), rmap_r0=0.05, softl=0.2, tsoft=1,
+                      flags=GX_FLAG_ROWBLOCK_TRANSFORMS if rowblock else 0)
     rec, pm = kt_disk(100_000, seed=31, rmax=4.5, ndim=3, z0=0.3, dt=0.02)
     cfg.pmass = pm
     G = ox.green(cfg, 64)
