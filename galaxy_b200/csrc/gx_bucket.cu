@@ -676,12 +676,15 @@ bool gx_fast_ok(const GxCtx* c) {
 static inline int bk_nplanes(const GxCtx* c) { return 2 * c->g.ndim + (c->g.comp ? c->g.ndim : 0); }
 
 // bucketed store -> the host records (x, y[, z], vx, vy[, vz]) in load
-// order, straight from the records (unload without the dense store): each
-// record is read once, coalesced, and written as one 16 / 24-byte record
-template <int NP, int NW>
-__global__ void k_bk_unload(const float4* __restrict__ Qin, int64_t bcap, float* __restrict__ aos,
-                            const int4* __restrict__ items, const int32_t* __restrict__ ctl) {
-    static_assert(NW == 4 || NW == 6, "2D or 3D records");
+// order, in two passes: k_bk_inv writes each record's slot at its load
+// index (4-byte scattered writes into an n-entry table that stays in L2),
+// k_bk_gather walks the load indices in order, reads each record (one
+// 32-byte access) and writes the host layout contiguously.  Writing the
+// 16 / 24-byte records straight to their scattered load positions (one
+// pass) made partial-sector writes over an output larger than L2.
+template <int NP>
+__global__ void k_bk_inv(const float4* __restrict__ Qin, int64_t bcap, int32_t* __restrict__ inv,
+                         const int4* __restrict__ items, const int32_t* __restrict__ ctl) {
     const int nit = ctl[0];
     for (int it = blockIdx.x; it < nit; it += gridDim.x) {
         const int4 I = items[it];
@@ -689,16 +692,36 @@ __global__ void k_bk_unload(const float4* __restrict__ Qin, int64_t bcap, float*
             float w[NP];
             int32_t o;
             rec_load<NP>(Qin, bcap, s, w, o);
-            if (NW == 4) {
-                reinterpret_cast<float4*>(aos)[o] = make_float4(w[0], w[1], w[2], w[3]);
-            } else {
-                float2* d = reinterpret_cast<float2*>(aos + (size_t)o * 6);
-                d[0] = make_float2(w[0], w[1]);
-                d[1] = make_float2(w[2], w[3]);
-                d[2] = make_float2(w[4], w[5]);
-            }
+            inv[o] = s;
         }
     }
+}
+
+template <int NP, int NW>
+__global__ void k_bk_gather(const float4* __restrict__ Qin, int64_t bcap, const int32_t* __restrict__ inv,
+                            float* __restrict__ aos, int64_t n) {
+    static_assert(NW == 4 || NW == 6, "2D or 3D records");
+    const int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (o >= n) return;
+    float w[NP];
+    int32_t oo;
+    rec_load<NP>(Qin, bcap, __ldg(inv + o), w, oo);
+    if (NW == 4) {
+        reinterpret_cast<float4*>(aos)[o] = make_float4(w[0], w[1], w[2], w[3]);
+    } else {
+        float2* d = reinterpret_cast<float2*>(aos + (size_t)o * 6);
+        d[0] = make_float2(w[0], w[1]);
+        d[1] = make_float2(w[2], w[3]);
+        d[2] = make_float2(w[4], w[5]);
+    }
+}
+
+template <int NP, int NW>
+static void bk_unload_launch(GxCtx* c, float* aos) {
+    int32_t* inv = c->pkey[0];  // free while the store is bucketed (the keys are recomputed after it)
+    k_bk_inv<NP><<<148 * 8, 256, 0, c->stream>>>(c->bq[c->bcur], c->bcap, inv, c->bk_items, c->bk_ctl + 8);
+    k_bk_gather<NP, NW><<<(unsigned)((c->n + 255) / 256), 256, 0, c->stream>>>(c->bq[c->bcur], c->bcap, inv,
+                                                                                aos, c->n);
 }
 
 // float4 words of one record of the bucketed store
@@ -859,19 +882,17 @@ int gx_dense(GxCtx* c) {
 
 // gx_unload's records from the bucketed store (the store stays as it is)
 int gx_bucket_unload(GxCtx* c, float* aos) {
-    const unsigned grid = 148 * 8;
-    const float4* Q = c->bq[c->bcur];
-    const int4* it = c->bk_items;
-    const int32_t* ctl = c->bk_ctl + 8;
+    if (c->n <= 0) return GX_OK;
     // record planes: the phase space (2D: 4, 3D: 6) and the compensated
     // update's low parts of the positions
     if (c->g.ndim == 3) {
-        if (c->g.comp) k_bk_unload<9, 6><<<grid, 256, 0, c->stream>>>(Q, c->bcap, aos, it, ctl);
-        else k_bk_unload<6, 6><<<grid, 256, 0, c->stream>>>(Q, c->bcap, aos, it, ctl);
+        if (c->g.comp) bk_unload_launch<9, 6>(c, aos);
+        else bk_unload_launch<6, 6>(c, aos);
     } else {
-        if (c->g.comp) k_bk_unload<6, 4><<<grid, 256, 0, c->stream>>>(Q, c->bcap, aos, it, ctl);
-        else k_bk_unload<4, 4><<<grid, 256, 0, c->stream>>>(Q, c->bcap, aos, it, ctl);
+        if (c->g.comp) bk_unload_launch<6, 4>(c, aos);
+        else bk_unload_launch<4, 4>(c, aos);
     }
+    c->launches++;  // two kernels: the inversion and the gather
     GX_LAUNCHED(c);
     return GX_OK;
 }
