@@ -1,5 +1,9 @@
 // gx_solve.cu -- field solve of the mixed-precision path (findf).
 //
+//   k_fwd_ring (3D)   p3manl.f:62-109: the azimuthal and vertical DFTs of
+//                     one ring per CTA, the ring's planes and the tables
+//                     bulk-copied into shared memory (grids whose ring data
+//                     fit, unless GX_FLAG_ROWBLOCK_TRANSFORMS);
 //   k_fwd_az, k_fwd_z (3D) / k_fwd2 (2D)   p3manl.f:62-109 / p2manl.f:32-45:
 //                     the azimuthal real DFT of every ring-plane row
 //                     restricted to the active harmonics (the m = 0 term

@@ -2,7 +2,10 @@
 // p2fsyn.f:34-56) fused with polcat (polcat.f:22-41).
 //
 // The inverse transforms are small GEMMs against twiddle tables built once
-// per context; both exploit the symmetry of a real inverse DFT:
+// per context.  In 3D, k_syn_ring does the vertical and the azimuthal
+// synthesis and polcat of one ring per CTA (grids whose ring data fit in
+// shared memory, unless GX_FLAG_ROWBLOCK_TRANSFORMS); the general kernels
+// below take any grid.  Both exploit the symmetry of a real inverse DFT:
 //   k_synz   vertical synthesis r(z) = sum_k A_k wA(k,z) + B_k wB(k,z) over
 //            the ngz + 1 wavenumbers of the doubled grid, only for the
 //            physical planes.  With E/O the sums over even/odd k,
