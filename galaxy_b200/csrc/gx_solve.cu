@@ -598,49 +598,54 @@ static size_t fwd_ring_smem(const DevGeo& g, const Spec& sp) {
     return b <= 200 * 1024 ? b : 0;
 }
 
-// 2D forward transform, RB rings per CTA.
-#define RB2 4
-// 2D forward (p2manl.f:32-45): RB2 rings per CTA, one warp per ring; lane c
-// sums column c of the active-harmonic DFT (the twiddle table of the
-// context, k_fwdtab) over the ring's na spokes in spoke order, the m = 0
-// column in FP64 over the warp.  S[a nr + ir] = (a_m, 0, b_m, 0).
-__global__ void __launch_bounds__(32 * RB2) k_fwd2(DevGeo g, int nact, int ncp, const float* __restrict__ mass,
-                                                   const float* __restrict__ Taz, float4* __restrict__ S) {
+// 2D forward (p2manl.f:32-45), one ring per CTA of F2_THREADS: thread
+// (a, q) sums harmonic a (of a block of F2_H) over the spokes j = q (mod
+// F2_Q) in spoke order, the twiddles read through L1 (the context's table,
+// k_fwdtab); the F2_Q partials are added in q order.  The m = 0 column is
+// summed in FP64 over a warp.  S[a nr + ir] = (a_m, 0, b_m, 0).
+#define F2_H 16
+#define F2_Q 16
+#define F2_THREADS (F2_H * F2_Q)
+__global__ void __launch_bounds__(F2_THREADS) k_fwd2(DevGeo g, int nact, int ncp, const float* __restrict__ mass,
+                                                     const float* __restrict__ Taz, float4* __restrict__ S) {
     extern __shared__ __align__(16) float sm[];
-    const int na = g.na, nr = g.nr;
-    const int ldx = na + 1;
-    const int ir0 = blockIdx.x * RB2;
-    float* X = sm;                   // [RB2][na + 1]
-    float* T = X + RB2 * ldx;        // [na][ncp]
-    for (int i = threadIdx.x; i < RB2 * na; i += blockDim.x) {
-        const int r = i / na, j = i - r * na, ir = ir0 + r;
-        X[r * ldx + j] = (ir < nr) ? __ldg(mass + (size_t)ir * na + j) : 0.f;
-    }
-    for (int i = threadIdx.x; i < na * ncp; i += blockDim.x) T[i] = __ldg(Taz + i);
+    __shared__ float2 part[F2_Q][F2_H];
+    const int na = g.na, nr = g.nr, ir = blockIdx.x;
+    float* x = sm;  // [na]
+    for (int j = threadIdx.x; j < na; j += blockDim.x) x[j] = __ldg(mass + (size_t)ir * na + j);
     __syncthreads();
-    const int r = threadIdx.x >> 5, lane = threadIdx.x & 31, ir = ir0 + r;
-    if (ir >= nr) return;
-    const float* x = X + r * ldx;
-    for (int c0 = 0; c0 < 2 * nact; c0 += 64) {
-        // two columns per lane per pass: cosine and sine of one harmonic
-        const int a = (c0 >> 1) + lane;
+    const int h = threadIdx.x % F2_H, q = threadIdx.x / F2_H;
+    for (int a0 = 0; a0 < nact; a0 += F2_H) {
+        const int a = a0 + h;
         float sc = 0.f, ss = 0.f;
         if (a < nact) {
-            for (int j = 0; j < na; j++) {
+#pragma unroll 4
+            for (int j = q; j < na; j += F2_Q) {
                 const float xv = x[j];
-                const float2 t = *reinterpret_cast<const float2*>(T + (size_t)j * ncp + 2 * a);
+                const float2 t = __ldg(reinterpret_cast<const float2*>(Taz + (size_t)j * ncp + 2 * a));
                 sc += xv * t.x;
                 ss += xv * t.y;
             }
         }
-        if (a < nact && !(a == 0 && g.act[0] == 0)) S[(size_t)a * nr + ir] = make_float4(sc, 0.f, ss, 0.f);
+        part[q][h] = make_float2(sc, ss);
+        __syncthreads();
+        if (threadIdx.x < F2_H && a0 + (int)threadIdx.x < nact) {
+            const int aa = a0 + threadIdx.x;
+            float2 v = part[0][threadIdx.x];
+            for (int k = 1; k < F2_Q; k++) {
+                v.x += part[k][threadIdx.x].x;
+                v.y += part[k][threadIdx.x].y;
+            }
+            if (!(aa == 0 && g.act[0] == 0)) S[(size_t)aa * nr + ir] = make_float4(v.x, 0.f, v.y, 0.f);
+        }
+        __syncthreads();
     }
-    if (g.act[0] == 0) {
+    if (g.act[0] == 0 && threadIdx.x < 32) {
         double s0 = 0.0;
-        for (int j = lane; j < na; j += 32) s0 += (double)x[j];
+        for (int j = threadIdx.x; j < na; j += 32) s0 += (double)x[j];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-        if (lane == 0) S[ir] = make_float4((float)s0, 0.f, 0.f, 0.f);
+        if (threadIdx.x == 0) S[ir] = make_float4((float)s0, 0.f, 0.f, 0.f);
     }
 }
 
@@ -800,10 +805,9 @@ int gx_mixed_findf(GxCtx* c, int lpot, bool polcat_only_field, const int32_t* fr
                                                                             nullptr, nullptr, 0, 0);
             GX_LAUNCHED(c);
         }
-        size_t sm = sizeof(float) * ((size_t)RB2 * (g.na + 1) + ntaz);
+        const size_t sm = sizeof(float) * (size_t)g.na;
         GX_CUDA(c, cudaFuncSetAttribute(k_fwd2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        int nb = (g.nr + RB2 - 1) / RB2;
-        k_fwd2<<<nb, 32 * RB2, sm, c->stream>>>(g, nact, ncp, c->mass, c->fwdtab, c->specS);
+        k_fwd2<<<g.nr, F2_THREADS, sm, c->stream>>>(g, nact, ncp, c->mass, c->fwdtab, c->specS);
         GX_LAUNCHED(c);
     }
     rc = gx_comm_reduce_spectrum(c);
